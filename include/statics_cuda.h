@@ -1,0 +1,201 @@
+/*
+ * statics_cuda.h — C ABI of the B200 (sm_100a) statics solver.
+ *
+ * The solver answers the reference's `statics::bodies::motions`
+ * (SupraSummus/parallax-world, statics/src/bodies.rs:429): every free node's 6-DOF
+ * motion (translation, rotation) under its loads, by conjugate gradients
+ * preconditioned with a smoothed-aggregation V-cycle over "bodies within bodies"
+ * (octree cells of 2^l level-0 cells, statics/src/lattice.rs:45-47), the top level
+ * solved by a dense Cholesky factor (statics/src/bodies.rs:286-328).
+ *
+ * Plain C types only: every array is caller-owned; host pointers unless a struct says
+ * otherwise. Every entry point returns an sc_status (SC_OK = 0) and never aborts; a
+ * context is used by one host thread at a time.
+ */
+#ifndef STATICS_CUDA_H
+#define STATICS_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum sc_status {
+    SC_OK = 0,
+    SC_MAXITER = 1,    /* iteration cap reached before the tolerance (reference: silent, bodies.rs:351) */
+    SC_BREAKDOWN = 2,  /* p'Ap <= 0 or a NaN in the CG recurrence */
+    SC_NOT_SPD = 3,    /* the top level's Cholesky met a non-positive pivot (reference: NaN, bodies.rs:308) */
+    SC_BAD_INPUT = 4,  /* sizes, pointers or indices out of range */
+    SC_TIMEOUT = 5,    /* the solve ran past sc_options.timeout_ms */
+    SC_CUDA = 6,       /* a CUDA runtime error; sc_last_error() has the text */
+    SC_NO_DEVICE = 7   /* no usable sm_100 device */
+} sc_status;
+
+enum { SC_CELL_EMPTY = 0, SC_CELL_FREE = 1, SC_CELL_HELD = 2 };
+enum { SC_K_UNIFORM = 0, SC_K_LOGNORMAL = 1 };
+enum { SC_FP64 = 0, SC_MIXED = 1 };
+
+typedef struct sc_options {
+    double tol;        /* stop at ||r|| <= tol ||b||; reference 1e-6 (bodies.rs:432) */
+    int64_t max_iter;  /* CG iteration cap; reference 100000 (bodies.rs:351) */
+    int64_t few;       /* coarsen while a piece has more parts than this; reference 64 (bodies.rs:430) */
+    int32_t precision; /* SC_FP64: the reference's algorithm in FP64. SC_MIXED: FP32 operators
+                          inside FP64 iterative refinement */
+    int32_t sweeps;    /* block-Jacobi sweeps before and after each coarse correction; the
+                          reference does 1 (bodies.rs:386, 397-401) */
+    double inner_tol;  /* SC_MIXED: relative residual each FP32 inner solve stops at */
+    int64_t timeout_ms;/* wall-clock bound of one call; 0 = none */
+} sc_options;
+
+/* The reference's constants (tol 1e-6, FEW 64, cap 100000, one sweep), FP64. */
+void sc_default_options(sc_options* opt);
+
+typedef struct sc_context sc_context;
+
+/* A solver on CUDA device `device`. Replaces nothing in the reference (which keeps no
+ * state between calls); it owns the device buffers reused across calls. */
+sc_status sc_create(int32_t device, sc_context** out);
+void sc_destroy(sc_context* ctx);
+const char* sc_last_error(const sc_context* ctx);
+const char* sc_status_string(sc_status s);
+
+/* What a solve did. */
+#define SC_MAX_LEVELS 24
+typedef struct sc_solve_info {
+    int64_t iterations;      /* CG iterations (SC_MIXED: inner iterations, all refinement steps) */
+    int64_t refinements;     /* SC_MIXED: FP64 true-residual refinement steps */
+    int32_t levels;          /* levels of the hierarchy, level 0 included */
+    int32_t status;          /* sc_status of the solve (batched solves: of this piece) */
+    int64_t parts[SC_MAX_LEVELS];   /* parts per level */
+    int64_t blocks[SC_MAX_LEVELS];  /* stored 6x6 blocks per level (both triangles, diagonal included) */
+    double steps[SC_MAX_LEVELS];    /* smoother step 4/3 / lambda_max per level (bodies.rs:174) */
+    double residual;         /* final relative residual ||b - A x|| / ||b||, recomputed in FP64 */
+    double work;             /* the reference's Work counter: parts + pairs per level apply (bodies.rs:194) */
+    double setup_ms;         /* hierarchy construction, device time */
+    double solve_ms;         /* conjugate gradients, device time */
+    int64_t n_nodes;         /* nodes of the lattice */
+    int64_t n_parts;         /* free nodes: level-0 unknowns / 6 */
+    int64_t peak_bytes;      /* device memory held by the solve at its peak */
+} sc_solve_info;
+
+/* ---------------------------------------------------------------------------
+ * Voxel pieces (the structured fast path).
+ *
+ * A piece is a grid of level-0 cells, flat index ((x*ny)+y)*nz+z (the order
+ * statics/src/lattice.rs:87-102 visits sites). Its lattice is the reference's
+ * `build(0, solids)` (statics/src/lattice.rs:124-163): a node on every face of a free
+ * cell, numbered in first-touch order, held where the other cell is held; 15 beams of
+ * 4 bonds join each free cell's faces; each cell has E = k, G = g_over_e * k, density
+ * rho. Each node's load is its mass times `gravity` (force and no moment).
+ * ------------------------------------------------------------------------- */
+typedef struct sc_grid {
+    int32_t nx, ny, nz;
+    const uint8_t* state; /* SC_CELL_EMPTY / FREE / HELD, nx*ny*nz */
+    const float* k;       /* stiffness per cell, nx*ny*nz */
+    double g_over_e;      /* 0.4 for every reference material (statics/src/model.rs:53-58) */
+    double rho;           /* density; 512 gives a level-0 cell (0.125 m) a mass of 1 */
+    double gravity[3];    /* load per unit mass, e.g. {0, 0, -1} */
+    int32_t on_device;    /* state and k are device pointers */
+} sc_grid;
+
+/* Seeded synthetic piece: value noise of period 8, threshold 0.5, bottom z layer held,
+ * the component joined to it kept; k uniform [0.5, 2] (SC_K_UNIFORM) or lognormal
+ * (mu 0, sigma 0.5) clipped to [0.1, 10] (SC_K_LOGNORMAL). Host memory, no device use.
+ * Replaces nothing in the reference: it makes the benchmark's inputs. */
+sc_status sc_generate_piece(int32_t nx, int32_t ny, int32_t nz, uint64_t seed, int32_t k_dist, uint8_t* state,
+                            float* k);
+
+/* Nodes and free nodes of a piece's lattice (host arithmetic, no device use). */
+sc_status sc_grid_count(const sc_grid* g, int64_t* n_nodes, int64_t* n_parts);
+
+/* Replaces `statics::bodies::motions` (statics/src/bodies.rs:429) for a voxel piece
+ * with every bond alive and no node gone: writes 6 values per node (n_nodes x 6, the
+ * reference's node order; held nodes zero) into `motions`, which holds `capacity`
+ * doubles. `motions_on_device` says whether it is a device pointer. */
+sc_status sc_solve_grid(sc_context* ctx, const sc_grid* g, const sc_options* opt, double* motions,
+                        int64_t capacity, int32_t motions_on_device, sc_solve_info* info);
+
+/* Many pieces at once: each its own hierarchy and its own CG, advanced together by
+ * batched kernels in one CUDA graph per iteration. motions[i] receives piece i's
+ * n_nodes x 6 values (host pointers); infos[i] its info. No counterpart in the
+ * reference, which solves one structure per call. */
+sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, const sc_options* opt,
+                              double* const* motions, sc_solve_info* infos);
+
+/* Compliance C = f.u of a piece and its gradient with respect to each cell's
+ * stiffness: dC/dk_c = -2 U_c / k_c, U_c the strain energy of the cell's 60 bonds
+ * (Bond::energy, statics/src/model.rs:132-136) at the solved motions. dc_dk has nx*ny*nz
+ * entries (zero for cells that are not free). No counterpart in the reference: the
+ * backward of `motions` for compliance. */
+sc_status sc_compliance_grad(sc_context* ctx, const sc_grid* g, const sc_options* opt, double* compliance,
+                             double* dc_dk, double* motions, int64_t capacity, sc_solve_info* info);
+
+/* Level 0's operator on a piece: y = K x over the free nodes (n_parts x 6, part order),
+ * the reference's Level::new + Level::apply (statics/src/bodies.rs:126-206), in FP64
+ * (SC_FP64) or FP32 arithmetic (SC_MIXED). Host arrays. For parity checks. */
+sc_status sc_grid_apply(sc_context* ctx, const sc_grid* g, int32_t precision, const double* x, double* y);
+
+/* After a solve: the body of each part at level `level` (the reference's `up` from
+ * bodies_of, statics/src/bodies.rs:472-496), parts[level] entries; and piece-level
+ * hierarchy sizes. For parity checks. */
+sc_status sc_last_up(sc_context* ctx, int32_t level, int32_t* up, int64_t capacity);
+
+/* ---------------------------------------------------------------------------
+ * General lattices (any `Lattice`: the reference's level 0, or a gathered level).
+ * Structure-of-arrays copy of statics/src/lattice.rs:61-71 and model.rs:92-111.
+ * ------------------------------------------------------------------------- */
+typedef struct sc_lattice {
+    int32_t level;          /* Lattice::level */
+    int64_t n_nodes;
+    int64_t n_bonds;
+    const double* x;        /* node centres, 3 per node */
+    const uint8_t* held;    /* 1 if held */
+    const int64_t* around;  /* the two cells each node lies between, 6 per node (lesser first) */
+    const int64_t* bond_i;  /* bond ends */
+    const int64_t* bond_j;
+    const double* bond_p;   /* 3 per bond */
+    const double* bond_n;   /* 3 per bond */
+    const double* bond_a;
+    const double* bond_d;
+    const double* bond_e;   /* the bond's material's E */
+    const double* bond_g;   /* the bond's material's G */
+} sc_lattice;
+
+/* Replaces `statics::bodies::motions` (statics/src/bodies.rs:429) for any lattice:
+ * alive (n_bonds, may be NULL: all alive), gone (n_nodes, may be NULL: none gone),
+ * loads (6 per node), motions out (6 per node; held and gone nodes zero). */
+sc_status sc_motions(sc_context* ctx, const sc_lattice* lattice, const uint8_t* alive, const uint8_t* gone,
+                     const double* loads, const sc_options* opt, double* motions, sc_solve_info* info);
+
+/* ---------------------------------------------------------------------------
+ * Measurement. No counterpart in the reference (which times whole calls with
+ * Instant, statics/examples/statics.rs:135-140, 373-391).
+ * ------------------------------------------------------------------------- */
+enum {
+    SC_FAM_STENCIL64 = 0, /* level-0 matrix-free stencil, FP64 */
+    SC_FAM_STENCIL32 = 1, /* the same, FP32 */
+    SC_FAM_SPMV64 = 2,    /* block-sparse operator products, FP64 */
+    SC_FAM_SPMV32 = 3,
+    SC_FAM_TRANSFER64 = 4,/* restriction and prolongation */
+    SC_FAM_TRANSFER32 = 5,
+    SC_FAM_SMOOTH64 = 6,  /* block-Jacobi steps */
+    SC_FAM_SMOOTH32 = 7,
+    SC_FAM_TOP = 8,       /* dense top-level solves */
+    SC_FAM_COUNT = 9
+};
+/* Bracket every launch of the families in `mask` (bit f = family f) with CUDA events
+ * on the context's stream, and reset the tallies. mask 0 turns it off. */
+sc_status sc_profile(sc_context* ctx, uint32_t mask);
+/* Tallies since sc_profile: launches, summed device milliseconds and algorithmic bytes
+ * (what the kernels must read and write: vectors, blocks, cell table). */
+sc_status sc_profile_read(sc_context* ctx, int32_t family, int64_t* launches, double* ms, double* bytes);
+/* Kernels this library has launched in this process. */
+int64_t sc_launches(void);
+/* The CUDA stream (cudaStream_t) the context launches on. */
+sc_status sc_context_stream(sc_context* ctx, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STATICS_CUDA_H */

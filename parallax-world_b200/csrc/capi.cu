@@ -1,0 +1,557 @@
+// The C ABI (include/statics_cuda.h): validation, one solve per call, statuses instead
+// of exceptions, results scattered back to the reference's node order.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "kernels.cuh"
+#include "template_gen.cuh"
+
+struct sc_context {
+    sc::Context c;
+};
+
+namespace sc {
+
+std::atomic<int64_t> g_launches{0};
+
+cudaEvent_t Profiler::get() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    SC_CK(cudaEventCreate(&e));
+    return e;
+}
+
+void Profiler::flush() {
+    if (pending.empty()) return;
+    SC_CK(cudaEventSynchronize(pending.back().b));
+    for (auto& p : pending) {
+        float t = 0;
+        SC_CK(cudaEventElapsedTime(&t, p.a, p.b));
+        launches[p.fam] += 1;
+        ms[p.fam] += t;
+        bytes[p.fam] += p.bytes;
+        pool.push_back(p.a);
+        pool.push_back(p.b);
+    }
+    pending.clear();
+}
+
+void Profiler::reset() {
+    flush();
+    for (int f = 0; f < SC_FAM_COUNT; f++) {
+        launches[f] = 0;
+        ms[f] = 0;
+        bytes[f] = 0;
+    }
+}
+
+Profiler::~Profiler() {
+    for (auto& p : pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : pool) cudaEventDestroy(e);
+}
+
+ProfScope::ProfScope(Context& ctx, int family, double algorithmic_bytes) {
+    if (!(ctx.prof.mask & (1u << family))) return;
+    c = &ctx;
+    fam = family;
+    bytes = algorithmic_bytes;
+    a = ctx.prof.get();
+    SC_CK(cudaEventRecord(a, ctx.stream));
+}
+
+ProfScope::~ProfScope() {
+    if (!c) return;
+    cudaEvent_t b = c->prof.get();
+    cudaEventRecord(b, c->stream);
+    c->prof.pending.push_back({fam, a, b, bytes});
+    if (c->prof.pending.size() > 4096) c->prof.flush();
+}
+
+void* Context::cub_scratch(size_t bytes) {
+    if (bytes > cub_bytes) {
+        if (cub_tmp) cudaFreeAsync(cub_tmp, stream);
+        size_t want = std::max(bytes, cub_bytes * 2);
+        SC_CK(cudaMallocAsync(&cub_tmp, want, stream));
+        cub_bytes = want;
+    }
+    return cub_tmp;
+}
+
+Context::~Context() {
+    last.reset();
+    partial.release();
+    scal.release();
+    if (cub_tmp) cudaFreeAsync(cub_tmp, stream);
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+}
+
+namespace {
+
+__global__ void k_scatter(int64_t n, const int32_t* __restrict__ piece, const int64_t* __restrict__ node_start,
+                          const int32_t* __restrict__ part_node, const double* __restrict__ x, double* __restrict__ out) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int64_t v = node_start[piece[k]] + part_node[k];
+    for (int q = 0; q < 6; q++) out[6 * v + q] = x[6 * k + q];
+}
+
+// dC/dk = -2 U / k per free cell, written at the cell's flat index
+__global__ void k_grad(int64_t nc, const int4* __restrict__ cell, const int64_t* __restrict__ cell_flat,
+                       const double* __restrict__ energy, double* __restrict__ grad) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    double k = (double)__int_as_float(cell[2 * c + 1].z);
+    grad[cell_flat[c]] = -2.0 * energy[c] / k;
+}
+
+template <class F>
+sc_status guarded(sc_context* ctx, F&& f) {
+    if (!ctx) return SC_BAD_INPUT;
+    try {
+        SC_CK(cudaSetDevice(ctx->c.device));
+        f();
+        ctx->c.last_error.clear();
+        return SC_OK;
+    } catch (const Error& e) {
+        ctx->c.last_error = e.what();
+        if (e.status == SC_CUDA) cudaGetLastError();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        ctx->c.last_error = "host allocation failed";
+        return SC_CUDA;
+    } catch (const std::exception& e) {
+        ctx->c.last_error = e.what();
+        return SC_CUDA;
+    }
+}
+
+void check_grid(const sc_grid& g) {
+    require(g.nx > 0 && g.ny > 0 && g.nz > 0, SC_BAD_INPUT, "grid dimensions must be positive");
+    require((int64_t)g.nx * g.ny * g.nz < (int64_t)1 << 31, SC_BAD_INPUT, "grid too large");
+    require(g.state && g.k, SC_BAD_INPUT, "grid state and k are required");
+    require(std::fabs(g.g_over_e - TPL_G_OVER_E) < 1e-12, SC_BAD_INPUT,
+            "voxel pieces take G/E = 0.4 (every reference material's); use sc_motions for others");
+    require(g.rho > 0 && std::isfinite(g.rho), SC_BAD_INPUT, "rho must be positive");
+}
+
+void check_options(const sc_options& o) {
+    require(o.tol >= 0 && std::isfinite(o.tol), SC_BAD_INPUT, "tol must be finite and non-negative");
+    require(o.max_iter >= 0, SC_BAD_INPUT, "max_iter must be non-negative");
+    require(o.few >= 1, SC_BAD_INPUT, "few must be at least 1");
+    require(o.precision == SC_FP64 || o.precision == SC_MIXED, SC_BAD_INPUT, "unknown precision");
+}
+
+// The reference's Work for a solve of one piece: parts + pairs per level apply
+// (bodies.rs:194): the CG's level-0 apply each iteration, and two applies per level
+// above the top in each V-cycle (one before the loop, one per iteration).
+double work_of(const Batch& b, int piece, int64_t iters) {
+    double w = 0;
+    const Level& L0 = b.levels[0];
+    auto parts = [&](const Level& L) { return (double)(L.pstart[piece + 1] - L.pstart[piece]); };
+    (void)L0;
+    int nl = b.piece_levels[piece];
+    // pairs of a piece's level: (blocks - parts) / 2 over its rows
+    auto pairs = [&](int l) -> double {
+        const Level& L = b.levels[l];
+        if (b.npieces == 1) return (double)(L.nnzb - L.n) / 2.0;
+        return 0.0;  // batched pieces: not tracked
+    };
+    w += (double)iters * (parts(b.levels[0]) + pairs(0));
+    for (int l = 0; l + 1 < nl; l++) w += (double)(iters + 1) * 2.0 * (parts(b.levels[l]) + pairs(l));
+    return w;
+}
+
+void fill_info(const Batch& b, int piece, const SolveStats& st, sc_solve_info* info, double solve_ms, int64_t peak) {
+    if (!info) return;
+    std::memset(info, 0, sizeof(*info));
+    info->iterations = st.iterations.empty() ? 0 : st.iterations[piece];
+    info->refinements = st.refinements.empty() ? 0 : st.refinements[piece];
+    int nl = b.piece_levels.empty() ? 1 : b.piece_levels[piece];
+    info->levels = nl;
+    for (int l = 0; l < nl && l < SC_MAX_LEVELS; l++) {
+        const Level& L = b.levels[l];
+        info->parts[l] = L.pstart[piece + 1] - L.pstart[piece];
+        info->blocks[l] = b.npieces == 1 ? L.nnzb : 0;
+    }
+    info->residual = st.residual.empty() ? 0 : st.residual[piece];
+    info->work = work_of(b, piece, info->iterations);
+    info->setup_ms = b.setup_ms;
+    info->solve_ms = solve_ms;
+    info->n_nodes = b.node_count[piece];
+    info->n_parts = b.levels[0].pstart[piece + 1] - b.levels[0].pstart[piece];
+    info->peak_bytes = peak;
+    info->status = b.piece_status.empty() ? 0 : b.piece_status[piece];
+}
+
+void read_steps(Context& ctx, const Batch& b, int piece, sc_solve_info* info) {
+    if (!info) return;
+    for (int l = 0; l < info->levels && l < SC_MAX_LEVELS; l++) {
+        double s = 0;
+        SC_CK(cudaMemcpyAsync(&s, b.levels[l].step.get() + piece, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+        SC_CK(cudaStreamSynchronize(ctx.stream));
+        info->steps[l] = s;
+    }
+}
+
+// Solves a batch already at level 0; returns per-piece statuses.
+sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st, double& solve_ms) {
+    build_hierarchy(ctx, b, opt);
+    auto t0 = std::chrono::steady_clock::now();
+    if (opt.precision == SC_MIXED)
+        pcg_mixed(ctx, b, opt, x, st);
+    else
+        pcg_fp64(ctx, b, opt, x, st);
+    SC_CK(cudaStreamSynchronize(ctx.stream));
+    solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    b.piece_status = b.status_d.to_host();
+    int worst = 0;
+    for (int s : b.piece_status) worst = std::max(worst, s);
+    return (sc_status)worst;
+}
+
+}  // namespace
+}  // namespace sc
+
+using namespace sc;
+
+extern "C" {
+
+void sc_default_options(sc_options* o) {
+    if (!o) return;
+    o->tol = 1e-6;
+    o->max_iter = 100000;
+    o->few = 64;
+    o->precision = SC_FP64;
+    o->sweeps = 1;
+    o->inner_tol = 1e-4;
+    o->timeout_ms = 0;
+}
+
+const char* sc_status_string(sc_status s) {
+    switch (s) {
+        case SC_OK: return "ok";
+        case SC_MAXITER: return "iteration cap reached";
+        case SC_BREAKDOWN: return "conjugate gradients broke down (p'Ap <= 0 or NaN)";
+        case SC_NOT_SPD: return "top level not positive definite";
+        case SC_BAD_INPUT: return "bad input";
+        case SC_TIMEOUT: return "time limit reached";
+        case SC_CUDA: return "CUDA error";
+        case SC_NO_DEVICE: return "no sm_100 device";
+    }
+    return "unknown status";
+}
+
+sc_status sc_create(int32_t device, sc_context** out) {
+    if (!out) return SC_BAD_INPUT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return SC_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return SC_NO_DEVICE;
+    auto* ctx = new sc_context;
+    ctx->c.device = device;
+    sc_status s = guarded(ctx, [&] {
+        SC_CK(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+        cudaMemPool_t pool;
+        SC_CK(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t thr = UINT64_MAX;
+        SC_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    });
+    if (s != SC_OK) {
+        delete ctx;
+        return s;
+    }
+    *out = ctx;
+    return SC_OK;
+}
+
+void sc_destroy(sc_context* ctx) { delete ctx; }
+
+const char* sc_last_error(const sc_context* ctx) { return ctx ? ctx->c.last_error.c_str() : "no context"; }
+
+sc_status sc_grid_count(const sc_grid* g, int64_t* n_nodes, int64_t* n_parts) {
+    if (!g || !n_nodes || !n_parts || g->on_device) return SC_BAD_INPUT;
+    if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || !g->state) return SC_BAD_INPUT;
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    auto st = [&](int x, int y, int z) -> int {
+        if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return SC_CELL_EMPTY;
+        return g->state[((int64_t)x * ny + y) * nz + z];
+    };
+    int64_t nodes = 0, held = 0;
+    for (int x = 0; x < nx; x++)
+        for (int y = 0; y < ny; y++)
+            for (int z = 0; z < nz; z++) {
+                if (st(x, y, z) != SC_CELL_FREE) continue;
+                int o[6][3] = {{x - 1, y, z}, {x + 1, y, z}, {x, y - 1, z}, {x, y + 1, z}, {x, y, z - 1}, {x, y, z + 1}};
+                for (int s = 0; s < 6; s++) {
+                    int other = st(o[s][0], o[s][1], o[s][2]);
+                    bool is_new = (s & 1) || other != SC_CELL_FREE;
+                    if (!is_new) continue;
+                    nodes++;
+                    if (other == SC_CELL_HELD) held++;
+                }
+            }
+    *n_nodes = nodes;
+    *n_parts = nodes - held;
+    return SC_OK;
+}
+
+sc_status sc_solve_grid(sc_context* ctx, const sc_grid* g, const sc_options* opt, double* motions, int64_t capacity,
+                        int32_t motions_on_device, sc_solve_info* info) {
+    if (!g || !opt || !motions) return SC_BAD_INPUT;
+    sc_status solve_status = SC_OK;
+    sc_status s = guarded(ctx, [&] {
+        Context& c = ctx->c;
+        check_grid(*g);
+        check_options(*opt);
+        auto b = std::make_unique<Batch>();
+        c.mem.peak = c.mem.now;
+        grid_level0(c, *b, {*g}, true);
+        int64_t nodes = b->node_count[0];
+        require(capacity >= 6 * nodes, SC_BAD_INPUT, "motions buffer holds fewer than 6 * n_nodes values");
+        DBuf<double> x;
+        SolveStats st;
+        double solve_ms = 0;
+        solve_status = solve_batch(c, *b, *opt, x, st, solve_ms);
+        DBuf<double> out;
+        double* dst = motions;
+        if (!motions_on_device) {
+            out.alloc(6 * nodes, c.stream, &c.mem);
+            dst = out.get();
+        }
+        SC_CK(cudaMemsetAsync(dst, 0, 6 * nodes * sizeof(double), c.stream));
+        const Level& L = b->levels[0];
+        k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(),
+                                                             b->part_node.get(), x.get(), dst);
+        SC_LAUNCH_CK();
+        if (!motions_on_device) out.download(motions, 6 * nodes);
+        SC_CK(cudaStreamSynchronize(c.stream));
+        fill_info(*b, 0, st, info, solve_ms, c.mem.peak);
+        read_steps(c, *b, 0, info);
+        c.last = std::move(b);
+    });
+    return s != SC_OK ? s : solve_status;
+}
+
+sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, const sc_options* opt,
+                              double* const* motions, sc_solve_info* infos) {
+    if (n <= 0 || !grids || !opt || !motions) return SC_BAD_INPUT;
+    sc_status solve_status = SC_OK;
+    sc_status s = guarded(ctx, [&] {
+        Context& c = ctx->c;
+        check_options(*opt);
+        std::vector<sc_grid> gs(grids, grids + n);
+        for (auto& g : gs) check_grid(g);
+        auto b = std::make_unique<Batch>();
+        c.mem.peak = c.mem.now;
+        grid_level0(c, *b, gs, true);
+        DBuf<double> x;
+        SolveStats st;
+        double solve_ms = 0;
+        solve_status = solve_batch(c, *b, *opt, x, st, solve_ms);
+        int64_t total = 0;
+        std::vector<int64_t> start(n + 1, 0);
+        for (int p = 0; p < n; p++) start[p + 1] = start[p] + b->node_count[p];
+        total = start[n];
+        DBuf<double> out;
+        out.alloc(6 * std::max<int64_t>(total, 1), c.stream, &c.mem);
+        out.zero();
+        const Level& L = b->levels[0];
+        k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(),
+                                                             b->part_node.get(), x.get(), out.get());
+        SC_LAUNCH_CK();
+        for (int p = 0; p < n; p++)
+            if (motions[p])
+                SC_CK(cudaMemcpyAsync(motions[p], out.get() + 6 * start[p], 6 * b->node_count[p] * sizeof(double),
+                                      cudaMemcpyDeviceToHost, c.stream));
+        SC_CK(cudaStreamSynchronize(c.stream));
+        if (infos)
+            for (int p = 0; p < n; p++) {
+                fill_info(*b, p, st, infos + p, solve_ms, c.mem.peak);
+                read_steps(c, *b, p, infos + p);
+            }
+        c.last = std::move(b);
+    });
+    return s != SC_OK ? s : solve_status;
+}
+
+sc_status sc_compliance_grad(sc_context* ctx, const sc_grid* g, const sc_options* opt, double* compliance,
+                             double* dc_dk, double* motions, int64_t capacity, sc_solve_info* info) {
+    if (!g || !opt || !dc_dk) return SC_BAD_INPUT;
+    sc_status solve_status = SC_OK;
+    sc_status s = guarded(ctx, [&] {
+        Context& c = ctx->c;
+        check_grid(*g);
+        check_options(*opt);
+        require(!g->on_device, SC_BAD_INPUT, "sc_compliance_grad takes host grids");
+        auto b = std::make_unique<Batch>();
+        c.mem.peak = c.mem.now;
+        grid_level0(c, *b, {*g}, true);
+        int64_t nodes = b->node_count[0];
+        require(!motions || capacity >= 6 * nodes, SC_BAD_INPUT, "motions buffer too small");
+        DBuf<double> x;
+        SolveStats st;
+        double solve_ms = 0;
+        solve_status = solve_batch(c, *b, *opt, x, st, solve_ms);
+        const Level& L = b->levels[0];
+        // C = f . u (FP64, deterministic per piece)
+        DBuf<double> cc;
+        cc.alloc(1, c.stream, &c.mem);
+        seg_dot(c, L, b->loads.get(), x.get(), cc.get());
+        double C = 0;
+        cc.download(&C, 1);
+        // the fused per-cell strain-energy gather, then dC/dk = -2 U / k
+        const Grid0& G = b->grid;
+        DBuf<double> energy, grad;
+        energy.alloc(std::max<int64_t>(G.ncells, 1), c.stream, &c.mem);
+        grid_cell_energy(c, *b, x.get(), energy.get());
+        int64_t ncell = (int64_t)g->nx * g->ny * g->nz;
+        grad.alloc(ncell, c.stream, &c.mem);
+        grad.zero();
+        k_grad<<<grid_for(G.ncells, 256), 256, 0, c.stream>>>(G.ncells, G.cell.get(), G.cell_flat.get(), energy.get(),
+                                                               grad.get());
+        SC_LAUNCH_CK();
+        grad.download(dc_dk, ncell);
+        if (motions) {
+            DBuf<double> out;
+            out.alloc(6 * nodes, c.stream, &c.mem);
+            out.zero();
+            k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(),
+                                                                 b->part_node.get(), x.get(), out.get());
+            SC_LAUNCH_CK();
+            out.download(motions, 6 * nodes);
+        }
+        SC_CK(cudaStreamSynchronize(c.stream));
+        if (compliance) *compliance = C;
+        fill_info(*b, 0, st, info, solve_ms, c.mem.peak);
+        read_steps(c, *b, 0, info);
+        c.last = std::move(b);
+    });
+    return s != SC_OK ? s : solve_status;
+}
+
+sc_status sc_grid_apply(sc_context* ctx, const sc_grid* g, int32_t precision, const double* xin, double* yout) {
+    if (!g || !xin || !yout) return SC_BAD_INPUT;
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        check_grid(*g);
+        Batch b;
+        grid_level0(c, b, {*g}, false);
+        const Level& L = b.levels[0];
+        int64_t n6 = 6 * L.n;
+        DBuf<double> x, y;
+        x.alloc(n6, c.stream, &c.mem);
+        y.alloc(n6, c.stream, &c.mem);
+        x.upload(xin, n6);
+        if (precision == SC_MIXED) {
+            DBuf<float> xf, yf;
+            to_float(c, x, xf);
+            yf.alloc(n6, c.stream, &c.mem);
+            stencil_apply<float>(c, b, xf.get(), yf.get(), nullptr, nullptr);
+            std::vector<float> h(n6);
+            yf.download(h.data(), n6);
+            SC_CK(cudaStreamSynchronize(c.stream));
+            for (int64_t i = 0; i < n6; i++) yout[i] = h[i];
+        } else {
+            stencil_apply<double>(c, b, x.get(), y.get(), nullptr, nullptr);
+            y.download(yout, n6);
+            SC_CK(cudaStreamSynchronize(c.stream));
+        }
+    });
+}
+
+sc_status sc_last_up(sc_context* ctx, int32_t level, int32_t* up, int64_t capacity) {
+    if (!up) return SC_BAD_INPUT;
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        require(c.last != nullptr, SC_BAD_INPUT, "no solve yet");
+        require(level >= 0 && level + 1 < (int)c.last->levels.size(), SC_BAD_INPUT, "no such coarsening");
+        const Level& L = c.last->levels[level];
+        require(capacity >= L.n, SC_BAD_INPUT, "capacity below the level's parts");
+        L.up.download(up, L.n);
+        SC_CK(cudaStreamSynchronize(c.stream));
+    });
+}
+
+sc_status sc_motions(sc_context* ctx, const sc_lattice* lat, const uint8_t* alive, const uint8_t* gone,
+                     const double* loads, const sc_options* opt, double* motions, sc_solve_info* info) {
+    if (!lat || !loads || !opt || !motions) return SC_BAD_INPUT;
+    sc_status solve_status = SC_OK;
+    sc_status s = guarded(ctx, [&] {
+        Context& c = ctx->c;
+        check_options(*opt);
+        require(lat->n_nodes > 0 && lat->n_bonds >= 0, SC_BAD_INPUT, "empty lattice");
+        require(lat->x && lat->held && lat->around, SC_BAD_INPUT, "node arrays are required");
+        require(lat->n_bonds == 0 || (lat->bond_i && lat->bond_j && lat->bond_p && lat->bond_n && lat->bond_a &&
+                                      lat->bond_d && lat->bond_e && lat->bond_g),
+                SC_BAD_INPUT, "bond arrays are required");
+        for (int64_t b = 0; b < lat->n_bonds; b++)
+            require(lat->bond_i[b] >= 0 && lat->bond_i[b] < lat->n_nodes && lat->bond_j[b] >= 0 &&
+                        lat->bond_j[b] < lat->n_nodes,
+                    SC_BAD_INPUT, "bond end out of range");
+        auto b = std::make_unique<Batch>();
+        c.mem.peak = c.mem.now;
+        lattice_level0(c, *b, *lat, alive, gone, loads);
+        DBuf<double> x;
+        SolveStats st;
+        double solve_ms = 0;
+        solve_status = solve_batch(c, *b, *opt, x, st, solve_ms);
+        int64_t nodes = lat->n_nodes;
+        DBuf<double> out;
+        out.alloc(6 * nodes, c.stream, &c.mem);
+        out.zero();
+        const Level& L = b->levels[0];
+        k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(),
+                                                             b->part_node.get(), x.get(), out.get());
+        SC_LAUNCH_CK();
+        out.download(motions, 6 * nodes);
+        SC_CK(cudaStreamSynchronize(c.stream));
+        fill_info(*b, 0, st, info, solve_ms, c.mem.peak);
+        read_steps(c, *b, 0, info);
+        c.last = std::move(b);
+    });
+    return s != SC_OK ? s : solve_status;
+}
+
+sc_status sc_profile(sc_context* ctx, uint32_t mask) {
+    return guarded(ctx, [&] {
+        ctx->c.prof.reset();
+        ctx->c.prof.mask = mask;
+    });
+}
+
+sc_status sc_profile_read(sc_context* ctx, int32_t family, int64_t* launches, double* ms, double* bytes) {
+    if (family < 0 || family >= SC_FAM_COUNT) return SC_BAD_INPUT;
+    return guarded(ctx, [&] {
+        ctx->c.prof.flush();
+        if (launches) *launches = ctx->c.prof.launches[family];
+        if (ms) *ms = ctx->c.prof.ms[family];
+        if (bytes) *bytes = ctx->c.prof.bytes[family];
+    });
+}
+
+int64_t sc_launches(void) { return g_launches.load(); }
+
+sc_status sc_context_stream(sc_context* ctx, void** stream) {
+    if (!ctx || !stream) return SC_BAD_INPUT;
+    *stream = (void*)ctx->c.stream;
+    return SC_OK;
+}
+
+}  // extern "C"

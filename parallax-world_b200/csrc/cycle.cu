@@ -1,0 +1,568 @@
+// The solve: conjugate gradients on level 0 (statics/src/bodies.rs:338-373),
+// preconditioned by one V-cycle (bodies.rs:377-403), for every piece of a batch at
+// once with per-piece scalars; and the mixed-precision variant, FP32 operators inside
+// FP64 iterative refinement.
+#include <chrono>
+
+#include "kernels.cuh"
+
+namespace sc {
+
+template <class T>
+static const T* VAL(const Level& L);
+template <>
+const double* VAL<double>(const Level& L) { return L.val.get(); }
+template <>
+const float* VAL<float>(const Level& L) { return L.val32.get(); }
+template <class T>
+static const T* INV(const Level& L);
+template <>
+const double* INV<double>(const Level& L) { return L.inv.get(); }
+template <>
+const float* INV<float>(const Level& L) { return L.inv32.get(); }
+template <class T>
+static const T* PVAL(const Level& L);
+template <>
+const double* PVAL<double>(const Level& L) { return L.pval.get(); }
+template <>
+const float* PVAL<float>(const Level& L) { return L.pval32.get(); }
+template <class T>
+static DBuf<T>& VR(Level& L);
+template <>
+DBuf<double>& VR<double>(Level& L) { return L.r; }
+template <>
+DBuf<float>& VR<float>(Level& L) { return L.r32; }
+template <class T>
+static DBuf<T>& VX(Level& L);
+template <>
+DBuf<double>& VX<double>(Level& L) { return L.x; }
+template <>
+DBuf<float>& VX<float>(Level& L) { return L.x32; }
+template <class T>
+static DBuf<T>& VL(Level& L);
+template <>
+DBuf<double>& VL<double>(Level& L) { return L.left; }
+template <>
+DBuf<float>& VL<float>(Level& L) { return L.left32; }
+template <class T>
+static DBuf<T>& VZ(Level& L);
+template <>
+DBuf<double>& VZ<double>(Level& L) { return L.z; }
+template <>
+DBuf<float>& VZ<float>(Level& L) { return L.z32; }
+
+template <class T>
+void level_apply(Context& ctx, const Batch& b, int l, const T* x, T* y) {
+    const Level& L = b.levels[l];
+    if (l == 0 && L.matrix_free)
+        stencil_apply<T>(ctx, b, x, y, nullptr, nullptr);
+    else
+        spmv<T>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, nullptr, y, nullptr, nullptr,
+                L.piece.get(), nullptr, nullptr);
+}
+template void level_apply<double>(Context&, const Batch&, int, const double*, double*);
+template void level_apply<float>(Context&, const Batch&, int, const float*, float*);
+
+template <class T>
+static void ensure(Context& ctx, DBuf<T>& v, int64_t n) {
+    if ((int64_t)v.size() < n) v.alloc(std::max<int64_t>(n, 1), ctx.stream, &ctx.mem);
+}
+
+template <class T>
+static void alloc_cycle(Context& ctx, Batch& b) {
+    for (size_t l = 0; l < b.levels.size(); l++) {
+        Level& L = b.levels[l];
+        int64_t n6 = 6 * L.n;
+        ensure(ctx, VX<T>(L), n6);
+        ensure(ctx, VL<T>(L), n6);
+        if (l > 0) {
+            ensure(ctx, VR<T>(L), n6);
+            ensure(ctx, VZ<T>(L), n6);
+        }
+    }
+}
+
+template <class T>
+constexpr int fam_of(int f64) {
+    return sizeof(T) == 8 ? f64 : f64 + 1;
+}
+// algorithmic bytes of a block-sparse product: blocks, x once, y (and r) once
+template <class T>
+static double spmv_bytes(const Level& L, int vec_passes) {
+    return (double)sizeof(T) * (36.0 * (double)L.nnzb + 6.0 * (double)L.n * vec_passes);
+}
+template <class T>
+static double transfer_bytes(const Level& L, const Level& C) {
+    return (double)sizeof(T) * (36.0 * (double)L.pnnz + 6.0 * (double)L.n + 6.0 * (double)C.n);
+}
+
+// One V-cycle from level l: z = M r (bodies.rs:377-403). Pieces whose top is level l are
+// solved directly there; the others smooth, hand the residual up, take the correction
+// back and smooth again.
+template <class T>
+static void cycle(Context& ctx, Batch& b, int l, const T* r, T* z, const int32_t* done) {
+    Level& L = b.levels[l];
+    bool deepest = l + 1 == (int)b.levels.size();
+    if (!deepest) {
+        const int32_t* skip = L.top_of_part.get();
+        T* x = VX<T>(L).get();
+        T* left = VL<T>(L).get();
+        bool mf = l == 0 && L.matrix_free;
+        double vb = (double)sizeof(T) * 6.0 * (double)L.n;
+        // x = step D^-1 r (bodies.rs:386)
+        {
+            ProfScope ps(ctx, fam_of<T>(SC_FAM_SMOOTH64), 2 * vb + 36.0 * sizeof(T) * L.n);
+            jacobi<T>(ctx, L.n, INV<T>(L), r, x, L.step.get(), L.piece.get(), skip, done);
+        }
+        // left = r - K x (bodies.rs:387)
+        if (mf) {
+            stencil_residual<T>(ctx, b, x, r, left, skip, done);
+        } else {
+            ProfScope ps(ctx, fam_of<T>(SC_FAM_SPMV64), spmv_bytes<T>(L, 3));
+            spmv<T>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, r, left, nullptr, nullptr,
+                    L.piece.get(), skip, done);
+        }
+        Level& C = b.levels[l + 1];
+        // coarse = P' left (bodies.rs:388-390)
+        {
+            ProfScope ps(ctx, fam_of<T>(SC_FAM_TRANSFER64), transfer_bytes<T>(L, C));
+            restrict_t<T>(ctx, C.n, L.tptr.get(), L.tent.get(), L.trow.get(), PVAL<T>(L), left, VR<T>(C).get(),
+                          C.piece.get(), done);
+        }
+        cycle<T>(ctx, b, l + 1, VR<T>(C).get(), VZ<T>(C).get(), done);
+        // x += P y (bodies.rs:392-395)
+        {
+            ProfScope ps(ctx, fam_of<T>(SC_FAM_TRANSFER64), transfer_bytes<T>(L, C) + vb);
+            spmv<T>(ctx, SPMV_ADD, L.n, L.prow.get(), L.pcol.get(), PVAL<T>(L), VZ<T>(C).get(), nullptr, x, nullptr,
+                    nullptr, L.piece.get(), skip, done);
+        }
+        // z = x + step D^-1 (r - K x) (bodies.rs:396-401)
+        if (mf) {
+            stencil_residual<T>(ctx, b, x, r, left, skip, done);
+            ProfScope ps(ctx, fam_of<T>(SC_FAM_SMOOTH64), 3 * vb + 36.0 * sizeof(T) * L.n);
+            jacobi_add<T>(ctx, L.n, INV<T>(L), left, x, z, L.step.get(), L.piece.get(), skip, done);
+        } else {
+            ProfScope ps(ctx, fam_of<T>(SC_FAM_SPMV64), spmv_bytes<T>(L, 3) + vb + 36.0 * sizeof(T) * L.n);
+            spmv<T>(ctx, SPMV_RES_SMOOTH, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, r, z, INV<T>(L),
+                    L.step.get(), L.piece.get(), skip, done);
+        }
+    }
+    if (!L.top_h.empty()) {
+        ProfScope ps(ctx, SC_FAM_TOP, 0.0);
+        top_solve<T>(ctx, L, r, z, done);
+    }
+}
+
+// ---- per-piece CG scalars and chunked vector updates ---------------------------------
+namespace {
+
+struct CgScalars {
+    double* bb;     // |b|^2
+    double* goal;   // tol |b|
+    double* rz;
+    double* rr;
+    double* pap;
+    double* next;
+    double* alpha;
+    int32_t* done;
+    int64_t* iters;
+    int32_t* status;
+};
+
+__global__ void k_cg_init(int np, double tol, CgScalars s, const int32_t* __restrict__ start_done) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    s.goal[p] = tol * sqrt(s.bb[p]);
+    s.done[p] = start_done ? start_done[p] : 0;
+    s.iters[p] = 0;
+}
+
+// top of an iteration (bodies.rs:352): stop when |r| <= goal; NaN stops with BREAKDOWN
+__global__ void k_cg_check(int np, int64_t max_iter, CgScalars s, int32_t* ndone) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    if (!s.done[p]) {
+        double nr = sqrt(s.rr[p]);
+        if (nr <= s.goal[p]) {
+            s.done[p] = 1;
+        } else if (!(nr == nr) || !(s.rz[p] == s.rz[p])) {
+            s.done[p] = 1;
+            atomicMax(s.status + p, (int)SC_BREAKDOWN);
+        } else if (s.iters[p] >= max_iter) {
+            s.done[p] = 1;
+            atomicMax(s.status + p, (int)SC_MAXITER);
+        }
+    }
+    if (s.done[p]) atomicAdd(ndone, 1);
+}
+
+__global__ void k_cg_alpha(int np, CgScalars s) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np || s.done[p]) return;
+    double pap = s.pap[p];
+    if (!(pap > 0.0)) {
+        s.done[p] = 1;
+        atomicMax(s.status + p, (int)SC_BREAKDOWN);
+        return;
+    }
+    s.alpha[p] = s.rz[p] / pap;  // bodies.rs:356
+}
+
+// beta = next / rz; rz = next (bodies.rs:366-370); counts the iteration
+__global__ void k_cg_beta(int np, CgScalars s, double* beta) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np || s.done[p]) return;
+    beta[p] = s.next[p] / s.rz[p];
+    s.rz[p] = s.next[p];
+    s.iters[p] += 1;
+}
+
+// x += alpha p; r -= alpha Ap (bodies.rs:357-362), one block per chunk
+template <class V, class S>
+__global__ void __launch_bounds__(256) k_axpy2(const int64_t* __restrict__ chunk_lo, const int32_t* __restrict__ cpiece,
+                                               const int32_t* __restrict__ done, const double* __restrict__ alpha,
+                                               S* __restrict__ x, const V* __restrict__ p, V* __restrict__ r,
+                                               const V* __restrict__ ap) {
+    int c = blockIdx.x;
+    int pc = cpiece[c];
+    if (done[pc]) return;
+    double a = alpha[pc];
+    int64_t lo = 6 * chunk_lo[c], hi = 6 * chunk_lo[c + 1];
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        x[i] += (S)(a * (double)p[i]);
+        r[i] = (V)((double)r[i] - a * (double)ap[i]);
+    }
+}
+
+// p = z + beta p (bodies.rs:365-369)
+template <class V>
+__global__ void __launch_bounds__(256) k_pupdate(const int64_t* __restrict__ chunk_lo, const int32_t* __restrict__ cpiece,
+                                                 const int32_t* __restrict__ done, const double* __restrict__ beta,
+                                                 V* __restrict__ p, const V* __restrict__ z) {
+    int c = blockIdx.x;
+    int pc = cpiece[c];
+    if (done[pc]) return;
+    double bt = beta[pc];
+    int64_t lo = 6 * chunk_lo[c], hi = 6 * chunk_lo[c + 1];
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) p[i] = (V)((double)z[i] + bt * (double)p[i]);
+}
+
+// two dots in one pass: out_a = a.b, out_c = a.a
+template <class T>
+__global__ void __launch_bounds__(256) k_chunk_dot2(const int64_t* __restrict__ chunk_lo, const int32_t* __restrict__ cpiece,
+                                                    const int32_t* __restrict__ done, const T* __restrict__ a,
+                                                    const T* __restrict__ b, double* __restrict__ pa,
+                                                    double* __restrict__ pb) {
+    int c = blockIdx.x;
+    __shared__ double r1[256], r2[256];
+    double s1 = 0.0, s2 = 0.0;
+    if (!done || !done[cpiece[c]]) {
+        int64_t lo = 6 * chunk_lo[c], hi = 6 * chunk_lo[c + 1];
+        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            double av = (double)a[i];
+            s1 = fma(av, (double)b[i], s1);
+            s2 = fma(av, av, s2);
+        }
+    }
+    r1[threadIdx.x] = s1;
+    r2[threadIdx.x] = s2;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            r1[threadIdx.x] += r1[threadIdx.x + w];
+            r2[threadIdx.x] += r2[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        pa[c] = r1[0];
+        pb[c] = r2[0];
+    }
+}
+
+__global__ void k_piece_sum2(int np, const int64_t* __restrict__ piece_chunk, const double* __restrict__ pa,
+                             const double* __restrict__ pb, const int32_t* __restrict__ done, double* __restrict__ oa,
+                             double* __restrict__ ob) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    if (done && done[p]) return;
+    double s1 = 0.0, s2 = 0.0;
+    for (int64_t c = piece_chunk[p]; c < piece_chunk[p + 1]; c++) {
+        s1 += pa[c];
+        s2 += pb[c];
+    }
+    oa[p] = s1;
+    if (ob) ob[p] = s2;
+}
+
+template <class T>
+__global__ void k_copy_cast(int64_t n, const double* __restrict__ a, T* __restrict__ b) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (T)a[i];
+}
+
+// r32 = r64 / |r64| per piece (inner right-hand side of unit norm)
+__global__ void k_scale_down(int64_t n, const int32_t* __restrict__ piece, const double* __restrict__ nrm,
+                             const int32_t* __restrict__ done, const double* __restrict__ a, float* __restrict__ b) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= 6 * n) return;
+    int p = piece[i / 6];
+    if (done[p]) return;
+    double s = nrm[p] > 0.0 ? 1.0 / nrm[p] : 0.0;
+    b[i] = (float)(a[i] * s);
+}
+
+// x64 += |r64| d32 per piece
+__global__ void k_refine_add(int64_t n, const int32_t* __restrict__ piece, const double* __restrict__ nrm,
+                             const int32_t* __restrict__ done, const float* __restrict__ d, double* __restrict__ x) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= 6 * n) return;
+    int p = piece[i / 6];
+    if (done[p]) return;
+    x[i] += nrm[p] * (double)d[i];
+}
+
+__global__ void k_sqrt(int np, const double* __restrict__ a, double* __restrict__ b) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np) b[p] = sqrt(a[p]);
+}
+
+}  // namespace
+
+struct CgState {
+    DBuf<double> scal;  // 9 arrays of np
+    DBuf<int32_t> flags;
+    DBuf<int64_t> iters;
+    DBuf<int32_t> ndone;
+    CgScalars s{};
+    double* beta = nullptr;
+    int np = 0;
+    void init(Context& ctx, int npieces, int32_t* status) {
+        np = npieces;
+        scal.alloc(9 * (size_t)np, ctx.stream, &ctx.mem);
+        scal.zero();
+        flags.alloc(np, ctx.stream, &ctx.mem);
+        flags.zero();
+        iters.alloc(np, ctx.stream, &ctx.mem);
+        iters.zero();
+        ndone.alloc(1, ctx.stream, &ctx.mem);
+        double* q = scal.get();
+        s.bb = q;
+        s.goal = q + np;
+        s.rz = q + 2 * np;
+        s.rr = q + 3 * np;
+        s.pap = q + 4 * np;
+        s.next = q + 5 * np;
+        s.alpha = q + 6 * np;
+        beta = q + 7 * np;
+        s.done = flags.get();
+        s.iters = iters.get();
+        s.status = status;
+    }
+};
+
+// two chunked dots (a.b and a.a) per piece
+template <class T>
+static void dot2(Context& ctx, const Level& L, const int32_t* done, const T* a, const T* b, double* oab, double* oaa) {
+    int np = (int)L.pstart.size() - 1;
+    if ((int64_t)ctx.partial.size() < 2 * std::max<int64_t>(L.nchunks, 1))
+        ctx.partial.alloc(2 * (L.nchunks + 1024), ctx.stream, &ctx.mem);
+    double* pa = ctx.partial.get();
+    double* pb = pa + std::max<int64_t>(L.nchunks, 1);
+    if (L.nchunks > 0) {
+        k_chunk_dot2<T><<<(unsigned)L.nchunks, 256, 0, ctx.stream>>>(L.chunk_lo.get(), L.chunk_piece.get(), done, a, b,
+                                                                    pa, pb);
+        SC_LAUNCH_CK();
+    }
+    k_piece_sum2<<<grid_for(np, 128), 128, 0, ctx.stream>>>(np, L.piece_chunk.get(), pa, pb, done, oab, oaa);
+    SC_LAUNCH_CK();
+}
+
+// PCG with per-piece scalars on level 0. V is the vector type of p, r, z, Ap; S the
+// type of x. On return x holds the solution of K x = rhs for each piece.
+template <class V, class S>
+static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V* ap, double tol, int64_t max_iter,
+                CgState& cg, int64_t timeout_ms, std::chrono::steady_clock::time_point t_start,
+                const int32_t* start_done = nullptr) {
+    Level& L = b.levels[0];
+    cudaStream_t st = ctx.stream;
+    int np = b.npieces;
+    int64_t n6 = 6 * L.n;
+    SC_CK(cudaMemsetAsync(x, 0, n6 * sizeof(S), st));
+    SC_CK(cudaMemcpyAsync(r, rhs, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
+    dot2<V>(ctx, L, nullptr, rhs, rhs, cg.s.bb, nullptr);
+    k_cg_init<<<grid_for(np, 128), 128, 0, st>>>(np, tol, cg.s, start_done);
+    SC_LAUNCH_CK();
+    cycle<V>(ctx, b, 0, r, z, cg.s.done);
+    SC_CK(cudaMemcpyAsync(p, z, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
+    dot2<V>(ctx, L, cg.s.done, r, z, cg.s.rz, cg.s.rr);
+    int32_t* ndone_h = nullptr;
+    SC_CK(cudaMallocHost((void**)&ndone_h, sizeof(int32_t)));
+    try {
+        for (int64_t it = 0;; it++) {
+            cg.ndone.zero();
+            k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
+            SC_LAUNCH_CK();
+            SC_CK(cudaMemcpyAsync(ndone_h, cg.ndone.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            SC_CK(cudaStreamSynchronize(st));
+            if (*ndone_h >= np) break;
+            if (timeout_ms > 0 &&
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count() >
+                    timeout_ms)
+                throw Error(SC_TIMEOUT, "solve ran past its time limit");
+            // Ap, alpha
+            if (L.matrix_free) {
+                stencil_apply<V>(ctx, b, p, ap, nullptr, cg.s.done);
+            } else {
+                ProfScope ps(ctx, fam_of<V>(SC_FAM_SPMV64), spmv_bytes<V>(L, 2));
+                spmv<V>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), VAL<V>(L), p, nullptr, ap, nullptr, nullptr,
+                        L.piece.get(), nullptr, cg.s.done);
+            }
+            dot2<V>(ctx, L, cg.s.done, p, ap, cg.s.pap, nullptr);
+            k_cg_alpha<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s);
+            SC_LAUNCH_CK();
+            if (L.nchunks > 0) {
+                k_axpy2<V, S><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
+                                                                  cg.s.alpha, x, p, r, ap);
+                SC_LAUNCH_CK();
+            }
+            cycle<V>(ctx, b, 0, r, z, cg.s.done);
+            dot2<V>(ctx, L, cg.s.done, r, z, cg.s.next, cg.s.rr);
+            k_cg_beta<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.beta);
+            SC_LAUNCH_CK();
+            if (L.nchunks > 0) {
+                k_pupdate<V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
+                                                                 cg.beta, p, z);
+                SC_LAUNCH_CK();
+            }
+        }
+    } catch (...) {
+        cudaFreeHost(ndone_h);
+        throw;
+    }
+    cudaFreeHost(ndone_h);
+}
+
+// |b - K x| / |b| per piece, in FP64
+static void true_residual(Context& ctx, Batch& b, const double* x, std::vector<double>& out) {
+    Level& L = b.levels[0];
+    int np = b.npieces;
+    DBuf<double> res, nr;
+    res.alloc(6 * L.n, ctx.stream, &ctx.mem);
+    nr.alloc(2 * np, ctx.stream, &ctx.mem);
+    if (L.matrix_free)
+        stencil_residual<double>(ctx, b, x, b.loads.get(), res.get(), nullptr, nullptr);
+    else
+        spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), x, b.loads.get(), res.get(),
+                     nullptr, nullptr, L.piece.get(), nullptr, nullptr);
+    dot2<double>(ctx, L, nullptr, res.get(), res.get(), nr.get(), nullptr);
+    dot2<double>(ctx, L, nullptr, b.loads.get(), b.loads.get(), nr.get() + np, nullptr);
+    std::vector<double> h = nr.to_host();
+    out.resize(np);
+    for (int p = 0; p < np; p++) out[p] = h[np + p] > 0 ? std::sqrt(h[p] / h[np + p]) : 0.0;
+}
+
+void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    Level& L = b.levels[0];
+    int64_t n6 = 6 * L.n;
+    alloc_cycle<double>(ctx, b);
+    x.alloc(n6, ctx.stream, &ctx.mem);
+    DBuf<double> r, z, p, ap;
+    r.alloc(n6, ctx.stream, &ctx.mem);
+    z.alloc(n6, ctx.stream, &ctx.mem);
+    p.alloc(n6, ctx.stream, &ctx.mem);
+    ap.alloc(n6, ctx.stream, &ctx.mem);
+    CgState cg;
+    cg.init(ctx, b.npieces, b.status_d.get());
+    pcg<double, double>(ctx, b, b.loads.get(), x.get(), r.get(), z.get(), p.get(), ap.get(), opt.tol, opt.max_iter, cg,
+                        opt.timeout_ms, t0);
+    std::vector<int64_t> it(b.npieces);
+    cg.iters.download(it.data(), b.npieces);
+    SC_CK(cudaStreamSynchronize(ctx.stream));
+    stats.iterations = it;
+    stats.refinements.assign(b.npieces, 0);
+    true_residual(ctx, b, x.get(), stats.residual);
+}
+
+// Mixed precision: FP32 operators, smoother, transfers and vectors inside FP64
+// iterative refinement; FP64 for the true residual, the CG scalars and the top solve.
+void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t st = ctx.stream;
+    int np = b.npieces;
+    for (size_t l = 0; l < b.levels.size(); l++) {
+        Level& L = b.levels[l];
+        if (!(l == 0 && L.matrix_free)) to_float(ctx, L.val, L.val32);
+        to_float(ctx, L.inv, L.inv32);
+        if (L.pval.size()) to_float(ctx, L.pval, L.pval32);
+    }
+    alloc_cycle<float>(ctx, b);
+    Level& L = b.levels[0];
+    int64_t n6 = 6 * L.n;
+    x.alloc(n6, st, &ctx.mem);
+    x.zero();
+    DBuf<double> r64;
+    r64.alloc(n6, st, &ctx.mem);
+    SC_CK(cudaMemcpyAsync(r64.get(), b.loads.get(), n6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    DBuf<float> rhs, d, r, z, p, ap;
+    for (auto* v : {&rhs, &d, &r, &z, &p, &ap}) v->alloc(n6, st, &ctx.mem);
+    DBuf<double> nrm;
+    nrm.alloc(3 * np, st, &ctx.mem);  // |r64|^2, |r64|, |b|^2
+    dot2<double>(ctx, L, nullptr, b.loads.get(), b.loads.get(), nrm.get() + 2 * np, nullptr);
+    std::vector<double> bb(np);
+    SC_CK(cudaMemcpyAsync(bb.data(), nrm.get() + 2 * np, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SC_CK(cudaStreamSynchronize(st));
+    DBuf<int32_t> outer_done;
+    outer_done.alloc(np, st, &ctx.mem);
+    outer_done.zero();
+    std::vector<int32_t> od(np, 0);
+    std::vector<int64_t> iters(np, 0), refs(np, 0);
+    double inner_tol = opt.inner_tol > 0 ? opt.inner_tol : 1e-4;
+    CgState cg;
+    cg.init(ctx, np, b.status_d.get());
+    for (int outer = 0; outer < 200; outer++) {
+        // FP64 true residual check
+        dot2<double>(ctx, L, nullptr, r64.get(), r64.get(), nrm.get(), nullptr);
+        k_sqrt<<<grid_for(np, 128), 128, 0, st>>>(np, nrm.get(), nrm.get() + np);
+        SC_LAUNCH_CK();
+        std::vector<double> rr(np);
+        SC_CK(cudaMemcpyAsync(rr.data(), nrm.get(), np * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SC_CK(cudaStreamSynchronize(st));
+        bool all = true;
+        for (int pc = 0; pc < np; pc++) {
+            if (!od[pc] && (std::sqrt(rr[pc]) <= opt.tol * std::sqrt(bb[pc]) || iters[pc] >= opt.max_iter)) od[pc] = 1;
+            all = all && od[pc];
+        }
+        if (all) break;
+        outer_done.upload(od.data(), np);
+        k_scale_down<<<grid_for(n6, 256), 256, 0, st>>>(L.n, L.piece.get(), nrm.get() + np, outer_done.get(),
+                                                        r64.get(), rhs.get());
+        SC_LAUNCH_CK();
+        // inner FP32 solve of K d = r64 / |r64| (pieces already converged start done)
+        pcg<float, float>(ctx, b, rhs.get(), d.get(), r.get(), z.get(), p.get(), ap.get(), inner_tol, opt.max_iter, cg,
+                          opt.timeout_ms, t0, outer_done.get());
+        std::vector<int64_t> it(np);
+        cg.iters.download(it.data(), np);
+        SC_CK(cudaStreamSynchronize(st));
+        for (int pc = 0; pc < np; pc++)
+            if (!od[pc]) {
+                iters[pc] += it[pc];
+                refs[pc] += 1;
+            }
+        k_refine_add<<<grid_for(n6, 256), 256, 0, st>>>(L.n, L.piece.get(), nrm.get() + np, outer_done.get(), d.get(),
+                                                        x.get());
+        SC_LAUNCH_CK();
+        // r64 = b - K x in FP64
+        if (L.matrix_free)
+            stencil_residual<double>(ctx, b, x.get(), b.loads.get(), r64.get(), nullptr, outer_done.get());
+        else
+            spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), x.get(), b.loads.get(),
+                         r64.get(), nullptr, nullptr, L.piece.get(), nullptr, outer_done.get());
+    }
+    stats.iterations = iters;
+    stats.refinements = refs;
+    true_residual(ctx, b, x.get(), stats.residual);
+}
+
+}  // namespace sc

@@ -1,0 +1,659 @@
+// Level 0 of voxel pieces on the device.
+//
+// Numbering follows the reference's `build` (statics/src/lattice.rs:124-163) exactly:
+// free cells are visited in flat order ((x*ny)+y)*nz+z; each creates a node for each of
+// its faces, in VOXEL_FACES order -x,+x,-y,+y,-z,+z (lattice/src/lib.rs:64), that no
+// earlier cell created. A + face is always new (its other cell comes later); a - face
+// is new unless the cell before it on that axis is free. A node is held when its other
+// cell is held. Free (not held) nodes are the parts, in node order (bodies.rs:435-442).
+// So node and part ids come from two exclusive scans, no hashing.
+//
+// The operator is matrix-free: a free cell's 36x36 stiffness is k * s * D Kt D
+// (template_gen.cuh); a part on axis a is the + face (slot 2a+1) of its lesser cell A
+// and the - face (slot 2a) of its greater cell B, so its row is
+//   y = k_A * strip_{2a+1}(x of A's six faces) + k_B * strip_{2a}(x of B's six faces),
+// gathered per part with no atomics. Roofline: HBM. Algorithmic bytes per apply:
+// read x and write y (2 * 6 * w per part) plus the cell table (32 B per free cell).
+#include <cub/cub.cuh>
+
+#include "solver.cuh"
+#include "template_gen.cuh"
+
+namespace sc {
+
+namespace {
+
+__device__ __forceinline__ int find_piece(const int64_t* __restrict__ off, int np, int64_t i) {
+    int lo = 0, hi = np;  // off[lo] <= i < off[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= i)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_iota(int64_t n, int32_t* __restrict__ v) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int32_t)i;
+}
+
+struct Dims {
+    int32_t nx, ny, nz, pad;
+};
+
+__device__ __forceinline__ bool is_free(const uint8_t* st, const Dims& d, int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= d.nx || y >= d.ny || z >= d.nz) return false;
+    return st[((int64_t)x * d.ny + y) * d.nz + z] == SC_CELL_FREE;
+}
+__device__ __forceinline__ bool is_held(const uint8_t* st, const Dims& d, int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= d.nx || y >= d.ny || z >= d.nz) return false;
+    return st[((int64_t)x * d.ny + y) * d.nz + z] == SC_CELL_HELD;
+}
+
+// New nodes of a free cell in slot order: slot 2a is new iff the cell before on axis a
+// is not free; slot 2a+1 always. Returns a 6-bit mask.
+__device__ __forceinline__ int new_mask(const uint8_t* st, const Dims& d, int x, int y, int z) {
+    int m = 0;
+    if (!is_free(st, d, x - 1, y, z)) m |= 1;
+    m |= 2;
+    if (!is_free(st, d, x, y - 1, z)) m |= 4;
+    m |= 8;
+    if (!is_free(st, d, x, y, z - 1)) m |= 16;
+    m |= 32;
+    return m;
+}
+
+__global__ void k_count_cells(int np, const int64_t* __restrict__ goff, const Dims* __restrict__ dims,
+                              const uint8_t* __restrict__ st, int64_t ncell, int64_t* __restrict__ new_nodes,
+                              int64_t* __restrict__ free_flag) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int p = find_piece(goff, np, c);
+    Dims d = dims[p];
+    const uint8_t* s = st + goff[p];
+    int64_t l = c - goff[p];
+    int z = (int)(l % d.nz), y = (int)(l / d.nz % d.ny), x = (int)(l / ((int64_t)d.nz * d.ny));
+    if (s[l] != SC_CELL_FREE) {
+        new_nodes[c] = 0;
+        free_flag[c] = 0;
+        return;
+    }
+    new_nodes[c] = __popc(new_mask(s, d, x, y, z));
+    free_flag[c] = 1;
+}
+
+// For every free cell: the node ids of its 6 faces, and for each node it creates: held
+// flag, axis, lesser cell. Each node's lesser and greater free cell (cella / cellb) is
+// written exactly once: by its creator, or, for a - face made by the cell before, by
+// the greater cell itself.
+__global__ void k_cell_nodes(int np, const int64_t* __restrict__ goff, const Dims* __restrict__ dims,
+                             const uint8_t* __restrict__ st, int64_t ncell, const int64_t* __restrict__ node_base,
+                             const int64_t* __restrict__ cell_index, int64_t* __restrict__ cell_node6,
+                             int64_t* __restrict__ node_held, int8_t* __restrict__ node_axis,
+                             int64_t* __restrict__ node_site, int32_t* __restrict__ node_cella,
+                             int32_t* __restrict__ node_cellb) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int p = find_piece(goff, np, c);
+    Dims d = dims[p];
+    const uint8_t* s = st + goff[p];
+    int64_t l = c - goff[p];
+    if (s[l] != SC_CELL_FREE) return;
+    int z = (int)(l % d.nz), y = (int)(l / d.nz % d.ny), x = (int)(l / ((int64_t)d.nz * d.ny));
+    int m = new_mask(s, d, x, y, z);
+    int32_t ci = (int32_t)cell_index[c];
+    int off = 0;
+    for (int slot = 0; slot < 6; slot++) {
+        int a = slot >> 1;
+        int o[3] = {x, y, z};
+        o[a] += (slot & 1) ? 1 : -1;
+        int64_t node;
+        if (m & (1 << slot)) {
+            node = node_base[c] + off;
+            off++;
+            node_held[node] = is_held(s, d, o[0], o[1], o[2]) ? 1 : 0;
+            node_axis[node] = (int8_t)a;
+            int lesser[3] = {x, y, z};
+            if (!(slot & 1)) lesser[a] -= 1;
+            for (int k = 0; k < 3; k++) node_site[3 * node + k] = lesser[k];
+            if (slot & 1) {
+                node_cella[node] = ci;
+                if (!is_free(s, d, o[0], o[1], o[2])) node_cellb[node] = -1;
+            } else {
+                node_cellb[node] = ci;
+                node_cella[node] = -1;
+            }
+        } else {
+            // the cell before on axis a is free and made this node as its + face
+            int64_t lc = ((int64_t)o[0] * d.ny + o[1]) * d.nz + o[2];
+            int mm = new_mask(s, d, o[0], o[1], o[2]);
+            int before = __popc(mm & ((1 << (2 * a + 1)) - 1));
+            node = node_base[goff[p] + lc] + before;
+            node_cellb[node] = ci;
+        }
+        cell_node6[6 * (int64_t)ci + slot] = node;
+    }
+}
+
+__global__ void k_node_parts(int64_t nnodes, const int64_t* __restrict__ held, const int64_t* __restrict__ held_before,
+                             int32_t* __restrict__ node_part) {
+    int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (v >= nnodes) return;
+    node_part[v] = held[v] ? -1 : (int32_t)(v - held_before[v]);
+}
+
+__global__ void k_part_data(int64_t nnodes, int np, const int64_t* __restrict__ node_start,
+                            const int32_t* __restrict__ node_part, const int8_t* __restrict__ node_axis,
+                            const int64_t* __restrict__ node_site, const int32_t* __restrict__ node_cella,
+                            const int32_t* __restrict__ node_cellb, const int64_t* __restrict__ part_start,
+                            const double* __restrict__ pmass, int32_t* __restrict__ piece,
+                            int32_t* __restrict__ part_node, int8_t* __restrict__ axis, int64_t* __restrict__ site,
+                            double* __restrict__ centre, int32_t* __restrict__ cella, int32_t* __restrict__ cellb,
+                            double* __restrict__ mass, double* __restrict__ loads) {
+    int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (v >= nnodes) return;
+    int32_t k = node_part[v];
+    if (k < 0) return;
+    int p = find_piece(node_start, np, v);
+    piece[k] = p;
+    part_node[k] = (int32_t)(v - node_start[p]);
+    int a = node_axis[v];
+    axis[k] = (int8_t)a;
+    int64_t ls[3];
+    for (int q = 0; q < 3; q++) ls[q] = site[3 * k + q] = node_site[3 * v + q];
+    // x = (centre(lesser) + centre(greater)) * 0.5, centre(c) = (c + 0.5) * UNIT (lattice.rs:39-41, 137)
+    for (int q = 0; q < 3; q++) {
+        double ca = ((double)ls[q] + 0.5) * 0.125;
+        double cb = ((double)(ls[q] + (q == a ? 1 : 0)) + 0.5) * 0.125;
+        centre[3 * k + q] = __dmul_rn(__dadd_rn(ca, cb), 0.5);
+    }
+    int32_t A = node_cella[v], B = node_cellb[v];
+    cella[k] = A;
+    cellb[k] = B < 0 ? -1 : B;
+    // node.m += rho s^3 / 6 per free cell it touches (lattice.rs:130, 143)
+    double mcell = pmass[4 * p];
+    double m = 0.0;
+    if (A >= 0) m += mcell;
+    if (B >= 0) m += mcell;
+    mass[k] = m;
+    loads[6 * k + 0] = m * pmass[4 * p + 1];
+    loads[6 * k + 1] = m * pmass[4 * p + 2];
+    loads[6 * k + 2] = m * pmass[4 * p + 3];
+    loads[6 * k + 3] = 0.0;
+    loads[6 * k + 4] = 0.0;
+    loads[6 * k + 5] = 0.0;
+}
+
+__global__ void k_cell_table(int64_t ncells, const int64_t* __restrict__ cell_node6, const int32_t* __restrict__ node_part,
+                             const int64_t* __restrict__ cell_flat, const float* __restrict__ gk, int4* __restrict__ cell) {
+    int64_t ci = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (ci >= ncells) return;
+    int32_t q[6];
+    for (int s = 0; s < 6; s++) q[s] = node_part[cell_node6[6 * ci + s]];
+    float k = gk[cell_flat[ci]];
+    cell[2 * ci] = make_int4(q[0], q[1], q[2], q[3]);
+    cell[2 * ci + 1] = make_int4(q[4], q[5], __float_as_int(k), 0);
+}
+
+__global__ void k_cell_flat(int64_t ncell, const int64_t* __restrict__ free_flag, const int64_t* __restrict__ cell_index,
+                            int64_t* __restrict__ cell_flat) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    if (free_flag[c]) cell_flat[cell_index[c]] = c;
+}
+
+// ---- assembled level-0 blocks (for the Galerkin setup) ----------------------------
+__device__ __forceinline__ double tpl_scaled(int i, int j, double s) {
+    double d = TPL_DEV[i][j] * s;
+    if ((i % 6) >= 3) d *= s;
+    if ((j % 6) >= 3) d *= s;
+    return d;
+}
+
+__global__ void k_row_count(int64_t n, const int8_t* __restrict__ axis, const int32_t* __restrict__ cella,
+                            const int32_t* __restrict__ cellb, const int4* __restrict__ cell, int64_t* __restrict__ cnt) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int c = 1;
+    for (int side = 0; side < 2; side++) {
+        int32_t C = side ? cellb[k] : cella[k];
+        if (C < 0) continue;
+        int4 a = cell[2 * C], b2 = cell[2 * C + 1];
+        int32_t q[6] = {a.x, a.y, a.z, a.w, b2.x, b2.y};
+        for (int s = 0; s < 6; s++)
+            if (q[s] >= 0 && q[s] != (int32_t)k) c++;
+    }
+    cnt[k] = c;
+}
+
+__global__ void k_row_fill(int64_t n, double s, const int8_t* __restrict__ axis, const int32_t* __restrict__ cella,
+                           const int32_t* __restrict__ cellb, const int4* __restrict__ cell,
+                           const int64_t* __restrict__ rowptr, int32_t* __restrict__ col, double* __restrict__ val) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int ax = axis[k];
+    // gather (column, cell side, slot of column, slot of k)
+    int32_t cols[11];
+    int8_t sideof[11], slotof[11];
+    int m = 0;
+    cols[m] = (int32_t)k;
+    sideof[m] = -1;
+    slotof[m] = -1;
+    m++;
+    for (int side = 0; side < 2; side++) {
+        int32_t C = side ? cellb[k] : cella[k];
+        if (C < 0) continue;
+        int4 a = cell[2 * C], b2 = cell[2 * C + 1];
+        int32_t q[6] = {a.x, a.y, a.z, a.w, b2.x, b2.y};
+        for (int sl = 0; sl < 6; sl++)
+            if (q[sl] >= 0 && q[sl] != (int32_t)k) {
+                cols[m] = q[sl];
+                sideof[m] = (int8_t)side;
+                slotof[m] = (int8_t)sl;
+                m++;
+            }
+    }
+    // insertion sort by column
+    for (int i = 1; i < m; i++) {
+        int32_t c0 = cols[i];
+        int8_t s0 = sideof[i], l0 = slotof[i];
+        int j = i - 1;
+        while (j >= 0 && cols[j] > c0) {
+            cols[j + 1] = cols[j];
+            sideof[j + 1] = sideof[j];
+            slotof[j + 1] = slotof[j];
+            j--;
+        }
+        cols[j + 1] = c0;
+        sideof[j + 1] = s0;
+        slotof[j + 1] = l0;
+    }
+    int64_t base = rowptr[k];
+    int32_t CA = cella[k], CB = cellb[k];
+    double kA = CA >= 0 ? (double)__int_as_float(cell[2 * CA + 1].z) : 0.0;
+    double kB = CB >= 0 ? (double)__int_as_float(cell[2 * CB + 1].z) : 0.0;
+    int slA = 2 * ax + 1, slB = 2 * ax;
+    for (int e = 0; e < m; e++) {
+        col[base + e] = cols[e];
+        double* blk = val + 36 * (base + e);
+        for (int i = 0; i < 6; i++)
+            for (int j = 0; j < 6; j++) {
+                double v;
+                if (sideof[e] < 0) {
+                    v = 0.0;
+                    if (CA >= 0) v += kA * tpl_scaled(6 * slA + i, 6 * slA + j, s);
+                    if (CB >= 0) v += kB * tpl_scaled(6 * slB + i, 6 * slB + j, s);
+                } else if (sideof[e] == 0) {
+                    v = kA * tpl_scaled(6 * slA + i, 6 * slotof[e] + j, s);
+                } else {
+                    v = kB * tpl_scaled(6 * slB + i, 6 * slotof[e] + j, s);
+                }
+                blk[6 * i + j] = v;
+            }
+    }
+}
+
+// ---- the matrix-free stencil ---------------------------------------------------------
+template <int SLOT, class T>
+__device__ __forceinline__ void strip(const T (&x)[6][6], T (&acc)[6]) {
+    if constexpr (SLOT == 0) strip_0<T>(x, acc);
+    if constexpr (SLOT == 1) strip_1<T>(x, acc);
+    if constexpr (SLOT == 2) strip_2<T>(x, acc);
+    if constexpr (SLOT == 3) strip_3<T>(x, acc);
+    if constexpr (SLOT == 4) strip_4<T>(x, acc);
+    if constexpr (SLOT == 5) strip_5<T>(x, acc);
+}
+
+template <class T>
+__device__ __forceinline__ void load6(const T* __restrict__ v, int32_t k, T (&o)[6]) {
+    if constexpr (sizeof(T) == 8) {
+        const double2* p = reinterpret_cast<const double2*>(v + 6 * (int64_t)k);
+        double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y; o[4] = c.x; o[5] = c.y;
+    } else {
+        const float2* p = reinterpret_cast<const float2*>(v + 6 * (int64_t)k);
+        float2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y; o[4] = c.x; o[5] = c.y;
+    }
+}
+template <class T>
+__device__ __forceinline__ void store6(T* __restrict__ v, int64_t k, const T (&o)[6]) {
+    if constexpr (sizeof(T) == 8) {
+        double2* p = reinterpret_cast<double2*>(v + 6 * k);
+        p[0] = make_double2(o[0], o[1]);
+        p[1] = make_double2(o[2], o[3]);
+        p[2] = make_double2(o[4], o[5]);
+    } else {
+        float2* p = reinterpret_cast<float2*>(v + 6 * k);
+        p[0] = make_float2(o[0], o[1]);
+        p[1] = make_float2(o[2], o[3]);
+        p[2] = make_float2(o[4], o[5]);
+    }
+}
+
+// acc += k_C * strip_SLOT(x of cell C's faces, rotations scaled by s)
+template <int SLOT, class T>
+__device__ __forceinline__ void cell_term(const int4* __restrict__ cell, int32_t C, const T* __restrict__ x, T s,
+                                          T (&acc)[6]) {
+    int4 a = __ldg(cell + 2 * C), b = __ldg(cell + 2 * C + 1);
+    int32_t q[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+    T kc = (T)__int_as_float(b.z);
+    T xs[6][6];
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        if (q[f] >= 0) {
+            load6<T>(x, q[f], xs[f]);
+            xs[f][3] *= s;
+            xs[f][4] *= s;
+            xs[f][5] *= s;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 6; j++) xs[f][j] = T(0);
+        }
+    }
+    T t[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    strip<SLOT, T>(xs, t);
+#pragma unroll
+    for (int i = 0; i < 6; i++) acc[i] = fma(kc, t[i], acc[i]);
+}
+
+// y = K x over the parts grouped by axis (perm). MODE 0: y = Kx. MODE 1: y = r - Kx.
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) k_stencil(int64_t n_perm, const int32_t* __restrict__ perm, int64_t off1,
+                                                 int64_t off2, const int32_t* __restrict__ cella,
+                                                 const int32_t* __restrict__ cellb, const int4* __restrict__ cell,
+                                                 const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
+                                                 T s, const int32_t* __restrict__ piece,
+                                                 const int32_t* __restrict__ skip_row, const int32_t* __restrict__ done) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n_perm) return;
+    int32_t k = perm[i];
+    if (skip_row && skip_row[k]) return;
+    if (done && done[piece[k]]) return;
+    int32_t A = cella[k], B = cellb[k];
+    T acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    if (i < off1) {
+        if (A >= 0) cell_term<1, T>(cell, A, x, s, acc);
+        if (B >= 0) cell_term<0, T>(cell, B, x, s, acc);
+    } else if (i < off2) {
+        if (A >= 0) cell_term<3, T>(cell, A, x, s, acc);
+        if (B >= 0) cell_term<2, T>(cell, B, x, s, acc);
+    } else {
+        if (A >= 0) cell_term<5, T>(cell, A, x, s, acc);
+        if (B >= 0) cell_term<4, T>(cell, B, x, s, acc);
+    }
+    T o[6];
+    o[0] = acc[0] * s;
+    o[1] = acc[1] * s;
+    o[2] = acc[2] * s;
+    o[3] = acc[3] * s * s;
+    o[4] = acc[4] * s * s;
+    o[5] = acc[5] * s * s;
+    if (MODE == 1) {
+        T rr[6];
+        load6<T>(r, k, rr);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] = rr[j] - o[j];
+    }
+    store6<T>(y, k, o);
+}
+
+// Strain energy of each free cell's 60 bonds at motions x: U = 1/2 x_c' K_c x_c with
+// K_c = k s D Kt D over its six faces (held faces contribute zero motion).
+__global__ void k_cell_energy(int64_t ncells, const int4* __restrict__ cell, const double* __restrict__ x, double s,
+                              double* __restrict__ energy) {
+    int64_t C = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (C >= ncells) return;
+    int4 a = cell[2 * C], b = cell[2 * C + 1];
+    int32_t q[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+    double kc = (double)__int_as_float(b.z);
+    double xs[36];
+    for (int f = 0; f < 6; f++)
+        for (int j = 0; j < 6; j++) {
+            double v = q[f] >= 0 ? x[6 * (int64_t)q[f] + j] : 0.0;
+            xs[6 * f + j] = j >= 3 ? v * s : v;
+        }
+    double e = 0.0;
+    for (int i = 0; i < 36; i++) {
+        double t = 0.0;
+        for (int j = 0; j < 36; j++) t = fma(TPL_DEV[i][j], xs[j], t);
+        e = fma(xs[i], t, e);
+    }
+    energy[C] = 0.5 * kc * s * e;
+}
+
+}  // namespace
+
+// Algorithmic bytes of one stencil launch: x read and y written once (and r read for
+// the residual form), 6 values a part; the cells' stiffness (4 B each) and occupancy
+// (one bit per grid cell).
+template <class T>
+static double stencil_bytes(const Batch& b, int vec_passes) {
+    const Grid0& g = b.grid;
+    double G = g.grid_off.empty() ? 0.0 : (double)g.grid_off.back();
+    return (double)sizeof(T) * 6.0 * (double)b.levels[0].n * vec_passes + 4.0 * (double)g.ncells + G / 8.0;
+}
+
+template <class T>
+void stencil_apply(Context& ctx, const Batch& b, const T* x, T* y, const int32_t* skip_row, const int32_t* done) {
+    const Grid0& g = b.grid;
+    const Level& L = b.levels[0];
+    int64_t n = g.axis_off[3];
+    ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_STENCIL64 : SC_FAM_STENCIL32, stencil_bytes<T>(b, 2));
+    k_stencil<T, 0><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.perm.get(), g.axis_off[1], g.axis_off[2],
+                                                               g.cella.get(), g.cellb.get(), g.cell.get(), x,
+                                                               nullptr, y, (T)g.s, L.piece.get(), skip_row, done);
+    SC_LAUNCH_CK();
+}
+template void stencil_apply<double>(Context&, const Batch&, const double*, double*, const int32_t*, const int32_t*);
+template void stencil_apply<float>(Context&, const Batch&, const float*, float*, const int32_t*, const int32_t*);
+
+template <class T>
+void stencil_residual(Context& ctx, const Batch& b, const T* x, const T* r, T* y, const int32_t* skip_row,
+                      const int32_t* done) {
+    const Grid0& g = b.grid;
+    const Level& L = b.levels[0];
+    int64_t n = g.axis_off[3];
+    ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_STENCIL64 : SC_FAM_STENCIL32, stencil_bytes<T>(b, 3));
+    k_stencil<T, 1><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.perm.get(), g.axis_off[1], g.axis_off[2],
+                                                               g.cella.get(), g.cellb.get(), g.cell.get(), x, r, y,
+                                                               (T)g.s, L.piece.get(), skip_row, done);
+    SC_LAUNCH_CK();
+}
+template void stencil_residual<double>(Context&, const Batch&, const double*, const double*, double*, const int32_t*,
+                                       const int32_t*);
+template void stencil_residual<float>(Context&, const Batch&, const float*, const float*, float*, const int32_t*,
+                                      const int32_t*);
+
+void grid_cell_energy(Context& ctx, const Batch& b, const double* x, double* energy_cells) {
+    const Grid0& g = b.grid;
+    k_cell_energy<<<grid_for(g.ncells, 128), 128, 0, ctx.stream>>>(g.ncells, g.cell.get(), x, g.s, energy_cells);
+    SC_LAUNCH_CK();
+}
+
+// Builds level 0 of a batch of voxel pieces. The grids' state/k are uploaded (or
+// copied device to device) into one concatenated array.
+void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks) {
+    cudaStream_t st = ctx.stream;
+    MemStats* ms = &ctx.mem;
+    int np = (int)grids.size();
+    b.npieces = np;
+    std::vector<int64_t> goff(np + 1, 0);
+    std::vector<Dims> dims(np);
+    for (int p = 0; p < np; p++) {
+        const sc_grid& g = grids[p];
+        dims[p] = Dims{g.nx, g.ny, g.nz, 0};
+        goff[p + 1] = goff[p] + (int64_t)g.nx * g.ny * g.nz;
+    }
+    int64_t ncell = goff[np];
+    DBuf<int64_t> goff_d;
+    goff_d.alloc(np + 1, st, ms);
+    goff_d.upload(goff.data(), np + 1);
+    DBuf<Dims> dims_d;
+    dims_d.alloc(np, st, ms);
+    dims_d.upload(dims.data(), np);
+    DBuf<uint8_t> gst;
+    gst.alloc(ncell, st, ms);
+    DBuf<float> gk;
+    gk.alloc(ncell, st, ms);
+    for (int p = 0; p < np; p++) {
+        const sc_grid& g = grids[p];
+        size_t cnt = (size_t)(goff[p + 1] - goff[p]);
+        auto kind = g.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        SC_CK(cudaMemcpyAsync(gst.get() + goff[p], g.state, cnt, kind, st));
+        SC_CK(cudaMemcpyAsync(gk.get() + goff[p], g.k, cnt * sizeof(float), kind, st));
+    }
+    // counts and scans
+    DBuf<int64_t> newn, freef, node_base, cell_index;
+    newn.alloc(ncell + 1, st, ms);
+    freef.alloc(ncell + 1, st, ms);
+    node_base.alloc(ncell + 1, st, ms);
+    cell_index.alloc(ncell + 1, st, ms);
+    SC_CK(cudaMemsetAsync(newn.get() + ncell, 0, sizeof(int64_t), st));
+    SC_CK(cudaMemsetAsync(freef.get() + ncell, 0, sizeof(int64_t), st));
+    k_count_cells<<<grid_for(ncell, 256), 256, 0, st>>>(np, goff_d.get(), dims_d.get(), gst.get(), ncell, newn.get(),
+                                                        freef.get());
+    SC_LAUNCH_CK();
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, newn.get(), node_base.get(), ncell + 1, st);
+    cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, newn.get(), node_base.get(), ncell + 1, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, freef.get(), cell_index.get(), ncell + 1, st);
+    cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, freef.get(), cell_index.get(), ncell + 1, st);
+    int64_t nnodes = 0, nfree = 0;
+    SC_CK(cudaMemcpyAsync(&nnodes, node_base.get() + ncell, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SC_CK(cudaMemcpyAsync(&nfree, cell_index.get() + ncell, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    // per-piece node starts
+    std::vector<int64_t> node_start(np + 1, 0);
+    for (int p = 0; p < np; p++)
+        SC_CK(cudaMemcpyAsync(&node_start[p], node_base.get() + goff[p], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SC_CK(cudaStreamSynchronize(st));
+    node_start[np] = nnodes;
+    require(nnodes < (int64_t)INT32_MAX && nfree < (int64_t)INT32_MAX, SC_BAD_INPUT, "piece too large");
+    b.node_count.resize(np);
+    for (int p = 0; p < np; p++) b.node_count[p] = node_start[p + 1] - node_start[p];
+    b.node_start.alloc(np + 1, st, ms);
+    b.node_start.upload(node_start.data(), np + 1);
+
+    DBuf<int64_t> cell_node6;
+    cell_node6.alloc(6 * std::max<int64_t>(nfree, 1), st, ms);
+    DBuf<int64_t> node_held;
+    node_held.alloc(nnodes + 1, st, ms);
+    DBuf<int8_t> node_axis;
+    node_axis.alloc(nnodes + 1, st, ms);
+    DBuf<int64_t> node_site;
+    node_site.alloc(3 * (nnodes + 1), st, ms);
+    DBuf<int32_t> node_cella, node_cellb;
+    node_cella.alloc(nnodes + 1, st, ms);
+    node_cellb.alloc(nnodes + 1, st, ms);
+    k_cell_nodes<<<grid_for(ncell, 256), 256, 0, st>>>(np, goff_d.get(), dims_d.get(), gst.get(), ncell, node_base.get(),
+                                                       cell_index.get(), cell_node6.get(), node_held.get(),
+                                                       node_axis.get(), node_site.get(), node_cella.get(),
+                                                       node_cellb.get());
+    SC_LAUNCH_CK();
+    // parts: free nodes in node order
+    DBuf<int64_t> held_before;
+    held_before.alloc(nnodes + 1, st, ms);
+    SC_CK(cudaMemsetAsync(node_held.get() + nnodes, 0, sizeof(int64_t), st));
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, node_held.get(), held_before.get(), nnodes + 1, st);
+    cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, node_held.get(), held_before.get(), nnodes + 1, st);
+    DBuf<int32_t> node_part;
+    node_part.alloc(nnodes + 1, st, ms);
+    k_node_parts<<<grid_for(nnodes, 256), 256, 0, st>>>(nnodes, node_held.get(), held_before.get(), node_part.get());
+    SC_LAUNCH_CK();
+    std::vector<int64_t> hb(np + 1);
+    for (int p = 0; p <= np; p++)
+        SC_CK(cudaMemcpyAsync(&hb[p], held_before.get() + node_start[p], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SC_CK(cudaStreamSynchronize(st));
+    Level& L = b.levels.emplace_back();
+    L.pstart.resize(np + 1);
+    for (int p = 0; p <= np; p++) L.pstart[p] = node_start[p] - hb[p];
+    int64_t n = L.pstart[np];
+    L.n = n;
+    require(n > 0, SC_BAD_INPUT, "no free node in the batch");
+    L.pstart_d.alloc(np + 1, st, ms);
+    L.pstart_d.upload(L.pstart.data(), np + 1);
+    L.piece.alloc(n, st, ms);
+    L.centre.alloc(3 * n, st, ms);
+    L.site.alloc(3 * n, st, ms);
+    b.part_node.alloc(n, st, ms);
+    b.mass.alloc(n, st, ms);
+    b.loads.alloc(6 * n, st, ms);
+    Grid0& g = b.grid;
+    g.s = 0.125;
+    g.ncells = nfree;
+    g.cella.alloc(n, st, ms);
+    g.cellb.alloc(n, st, ms);
+    g.axis.alloc(n, st, ms);
+    // per piece: a cell's share of weight on each face (lattice.rs:130) and gravity
+    std::vector<double> pm(4 * (size_t)np);
+    for (int p = 0; p < np; p++) {
+        pm[4 * p] = grids[p].rho * g.s * g.s * g.s / 6.0;
+        for (int q = 0; q < 3; q++) pm[4 * p + 1 + q] = grids[p].gravity[q];
+    }
+    DBuf<double> pm_d;
+    pm_d.alloc(pm.size(), st, ms);
+    pm_d.upload(pm.data(), pm.size());
+    k_part_data<<<grid_for(nnodes, 256), 256, 0, st>>>(
+        nnodes, np, b.node_start.get(), node_part.get(), node_axis.get(), node_site.get(), node_cella.get(),
+        node_cellb.get(), L.pstart_d.get(), pm_d.get(), L.piece.get(),
+        b.part_node.get(), g.axis.get(), L.site.get(), L.centre.get(), g.cella.get(), g.cellb.get(), b.mass.get(),
+        b.loads.get());
+    SC_LAUNCH_CK();
+    // cell table
+    g.cell_flat.alloc(std::max<int64_t>(nfree, 1), st, ms);
+    k_cell_flat<<<grid_for(ncell, 256), 256, 0, st>>>(ncell, freef.get(), cell_index.get(), g.cell_flat.get());
+    SC_LAUNCH_CK();
+    g.cell.alloc(2 * std::max<int64_t>(nfree, 1), st, ms);
+    k_cell_table<<<grid_for(nfree, 256), 256, 0, st>>>(nfree, cell_node6.get(), node_part.get(), g.cell_flat.get(),
+                                                        gk.get(), g.cell.get());
+    SC_LAUNCH_CK();
+    // parts grouped by axis (stable: ascending part id within an axis)
+    {
+        DBuf<int32_t> ids, ids_out;
+        ids.alloc(n, st, ms);
+        ids_out.alloc(n, st, ms);
+        DBuf<int8_t> ax_out;
+        ax_out.alloc(n, st, ms);
+        k_iota<<<grid_for(n, 256), 256, 0, st>>>(n, ids.get());
+        SC_LAUNCH_CK();
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, g.axis.get(), ax_out.get(), ids.get(), ids_out.get(), n, 0, 2, st);
+        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, g.axis.get(), ax_out.get(), ids.get(),
+                                        ids_out.get(), n, 0, 2, st);
+        g.perm = std::move(ids_out);
+        std::vector<int8_t> axh = ax_out.to_host();
+        g.axis_off[0] = 0;
+        for (int a = 0; a < 3; a++) {
+            int64_t cnt = 0;
+            for (int8_t v : axh) cnt += (v == a);
+            g.axis_off[a + 1] = g.axis_off[a] + cnt;
+        }
+    }
+    // assembled blocks for the setup
+    L.rowptr.alloc(n + 1, st, ms);
+    {
+        DBuf<int64_t> cnt;
+        cnt.alloc(n + 1, st, ms);
+        SC_CK(cudaMemsetAsync(cnt.get() + n, 0, sizeof(int64_t), st));
+        k_row_count<<<grid_for(n, 256), 256, 0, st>>>(n, g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(),
+                                                      cnt.get());
+        SC_LAUNCH_CK();
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.get(), L.rowptr.get(), n + 1, st);
+        cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, cnt.get(), L.rowptr.get(), n + 1, st);
+    }
+    SC_CK(cudaMemcpyAsync(&L.nnzb, L.rowptr.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SC_CK(cudaStreamSynchronize(st));
+    L.col.alloc(L.nnzb, st, ms);
+    L.val.alloc(36 * L.nnzb, st, ms);
+    k_row_fill<<<grid_for(n, 128), 128, 0, st>>>(n, g.s, g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(),
+                                                 L.rowptr.get(), L.col.get(), L.val.get());
+    SC_LAUNCH_CK();
+    L.matrix_free = true;
+    g.grid_off = std::move(goff);
+    (void)keep_blocks;
+    SC_CK(cudaStreamSynchronize(st));
+}
+
+}  // namespace sc

@@ -1,0 +1,999 @@
+// The hierarchy of bodies within bodies (statics/src/bodies.rs:123-282, 444-461), built
+// on the device for every piece of a batch at once:
+//   * block inverses of each part's own block (Gauss-Jordan, bodies.rs:576-602);
+//   * the smoother step 4/3 / lambda_max(D^-1 K) by 12 power steps from the reference's
+//     start vector (bodies.rs:180-190);
+//   * bodies: connected pieces of equal octree key over the level's stored pairs, ids by
+//     first appearance (bodies.rs:472-496) -- bit-exact: component minima by label
+//     propagation, ids by an exclusive scan over the roots in part order;
+//   * the smoothed prolongator P = (I - step D^-1 K) P0 and the Galerkin product P'KP
+//     (bodies.rs:228-282), symbolic patterns by expand / sort / unique (the pattern is
+//     the reference's merge pattern, structural zeros included), values by one warp
+//     per output row;
+//   * each piece's top level as a dense factor (bodies.rs:286-315), kept as its inverse.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+
+#include "kernels.cuh"
+
+namespace sc {
+
+
+namespace {
+
+__global__ void k_find_diag_invert(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                   const double* __restrict__ val, double* __restrict__ inv,
+                                   const int32_t* __restrict__ piece, int32_t* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int64_t e = lower_bound_i32(col, rowptr[k], rowptr[k + 1], (int32_t)k);
+    bool ok = e < rowptr[k + 1] && col[e] == (int32_t)k;
+    double tmp[36];
+    if (ok) ok = invert6(val + 36 * e, tmp);
+    if (!ok) {
+        for (int i = 0; i < 36; i++) tmp[i] = 0.0;
+        if (status) atomicMax(status + piece[k], (int)SC_BREAKDOWN);
+    }
+    for (int i = 0; i < 36; i++) inv[36 * k + i] = tmp[i];
+}
+
+__global__ void k_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+
+// v[k][s] = 1 + ((7k + 3s) mod 11) / 11, k counted within the piece (bodies.rs:181)
+__global__ void k_power_start(int64_t n, const int64_t* __restrict__ pstart, const int32_t* __restrict__ piece,
+                              double* __restrict__ v) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int64_t kl = k - pstart[piece[k]];
+    for (int s = 0; s < 6; s++) v[6 * k + s] = 1.0 + (double)((7 * kl + 3 * s) % 11) / 11.0;
+}
+
+// most = |w| / |v|; v = w / |w| (bodies.rs:184-187)
+__global__ void k_power_scale(int64_t n, const int32_t* __restrict__ piece, const double* __restrict__ ww,
+                              const double* __restrict__ w, double* __restrict__ v) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= 6 * n) return;
+    double scale = 1.0 / sqrt(ww[piece[i / 6]]);
+    v[i] = w[i] * scale;
+}
+
+__global__ void k_power_most(int np, const double* __restrict__ ww, const double* __restrict__ vv,
+                             double* __restrict__ most) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    most[p] = sqrt(ww[p]) / sqrt(vv[p]);
+}
+
+__global__ void k_step(int np, const double* __restrict__ most, double* __restrict__ step) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    step[p] = 4.0 / 3.0 / most[p];
+}
+
+// ---- bodies ---------------------------------------------------------------------
+__device__ __forceinline__ bool same_key(const int64_t* __restrict__ site, int64_t i, int64_t j, int64_t mask) {
+    return (site[3 * i] & mask) == (site[3 * j] & mask) && (site[3 * i + 1] & mask) == (site[3 * j + 1] & mask) &&
+           (site[3 * i + 2] & mask) == (site[3 * j + 2] & mask);
+}
+
+__global__ void k_label_init(int64_t n, int32_t* __restrict__ label) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < n) label[k] = (int32_t)k;
+}
+
+// One sweep of minimum-label propagation over pairs of equal key, then pointer jumping.
+__global__ void k_label_sweep(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                              const int64_t* __restrict__ site, int64_t mask, const int32_t* __restrict__ active,
+                              const int32_t* __restrict__ piece, int32_t* __restrict__ label,
+                              int32_t* __restrict__ changed) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (!active[piece[k]]) return;
+    int32_t m = label[k];
+    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
+        int32_t j = col[e];
+        if (j == (int32_t)k) continue;
+        if (same_key(site, k, j, mask)) {
+            int32_t lj = label[j];
+            if (lj < m) m = lj;
+        }
+    }
+    int32_t old = label[k];
+    if (m < old) {
+        atomicMin(label + k, m);
+        atomicMin(label + old, m);
+        *changed = 1;
+    }
+}
+
+__global__ void k_label_jump(int64_t n, int32_t* __restrict__ label) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int32_t l = label[k];
+    int32_t ll = label[l];
+    while (ll != l) {
+        l = ll;
+        ll = label[l];
+    }
+    label[k] = l;
+}
+
+__global__ void k_roots(int64_t n, const int32_t* __restrict__ label, const int32_t* __restrict__ piece,
+                        int64_t* __restrict__ root, int32_t* __restrict__ bodies_per_piece) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int r = label[k] == (int32_t)k;
+    root[k] = r;
+    if (r) atomicAdd(bodies_per_piece + piece[k], 1);
+}
+
+__global__ void k_mask_roots(int64_t n, const int32_t* __restrict__ piece, const int32_t* __restrict__ active,
+                             int64_t* __restrict__ root) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (!active[piece[k]]) root[k] = 0;
+}
+
+__global__ void k_up(int64_t n, const int32_t* __restrict__ label, const int64_t* __restrict__ id,
+                     const int32_t* __restrict__ piece, const int32_t* __restrict__ active, int32_t* __restrict__ up,
+                     int32_t* __restrict__ top_of_part) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    bool a = active[piece[k]];
+    up[k] = a ? (int32_t)id[label[k]] : -1;
+    top_of_part[k] = a ? 0 : 1;
+}
+
+// members of each body in part order: body c's parts are mem[moff[c] .. moff[c+1])
+__global__ void k_centroid(int64_t nc, const int64_t* __restrict__ moff, const int32_t* __restrict__ mem,
+                           const double* __restrict__ centre, const int64_t* __restrict__ site,
+                           const int32_t* __restrict__ piece, double* __restrict__ centre_c,
+                           int64_t* __restrict__ site_c, int32_t* __restrict__ piece_c) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, cnt = 0.0;
+    for (int64_t t = moff[c]; t < moff[c + 1]; t++) {
+        int32_t k = mem[t];
+        s0 += centre[3 * (int64_t)k];
+        s1 += centre[3 * (int64_t)k + 1];
+        s2 += centre[3 * (int64_t)k + 2];
+        cnt += 1.0;
+    }
+    double inv = 1.0 / cnt;
+    centre_c[3 * c] = s0 * inv;
+    centre_c[3 * c + 1] = s1 * inv;
+    centre_c[3 * c + 2] = s2 * inv;
+    int32_t k0 = mem[moff[c]];
+    for (int q = 0; q < 3; q++) site_c[3 * c + q] = site[3 * (int64_t)k0 + q];
+    piece_c[c] = piece[k0];
+}
+
+__global__ void k_offsets_from_sorted(int64_t m, const int32_t* __restrict__ keys, int64_t nkeys,
+                                      int64_t* __restrict__ off) {
+    // off[c] = first index with keys >= c, for c in [0, nkeys]; keys sorted
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i > m) return;
+    int32_t prev = i == 0 ? -1 : keys[i - 1];
+    int32_t cur = i == m ? (int32_t)nkeys : keys[i];
+    for (int32_t c = prev + 1; c <= cur; c++) off[c] = i;
+}
+
+// ---- patterns by expand / sort / unique --------------------------------------------
+__global__ void k_count_P(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ up,
+                          int64_t* __restrict__ cnt) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    cnt[k] = up[k] >= 0 ? rowptr[k + 1] - rowptr[k] : 0;
+}
+__global__ void k_fill_P(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                         const int32_t* __restrict__ up, const int64_t* __restrict__ off, uint64_t* __restrict__ keys) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (up[k] < 0) return;
+    int64_t o = off[k];
+    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) keys[o++] = ((uint64_t)k << 32) | (uint32_t)up[col[e]];
+}
+__global__ void k_count_KP(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                           const int64_t* __restrict__ prow, const int32_t* __restrict__ up, int64_t* __restrict__ cnt) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int64_t c = 0;
+    if (up[k] >= 0)
+        for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
+            int32_t o = col[e];
+            c += prow[o + 1] - prow[o];
+        }
+    cnt[k] = c;
+}
+__global__ void k_fill_KP(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                          const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+                          const int32_t* __restrict__ up, const int64_t* __restrict__ off, uint64_t* __restrict__ keys) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (up[k] < 0) return;
+    int64_t o = off[k];
+    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
+        int32_t q = col[e];
+        for (int64_t f = prow[q]; f < prow[q + 1]; f++) keys[o++] = ((uint64_t)k << 32) | (uint32_t)pcol[f];
+    }
+}
+// per P entry (k, c): the columns d >= c of KP row k
+__global__ void k_count_C(int64_t n, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+                          const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol, int64_t* __restrict__ cnt) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    for (int64_t e = prow[k]; e < prow[k + 1]; e++) {
+        int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], pcol[e]);
+        cnt[e] = kprow[k + 1] - lb;
+    }
+}
+__global__ void k_fill_C(int64_t n, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+                         const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol,
+                         const int64_t* __restrict__ off, uint64_t* __restrict__ keys) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    for (int64_t e = prow[k]; e < prow[k + 1]; e++) {
+        int32_t c = pcol[e];
+        int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], c);
+        int64_t o = off[e];
+        for (int64_t f = lb; f < kprow[k + 1]; f++) keys[o++] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)kpcol[f];
+    }
+}
+__global__ void k_unpack_pattern(int64_t m, const uint64_t* __restrict__ keys, int32_t* __restrict__ col,
+                                 int32_t* __restrict__ row) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    col[i] = (int32_t)(keys[i] & 0xffffffffu);
+    row[i] = (int32_t)(keys[i] >> 32);
+}
+
+// ---- numeric products, one warp per output row ----------------------------------------
+// acc(r, c) += sum_j A(r, j) B(j, c) for the lane's entries (e = lane, lane + 32 < 36).
+// A transposed when TA. B is a rigid shift [I M; 0 I] with M w = w x r when RB (rv = r).
+template <bool TA, bool RB>
+__device__ __forceinline__ void warp_block_mac(int lane, const double* __restrict__ A, const double* __restrict__ B,
+                                               const double* rv, double* __restrict__ C) {
+#pragma unroll
+    for (int rep = 0; rep < 2; rep++) {
+        int e = lane + 32 * rep;
+        if (e >= 36) break;
+        int r = e / 6, c = e % 6;
+        double s = 0.0;
+        if (RB) {
+            // column c of R: c < 3 -> e_c; c >= 3 -> (M[:, c-3], e_c)
+            double a0 = TA ? A[0 * 6 + r] : A[r * 6 + 0];
+            double a1 = TA ? A[1 * 6 + r] : A[r * 6 + 1];
+            double a2 = TA ? A[2 * 6 + r] : A[r * 6 + 2];
+            if (c < 3) {
+                s = c == 0 ? a0 : (c == 1 ? a1 : a2);
+            } else {
+                double ac = TA ? A[c * 6 + r] : A[r * 6 + c];
+                // M = [[0, r2, -r1], [-r2, 0, r0], [r1, -r0, 0]]
+                double m0, m1, m2;
+                if (c == 3) { m0 = 0.0; m1 = -rv[2]; m2 = rv[1]; }
+                else if (c == 4) { m0 = rv[2]; m1 = 0.0; m2 = -rv[0]; }
+                else { m0 = -rv[1]; m1 = rv[0]; m2 = 0.0; }
+                s = fma(a0, m0, fma(a1, m1, fma(a2, m2, ac)));
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                double a = TA ? A[j * 6 + r] : A[r * 6 + j];
+                s = fma(a, B[j * 6 + c], s);
+            }
+        }
+        C[e] += s;
+    }
+}
+
+// S[k][pos(up[o])] += K_ko R_o over the row; then P_k = delta R_k - step D_k^-1 S.
+__global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restrict__ rowptr,
+                                               const int32_t* __restrict__ col, const double* __restrict__ val,
+                                               const int32_t* __restrict__ up, const double* __restrict__ rvec,
+                                               const double* __restrict__ inv, const double* __restrict__ step,
+                                               const int32_t* __restrict__ piece, const int64_t* __restrict__ prow,
+                                               const int32_t* __restrict__ pcol, double* __restrict__ pval) {
+    int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (k >= n) return;
+    int lane = threadIdx.x & 31;
+    if (up[k] < 0) return;
+    int64_t p0 = prow[k], p1 = prow[k + 1];
+    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
+        int32_t o = col[e];
+        int64_t pos = lower_bound_i32(pcol, p0, p1, up[o]);
+        double rv[3] = {rvec[3 * (int64_t)o], rvec[3 * (int64_t)o + 1], rvec[3 * (int64_t)o + 2]};
+        warp_block_mac<false, true>(lane, val + 36 * e, nullptr, rv, pval + 36 * pos);
+        __syncwarp();
+    }
+    double st = step[piece[k]];
+    const double* D = inv + 36 * k;
+    double rk[3] = {rvec[3 * k], rvec[3 * k + 1], rvec[3 * k + 2]};
+    for (int64_t pos = p0; pos < p1; pos++) {
+        double* S = pval + 36 * pos;
+        double out[2];
+#pragma unroll
+        for (int rep = 0; rep < 2; rep++) {
+            int e = lane + 32 * rep;
+            out[rep] = 0.0;
+            if (e < 36) {
+                int r = e / 6, c = e % 6;
+                double s = 0.0;
+                for (int j = 0; j < 6; j++) s = fma(D[r * 6 + j], S[j * 6 + c], s);
+                double rig = 0.0;
+                if (pcol[pos] == up[k]) {
+                    if (r == c) rig = 1.0;
+                    else if (r < 3 && c >= 3) {
+                        // M[r][c-3]
+                        int cc = c - 3;
+                        if (r == 0) rig = cc == 1 ? rk[2] : (cc == 2 ? -rk[1] : 0.0);
+                        if (r == 1) rig = cc == 0 ? -rk[2] : (cc == 2 ? rk[0] : 0.0);
+                        if (r == 2) rig = cc == 0 ? rk[1] : (cc == 1 ? -rk[0] : 0.0);
+                    }
+                }
+                out[rep] = rig + (-st) * s;
+            }
+        }
+        __syncwarp();
+        if (lane < 36) S[lane] = out[0];
+        if (lane + 32 < 36) S[lane + 32] = out[1];
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_num_KP(int64_t n, const int64_t* __restrict__ rowptr,
+                                                const int32_t* __restrict__ col, const double* __restrict__ val,
+                                                const int32_t* __restrict__ up, const int64_t* __restrict__ prow,
+                                                const int32_t* __restrict__ pcol, const double* __restrict__ pval,
+                                                const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol,
+                                                double* __restrict__ kpval) {
+    int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (k >= n) return;
+    int lane = threadIdx.x & 31;
+    if (up[k] < 0) return;
+    int64_t q0 = kprow[k], q1 = kprow[k + 1];
+    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
+        int32_t o = col[e];
+        for (int64_t f = prow[o]; f < prow[o + 1]; f++) {
+            int64_t pos = lower_bound_i32(kpcol, q0, q1, pcol[f]);
+            warp_block_mac<false, false>(lane, val + 36 * e, pval + 36 * f, nullptr, kpval + 36 * pos);
+            __syncwarp();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_num_C(int64_t nc, const int64_t* __restrict__ tptr,
+                                               const int64_t* __restrict__ tent, const int32_t* __restrict__ trow,
+                                               const double* __restrict__ pval, const int64_t* __restrict__ kprow,
+                                               const int32_t* __restrict__ kpcol, const double* __restrict__ kpval,
+                                               const int64_t* __restrict__ crow, const int32_t* __restrict__ ccol,
+                                               double* __restrict__ cval) {
+    int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (c >= nc) return;
+    int lane = threadIdx.x & 31;
+    int64_t c0 = crow[c], c1 = crow[c + 1];
+    for (int64_t t = tptr[c]; t < tptr[c + 1]; t++) {
+        int64_t e = tent[t];
+        int32_t k = trow[t];
+        int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], (int32_t)c);
+        for (int64_t f = lb; f < kprow[k + 1]; f++) {
+            int64_t pos = lower_bound_i32(ccol, c0, c1, kpcol[f]);
+            warp_block_mac<true, false>(lane, pval + 36 * e, kpval + 36 * f, nullptr, cval + 36 * pos);
+            __syncwarp();
+        }
+    }
+}
+
+// full symmetric storage: entry i of the full pattern copies upper entry src[i] & mask,
+// transposed when its top bit is set
+__global__ void k_mirror_vals(int64_t m, const int64_t* __restrict__ src, const double* __restrict__ up_val,
+                              double* __restrict__ val) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= 36 * m) return;
+    int64_t b = i / 36;
+    int e = (int)(i % 36);
+    int64_t s = src[b];
+    bool tr = s < 0;
+    int64_t u = tr ? ~s : s;
+    int r = e / 6, c = e % 6;
+    val[i] = tr ? up_val[36 * u + c * 6 + r] : up_val[36 * u + e];
+}
+__global__ void k_mirror_keys(int64_t m, const int32_t* __restrict__ row, const int32_t* __restrict__ col,
+                              uint64_t* __restrict__ keys, int64_t* __restrict__ src, const int64_t* __restrict__ off) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    int64_t o = off[i];
+    uint32_t r = (uint32_t)row[i], c = (uint32_t)col[i];
+    keys[o] = ((uint64_t)r << 32) | c;
+    src[o] = i;
+    if (c != r) {
+        keys[o + 1] = ((uint64_t)c << 32) | r;
+        src[o + 1] = ~i;
+    }
+}
+__global__ void k_mirror_count(int64_t m, const int32_t* __restrict__ row, const int32_t* __restrict__ col,
+                               int64_t* __restrict__ cnt) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    cnt[i] = row[i] == col[i] ? 1 : 2;
+}
+
+__global__ void k_rvec(int64_t n, const int32_t* __restrict__ up, const double* __restrict__ centre,
+                       const double* __restrict__ centre_c, double* __restrict__ rvec) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int32_t c = up[k];
+    for (int q = 0; q < 3; q++) rvec[3 * k + q] = c >= 0 ? centre[3 * k + q] - centre_c[3 * (int64_t)c + q] : 0.0;
+}
+
+// ---- dense top ---------------------------------------------------------------------
+__global__ void k_dense_from_bsr(int top_i, const int32_t* __restrict__ top, const int64_t* __restrict__ pstart,
+                                 const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                 const double* __restrict__ val, double* __restrict__ A) {
+    int p = top[top_i];
+    int64_t k0 = pstart[p], k1 = pstart[p + 1];
+    int64_t n = 6 * (k1 - k0);
+    for (int64_t k = k0 + blockIdx.x; k < k1; k += gridDim.x)
+        for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
+            int64_t j = col[e];
+            for (int t = threadIdx.x; t < 36; t += blockDim.x) {
+                int r = t / 6, c = t % 6;
+                A[(6 * (k - k0) + r) * n + 6 * (j - k0) + c] = val[36 * e + t];
+            }
+        }
+}
+
+// Left-looking Cholesky in the reference's order (bodies.rs:307-313), then
+// X = L^-1 by columns and Kinv = X' X. One block per piece.
+__global__ void __launch_bounds__(1024) k_cholesky_inverse(int n, double* __restrict__ A, double* __restrict__ X,
+                                                           double* __restrict__ Kinv, int32_t* __restrict__ status,
+                                                           int piece) {
+    __shared__ double red[1024];
+    __shared__ double dsh;
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    for (int j = 0; j < n; j++) {
+        double s = 0.0;
+        for (int k = threadIdx.x; k < j; k += blockDim.x) s = fma(A[(int64_t)j * n + k], A[(int64_t)j * n + k], s);
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            double v = A[(int64_t)j * n + j] - red[0];
+            if (!(v > 0.0)) bad = 1;
+            dsh = sqrt(v);
+            A[(int64_t)j * n + j] = dsh;
+        }
+        __syncthreads();
+        double d = dsh;
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+            double t = 0.0;
+            for (int k = 0; k < j; k++) t = fma(A[(int64_t)i * n + k], A[(int64_t)j * n + k], t);
+            A[(int64_t)i * n + j] = (A[(int64_t)i * n + j] - t) / d;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && bad) atomicMax(status + piece, (int)SC_NOT_SPD);
+    // X = L^-1, column j by thread j
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        for (int i = 0; i < j; i++) X[(int64_t)i * n + j] = 0.0;
+        X[(int64_t)j * n + j] = 1.0 / A[(int64_t)j * n + j];
+        for (int i = j + 1; i < n; i++) {
+            double t = 0.0;
+            for (int k = j; k < i; k++) t = fma(A[(int64_t)i * n + k], X[(int64_t)k * n + j], t);
+            X[(int64_t)i * n + j] = -t / A[(int64_t)i * n + i];
+        }
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+        int i = (int)(e / n), j = (int)(e % n);
+        int k0 = i > j ? i : j;
+        double t = 0.0;
+        for (int k = k0; k < n; k++) t = fma(X[(int64_t)k * n + i], X[(int64_t)k * n + j], t);
+        Kinv[e] = t;
+    }
+}
+
+__global__ void k_fill_i32(int64_t n, int32_t* __restrict__ a, int32_t v) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+__global__ void k_iota32(int64_t n, int32_t* __restrict__ v) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int32_t)i;
+}
+__global__ void k_iota64(int64_t n, int64_t* __restrict__ v) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+__global__ void k_row_of_entry(int64_t n, const int64_t* __restrict__ rowptr, int32_t* __restrict__ row) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) row[e] = (int32_t)k;
+}
+
+int bits_for(int64_t v) {
+    int b = 1;
+    while (b < 63 && (int64_t(1) << b) <= v) b++;
+    return b;
+}
+
+int64_t d2h_i64(Context& ctx, const int64_t* p) {
+    int64_t v = 0;
+    SC_CK(cudaMemcpyAsync(&v, p, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx.stream));
+    SC_CK(cudaStreamSynchronize(ctx.stream));
+    return v;
+}
+
+void exclusive_scan(Context& ctx, const int64_t* in, int64_t* out, int64_t n) {
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, ctx.stream);
+    cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, in, out, n, ctx.stream);
+}
+
+// Sorted, unique (row << 32 | col) keys -> CSR pattern.
+void keys_to_csr(Context& ctx, DBuf<uint64_t>& keys, int64_t nkeys, int64_t nrows, int64_t ncols, DBuf<int64_t>& rowptr,
+                 DBuf<int32_t>& col, int64_t& nnz) {
+    cudaStream_t st = ctx.stream;
+    MemStats* ms = &ctx.mem;
+    DBuf<uint64_t> sorted;
+    sorted.alloc(std::max<int64_t>(nkeys, 1), st, ms);
+    int end_bit = 32 + bits_for(nrows);
+    size_t tb = 0;
+    if (nkeys > 0) {
+        cub::DeviceRadixSort::SortKeys(nullptr, tb, keys.get(), sorted.get(), nkeys, 0, end_bit, st);
+        cub::DeviceRadixSort::SortKeys(ctx.cub_scratch(tb), tb, keys.get(), sorted.get(), nkeys, 0, end_bit, st);
+    }
+    keys.release();
+    DBuf<uint64_t> uniq;
+    uniq.alloc(std::max<int64_t>(nkeys, 1), st, ms);
+    DBuf<int64_t> nsel;
+    nsel.alloc(1, st, ms);
+    nsel.zero();
+    if (nkeys > 0) {
+        cub::DeviceSelect::Unique(nullptr, tb, sorted.get(), uniq.get(), nsel.get(), nkeys, st);
+        cub::DeviceSelect::Unique(ctx.cub_scratch(tb), tb, sorted.get(), uniq.get(), nsel.get(), nkeys, st);
+    }
+    nnz = d2h_i64(ctx, nsel.get());
+    sorted.release();
+    col.alloc(std::max<int64_t>(nnz, 1), st, ms);
+    DBuf<int32_t> rows;
+    rows.alloc(std::max<int64_t>(nnz, 1), st, ms);
+    k_unpack_pattern<<<grid_for(nnz, 256), 256, 0, st>>>(nnz, uniq.get(), col.get(), rows.get());
+    SC_LAUNCH_CK();
+    rowptr.alloc(nrows + 1, st, ms);
+    k_offsets_from_sorted<<<grid_for(nnz + 1, 256), 256, 0, st>>>(nnz, rows.get(), nrows, rowptr.get());
+    SC_LAUNCH_CK();
+    (void)ncols;
+}
+
+}  // namespace
+
+void setup_chunks(Context& ctx, Level& L, int32_t np) {
+    std::vector<int64_t> lo;
+    std::vector<int32_t> cp;
+    std::vector<int64_t> pc(np + 1, 0);
+    for (int p = 0; p < np; p++) {
+        pc[p] = (int64_t)cp.size();
+        for (int64_t a = L.pstart[p]; a < L.pstart[p + 1]; a += CHUNK) {
+            lo.push_back(a);
+            cp.push_back(p);
+        }
+    }
+    pc[np] = (int64_t)cp.size();
+    L.nchunks = (int64_t)cp.size();
+    lo.push_back(L.n);
+    L.chunk_lo.alloc(lo.size(), ctx.stream, &ctx.mem);
+    L.chunk_lo.upload(lo.data(), lo.size());
+    L.chunk_piece.alloc(std::max<size_t>(cp.size(), 1), ctx.stream, &ctx.mem);
+    L.chunk_piece.upload(cp.data(), cp.size());
+    L.piece_chunk.alloc(np + 1, ctx.stream, &ctx.mem);
+    L.piece_chunk.upload(pc.data(), np + 1);
+}
+
+void invert_blocks(Context& ctx, Level& L, int32_t* status) {
+    L.inv.alloc(36 * L.n, ctx.stream, &ctx.mem);
+    k_find_diag_invert<<<grid_for(L.n, 128), 128, 0, ctx.stream>>>(L.n, L.rowptr.get(), L.col.get(), L.val.get(),
+                                                                   L.inv.get(), L.piece.get(), status);
+    SC_LAUNCH_CK();
+}
+
+void invert_blocks(Context& ctx, Level& L) { invert_blocks(ctx, L, nullptr); }
+
+// step = 4/3 / lambda_max(D^-1 K) per piece (bodies.rs:174, 180-190)
+static void smoother_step(Context& ctx, Batch& b, int l) {
+    Level& L = b.levels[l];
+    cudaStream_t st = ctx.stream;
+    int np = b.npieces;
+    DBuf<double> v, w, t;
+    v.alloc(6 * L.n, st, &ctx.mem);
+    w.alloc(6 * L.n, st, &ctx.mem);
+    t.alloc(6 * L.n, st, &ctx.mem);
+    DBuf<double> ww, vv, most;
+    ww.alloc(np, st, &ctx.mem);
+    vv.alloc(np, st, &ctx.mem);
+    most.alloc(np, st, &ctx.mem);
+    k_power_start<<<grid_for(L.n, 256), 256, 0, st>>>(L.n, L.pstart_d.get(), L.piece.get(), v.get());
+    SC_LAUNCH_CK();
+    for (int it = 0; it < 12; it++) {
+        level_apply<double>(ctx, b, l, v.get(), t.get());
+        jacobi<double>(ctx, L.n, L.inv.get(), t.get(), w.get(), nullptr, L.piece.get(), nullptr, nullptr);
+        seg_dot_t<double>(ctx, L, w.get(), w.get(), ww.get());
+        seg_dot_t<double>(ctx, L, v.get(), v.get(), vv.get());
+        k_power_most<<<grid_for(np, 128), 128, 0, st>>>(np, ww.get(), vv.get(), most.get());
+        SC_LAUNCH_CK();
+        k_power_scale<<<grid_for(6 * L.n, 256), 256, 0, st>>>(L.n, L.piece.get(), ww.get(), w.get(), v.get());
+        SC_LAUNCH_CK();
+    }
+    L.step.alloc(np, st, &ctx.mem);
+    k_step<<<grid_for(np, 128), 128, 0, st>>>(np, most.get(), L.step.get());
+    SC_LAUNCH_CK();
+}
+
+void gather_i32(Context& ctx, int64_t n, const int64_t* idx, const int32_t* src, int32_t* dst);
+
+// The next level from level l (bodies.rs:228-282); returns false when every piece tops
+// out at level l.
+static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_options& opt) {
+    cudaStream_t st = ctx.stream;
+    MemStats* ms = &ctx.mem;
+    int np = b.npieces;
+    Level& F = b.levels[l];
+    int64_t n = F.n;
+    // which pieces go on: more than FEW parts (bodies.rs:447)
+    std::vector<int32_t> active(np, 0);
+    for (int p = 0; p < np; p++) active[p] = (F.pstart[p + 1] - F.pstart[p]) > opt.few ? 1 : 0;
+    DBuf<int32_t> active_d;
+    active_d.alloc(np, st, ms);
+    active_d.upload(active.data(), np);
+    // bodies_of (bodies.rs:472-496)
+    int64_t mask = ~((int64_t(1) << octree_level) - 1);
+    DBuf<int32_t> label;
+    label.alloc(n, st, ms);
+    k_label_init<<<grid_for(n, 256), 256, 0, st>>>(n, label.get());
+    SC_LAUNCH_CK();
+    DBuf<int32_t> changed;
+    changed.alloc(1, st, ms);
+    for (int it = 0; it < 100000; it++) {
+        changed.zero();
+        k_label_sweep<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.site.get(), mask,
+                                                        active_d.get(), F.piece.get(), label.get(), changed.get());
+        SC_LAUNCH_CK();
+        k_label_jump<<<grid_for(n, 256), 256, 0, st>>>(n, label.get());
+        SC_LAUNCH_CK();
+        int32_t ch = 0;
+        SC_CK(cudaMemcpyAsync(&ch, changed.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SC_CK(cudaStreamSynchronize(st));
+        if (!ch) break;
+    }
+    DBuf<int64_t> root, id;
+    root.alloc(n + 1, st, ms);
+    id.alloc(n + 1, st, ms);
+    DBuf<int32_t> bodies_d;
+    bodies_d.alloc(np, st, ms);
+    bodies_d.zero();
+    SC_CK(cudaMemsetAsync(root.get() + n, 0, sizeof(int64_t), st));
+    k_roots<<<grid_for(n, 256), 256, 0, st>>>(n, label.get(), F.piece.get(), root.get(), bodies_d.get());
+    SC_LAUNCH_CK();
+    std::vector<int32_t> bodies = bodies_d.to_host();
+    bool any = false;
+    for (int p = 0; p < np; p++) {
+        if (active[p] && bodies[p] == (int32_t)(F.pstart[p + 1] - F.pstart[p])) active[p] = 0;  // bodies.rs:453-455
+        any = any || active[p];
+    }
+    F.top_of_part.alloc(n, st, ms);
+    F.up.alloc(n, st, ms);
+    if (!any) {
+        k_fill_i32<<<grid_for(n, 256), 256, 0, st>>>(n, F.top_of_part.get(), 1);
+        k_fill_i32<<<grid_for(n, 256), 256, 0, st>>>(n, F.up.get(), -1);
+        SC_LAUNCH_CK();
+        return false;
+    }
+    active_d.upload(active.data(), np);
+    k_mask_roots<<<grid_for(n, 256), 256, 0, st>>>(n, F.piece.get(), active_d.get(), root.get());
+    SC_LAUNCH_CK();
+    exclusive_scan(ctx, root.get(), id.get(), n + 1);
+    int64_t nc = d2h_i64(ctx, id.get() + n);
+    k_up<<<grid_for(n, 256), 256, 0, st>>>(n, label.get(), id.get(), F.piece.get(), active_d.get(), F.up.get(),
+                                           F.top_of_part.get());
+    SC_LAUNCH_CK();
+    label.release();
+    root.release();
+    id.release();
+
+    Level C;
+    C.n = nc;
+    C.pstart.assign(np + 1, 0);
+    for (int p = 0; p < np; p++) C.pstart[p + 1] = C.pstart[p] + (active[p] ? bodies[p] : 0);
+    C.pstart_d.alloc(np + 1, st, ms);
+    C.pstart_d.upload(C.pstart.data(), np + 1);
+    // members of each body in part order (stable sort by body)
+    DBuf<int32_t> mem_part, mem_body;
+    {
+        DBuf<int32_t> ids;
+        ids.alloc(n, st, ms);
+        k_iota32<<<grid_for(n, 256), 256, 0, st>>>(n, ids.get());
+        SC_LAUNCH_CK();
+        DBuf<int32_t> keys_in;
+        keys_in.alloc(n, st, ms);
+        // parts of stopped pieces (up = -1) sort first as 0xffffffff... use unsigned keys
+        SC_CK(cudaMemcpyAsync(keys_in.get(), F.up.get(), n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+        mem_part.alloc(n, st, ms);
+        mem_body.alloc(n, st, ms);
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint32_t*)keys_in.get(), (uint32_t*)mem_body.get(), ids.get(),
+                                        mem_part.get(), n, 0, 32, st);
+        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, (uint32_t*)keys_in.get(), (uint32_t*)mem_body.get(),
+                                        ids.get(), mem_part.get(), n, 0, 32, st);
+    }
+    // active parts are the first m entries (up < 2^31 sorts below 0xffffffff)
+    int64_t m = 0;
+    for (int p = 0; p < np; p++)
+        if (active[p]) m += F.pstart[p + 1] - F.pstart[p];
+    DBuf<int64_t> moff;
+    moff.alloc(nc + 1, st, ms);
+    k_offsets_from_sorted<<<grid_for(m + 1, 256), 256, 0, st>>>(m, mem_body.get(), nc, moff.get());
+    SC_LAUNCH_CK();
+    C.centre.alloc(3 * nc, st, ms);
+    C.site.alloc(3 * nc, st, ms);
+    C.piece.alloc(nc, st, ms);
+    k_centroid<<<grid_for(nc, 128), 128, 0, st>>>(nc, moff.get(), mem_part.get(), F.centre.get(), F.site.get(),
+                                                  F.piece.get(), C.centre.get(), C.site.get(), C.piece.get());
+    SC_LAUNCH_CK();
+    mem_part.release();
+    mem_body.release();
+    moff.release();
+    DBuf<double> rvec;
+    rvec.alloc(3 * n, st, ms);
+    k_rvec<<<grid_for(n, 256), 256, 0, st>>>(n, F.up.get(), F.centre.get(), C.centre.get(), rvec.get());
+    SC_LAUNCH_CK();
+
+    // --- P pattern and values
+    DBuf<int64_t> cnt, off;
+    cnt.alloc(n + 1, st, ms);
+    off.alloc(n + 1, st, ms);
+    SC_CK(cudaMemsetAsync(cnt.get() + n, 0, sizeof(int64_t), st));
+    k_count_P<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.up.get(), cnt.get());
+    SC_LAUNCH_CK();
+    exclusive_scan(ctx, cnt.get(), off.get(), n + 1);
+    int64_t tot = d2h_i64(ctx, off.get() + n);
+    {
+        DBuf<uint64_t> keys;
+        keys.alloc(std::max<int64_t>(tot, 1), st, ms);
+        k_fill_P<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.up.get(), off.get(), keys.get());
+        SC_LAUNCH_CK();
+        keys_to_csr(ctx, keys, tot, n, nc, F.prow, F.pcol, F.pnnz);
+    }
+    F.pval.alloc(36 * std::max<int64_t>(F.pnnz, 1), st, ms);
+    F.pval.zero();
+    k_num_P<<<grid_for(n * 32, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.val.get(), F.up.get(),
+                                                   rvec.get(), F.inv.get(), F.step.get(), F.piece.get(), F.prow.get(),
+                                                   F.pcol.get(), F.pval.get());
+    SC_LAUNCH_CK();
+    rvec.release();
+    // P transposed: entries sorted by column, stable (fine-row order within a column)
+    {
+        DBuf<int32_t> prow_of;
+        prow_of.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
+        k_row_of_entry<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), prow_of.get());
+        SC_LAUNCH_CK();
+        DBuf<int64_t> ent;
+        ent.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
+        k_iota64<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, ent.get());
+        SC_LAUNCH_CK();
+        DBuf<int32_t> ccol;
+        ccol.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
+        F.tent.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, F.pcol.get(), ccol.get(), ent.get(), F.tent.get(), F.pnnz, 0,
+                                        bits_for(nc), st);
+        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, F.pcol.get(), ccol.get(), ent.get(), F.tent.get(),
+                                        F.pnnz, 0, bits_for(nc), st);
+        F.tptr.alloc(nc + 1, st, ms);
+        k_offsets_from_sorted<<<grid_for(F.pnnz + 1, 256), 256, 0, st>>>(F.pnnz, ccol.get(), nc, F.tptr.get());
+        SC_LAUNCH_CK();
+        F.trow.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
+        // trow[t] = row of entry tent[t]
+        gather_i32(ctx, F.pnnz, F.tent.get(), prow_of.get(), F.trow.get());
+    }
+    // --- K P
+    DBuf<int64_t> kprow;
+    DBuf<int32_t> kpcol;
+    int64_t kpnnz = 0;
+    k_count_KP<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.prow.get(), F.up.get(), cnt.get());
+    SC_LAUNCH_CK();
+    exclusive_scan(ctx, cnt.get(), off.get(), n + 1);
+    tot = d2h_i64(ctx, off.get() + n);
+    {
+        DBuf<uint64_t> keys;
+        keys.alloc(std::max<int64_t>(tot, 1), st, ms);
+        k_fill_KP<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.prow.get(), F.pcol.get(),
+                                                    F.up.get(), off.get(), keys.get());
+        SC_LAUNCH_CK();
+        keys_to_csr(ctx, keys, tot, n, nc, kprow, kpcol, kpnnz);
+    }
+    DBuf<double> kpval;
+    kpval.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
+    kpval.zero();
+    k_num_KP<<<grid_for(n * 32, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.val.get(), F.up.get(),
+                                                    F.prow.get(), F.pcol.get(), F.pval.get(), kprow.get(), kpcol.get(),
+                                                    kpval.get());
+    SC_LAUNCH_CK();
+    // --- P' K P, upper triangle (d >= c)
+    DBuf<int64_t> urow;
+    DBuf<int32_t> ucol;
+    int64_t unnz = 0;
+    {
+        DBuf<int64_t> ecnt, eoff;
+        ecnt.alloc(F.pnnz + 1, st, ms);
+        eoff.alloc(F.pnnz + 1, st, ms);
+        SC_CK(cudaMemsetAsync(ecnt.get() + F.pnnz, 0, sizeof(int64_t), st));
+        k_count_C<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), F.pcol.get(), kprow.get(), kpcol.get(), ecnt.get());
+        SC_LAUNCH_CK();
+        exclusive_scan(ctx, ecnt.get(), eoff.get(), F.pnnz + 1);
+        tot = d2h_i64(ctx, eoff.get() + F.pnnz);
+        DBuf<uint64_t> keys;
+        keys.alloc(std::max<int64_t>(tot, 1), st, ms);
+        k_fill_C<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), F.pcol.get(), kprow.get(), kpcol.get(), eoff.get(),
+                                                   keys.get());
+        SC_LAUNCH_CK();
+        keys_to_csr(ctx, keys, tot, nc, nc, urow, ucol, unnz);
+    }
+    DBuf<double> uval;
+    uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
+    uval.zero();
+    k_num_C<<<grid_for(nc * 32, 256), 256, 0, st>>>(nc, F.tptr.get(), F.tent.get(), F.trow.get(), F.pval.get(),
+                                                    kprow.get(), kpcol.get(), kpval.get(), urow.get(), ucol.get(),
+                                                    uval.get());
+    SC_LAUNCH_CK();
+    kpval.release();
+    kprow.release();
+    kpcol.release();
+    // --- full symmetric storage
+    {
+        DBuf<int32_t> urows;
+        urows.alloc(std::max<int64_t>(unnz, 1), st, ms);
+        k_row_of_entry<<<grid_for(nc, 256), 256, 0, st>>>(nc, urow.get(), urows.get());
+        SC_LAUNCH_CK();
+        DBuf<int64_t> mc, mo;
+        mc.alloc(unnz + 1, st, ms);
+        mo.alloc(unnz + 1, st, ms);
+        SC_CK(cudaMemsetAsync(mc.get() + unnz, 0, sizeof(int64_t), st));
+        k_mirror_count<<<grid_for(unnz, 256), 256, 0, st>>>(unnz, urows.get(), ucol.get(), mc.get());
+        SC_LAUNCH_CK();
+        exclusive_scan(ctx, mc.get(), mo.get(), unnz + 1);
+        int64_t fn = d2h_i64(ctx, mo.get() + unnz);
+        DBuf<uint64_t> keys, keys_s;
+        DBuf<int64_t> src, src_s;
+        keys.alloc(fn, st, ms);
+        src.alloc(fn, st, ms);
+        k_mirror_keys<<<grid_for(unnz, 256), 256, 0, st>>>(unnz, urows.get(), ucol.get(), keys.get(), src.get(), mo.get());
+        SC_LAUNCH_CK();
+        keys_s.alloc(fn, st, ms);
+        src_s.alloc(fn, st, ms);
+        size_t tb = 0;
+        int end_bit = 32 + bits_for(nc);
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys_s.get(), src.get(), src_s.get(), fn, 0, end_bit, st);
+        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, keys.get(), keys_s.get(), src.get(), src_s.get(), fn, 0,
+                                        end_bit, st);
+        keys.release();
+        src.release();
+        C.nnzb = fn;
+        C.col.alloc(fn, st, ms);
+        DBuf<int32_t> rows;
+        rows.alloc(fn, st, ms);
+        k_unpack_pattern<<<grid_for(fn, 256), 256, 0, st>>>(fn, keys_s.get(), C.col.get(), rows.get());
+        SC_LAUNCH_CK();
+        C.rowptr.alloc(nc + 1, st, ms);
+        k_offsets_from_sorted<<<grid_for(fn + 1, 256), 256, 0, st>>>(fn, rows.get(), nc, C.rowptr.get());
+        SC_LAUNCH_CK();
+        C.val.alloc(36 * fn, st, ms);
+        k_mirror_vals<<<grid_for(36 * fn, 256), 256, 0, st>>>(fn, src_s.get(), uval.get(), C.val.get());
+        SC_LAUNCH_CK();
+    }
+    b.levels.push_back(std::move(C));
+    return true;
+}
+
+void gather_i32(Context& ctx, int64_t n, const int64_t* idx, const int32_t* src, int32_t* dst);
+
+static void build_top(Context& ctx, Batch& b, int l, const std::vector<int32_t>& pieces) {
+    Level& L = b.levels[l];
+    cudaStream_t st = ctx.stream;
+    L.top_h = pieces;
+    if (pieces.empty()) return;
+    L.top.alloc(pieces.size(), st, &ctx.mem);
+    L.top.upload(pieces.data(), pieces.size());
+    std::vector<int64_t> off(pieces.size() + 1, 0);
+    for (size_t i = 0; i < pieces.size(); i++) {
+        int64_t nn = 6 * (L.pstart[pieces[i] + 1] - L.pstart[pieces[i]]);
+        off[i + 1] = off[i] + nn * nn;
+    }
+    L.kinv_off.alloc(off.size(), st, &ctx.mem);
+    L.kinv_off.upload(off.data(), off.size());
+    L.kinv.alloc(std::max<int64_t>(off.back(), 1), st, &ctx.mem);
+    int64_t maxnn = 1;
+    for (size_t i = 0; i < pieces.size(); i++) maxnn = std::max(maxnn, off[i + 1] - off[i]);
+    DBuf<double> A, X;
+    A.alloc(maxnn, st, &ctx.mem);
+    X.alloc(maxnn, st, &ctx.mem);
+    for (size_t i = 0; i < pieces.size(); i++) {
+        int64_t nn = off[i + 1] - off[i];
+        int n = (int)(6 * (L.pstart[pieces[i] + 1] - L.pstart[pieces[i]]));
+        if (n == 0) continue;
+        SC_CK(cudaMemsetAsync(A.get(), 0, nn * sizeof(double), st));
+        k_dense_from_bsr<<<64, 64, 0, st>>>((int)i, L.top.get(), L.pstart_d.get(), L.rowptr.get(), L.col.get(),
+                                             L.val.get(), A.get());
+        SC_LAUNCH_CK();
+        k_cholesky_inverse<<<1, 1024, 0, st>>>(n, A.get(), X.get(), L.kinv.get() + off[i], b.status_d.get(), pieces[i]);
+        SC_LAUNCH_CK();
+    }
+}
+
+template <class T>
+__global__ void k_gather(int64_t n, const int64_t* __restrict__ idx, const T* __restrict__ src, T* __restrict__ dst) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i]];
+}
+void gather_i32(Context& ctx, int64_t n, const int64_t* idx, const int32_t* src, int32_t* dst) {
+    if (n <= 0) return;
+    k_gather<int32_t><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, idx, src, dst);
+    SC_LAUNCH_CK();
+}
+
+void to_float(Context& ctx, const DBuf<double>& a, DBuf<float>& b) {
+    b.alloc(a.size(), ctx.stream, &ctx.mem);
+    if (a.size()) {
+        k_to_float<<<grid_for((int64_t)a.size(), 256), 256, 0, ctx.stream>>>((int64_t)a.size(), a.get(), b.get());
+        SC_LAUNCH_CK();
+    }
+}
+
+// Levels for every piece: while a piece has more than FEW parts and its bodies are fewer
+// than its parts, coarsen it (bodies.rs:444-461); then factor each piece's top.
+void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
+    auto t0 = std::chrono::steady_clock::now();
+    int np = b.npieces;
+    b.levels.reserve(SC_MAX_LEVELS + 1);
+    b.status_d.alloc(np, ctx.stream, &ctx.mem);
+    b.status_d.zero();
+    int octree = b.base_level;
+    for (int l = 0;; l++) {
+        Level& L = b.levels[l];
+        setup_chunks(ctx, L, np);
+        invert_blocks(ctx, L, b.status_d.get());
+        smoother_step(ctx, b, l);
+        octree += 1;
+        bool more = l + 1 < SC_MAX_LEVELS && coarsen(ctx, b, l, octree, opt);
+        Level& F = b.levels[l];  // reference may have moved
+        // pieces whose top is this level
+        std::vector<int32_t> tops;
+        {
+            std::vector<int32_t> topp = F.top_of_part.size() ? F.top_of_part.to_host() : std::vector<int32_t>();
+            for (int p = 0; p < np; p++) {
+                int64_t a = F.pstart[p], e = F.pstart[p + 1];
+                if (a == e) continue;  // not on this level
+                bool top = !more || topp.empty() || topp[a];
+                if (top) tops.push_back(p);
+            }
+        }
+        build_top(ctx, b, l, tops);
+        if (!more) break;
+    }
+    b.piece_levels.assign(np, 0);
+    for (size_t l = 0; l < b.levels.size(); l++)
+        for (int p = 0; p < np; p++)
+            if (b.levels[l].pstart[p + 1] > b.levels[l].pstart[p]) b.piece_levels[p] = (int32_t)l + 1;
+    SC_CK(cudaStreamSynchronize(ctx.stream));
+    b.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace sc

@@ -1,0 +1,180 @@
+// The statics solve on the device: a batch of independent pieces, each with its own
+// smoothed-aggregation hierarchy (statics/src/bodies.rs:123-282), solved by conjugate
+// gradients (bodies.rs:338-373) preconditioned by V-cycles (bodies.rs:377-403), all
+// pieces advanced together by batched kernels. A single structure is a batch of one.
+//
+// Layout in HBM, per level: parts of piece 0, then piece 1, ... (pieces contiguous);
+// six-vectors as 6 consecutive values per part (48 B FP64, 24 B FP32); operators as
+// block-sparse rows of 6x6 blocks (36 values, row-major), both triangles stored, columns
+// sorted; level 0 of voxel pieces is matrix-free (a per-cell template, see grid.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sc {
+
+constexpr int CHUNK = 4096;  // parts per reduction chunk (chunks never cross pieces)
+
+// Level 0 of voxel pieces: the cells, and for each part its two cells.
+struct Grid0 {
+    int64_t ncells = 0;
+    double s = 0.125;           // spacing (statics/src/lattice.rs:16, 34-36)
+    DBuf<int4> cell;            // 2 int4 per free cell: part ids of slots 0..5 (-1 held), k bits, 0
+    DBuf<int32_t> perm;         // parts grouped by axis, each group padded to a multiple of 32 with -1
+    int64_t axis_off[4] = {0, 0, 0, 0};
+    DBuf<int32_t> cella, cellb; // per part: its lesser cell (node is that cell's + face) and greater cell; -1 if not free
+    DBuf<int8_t> axis;          // per part
+    DBuf<int64_t> cell_flat;    // per free cell: its flat index in the batch's concatenated grids
+    std::vector<int64_t> grid_off;  // per piece: first flat cell index; npieces + 1
+};
+
+struct Level {
+    int64_t n = 0;                   // parts
+    int64_t nnzb = 0;                // stored blocks
+    std::vector<int64_t> pstart;     // host copy: piece p's parts are [pstart[p], pstart[p+1])
+    DBuf<int64_t> pstart_d;
+    DBuf<int32_t> piece;             // part -> piece
+    DBuf<double> centre;             // 3 per part
+    DBuf<int64_t> site;              // 3 per part: a member node's lesser cell, level-0 units
+
+    bool matrix_free = false;        // level 0 of voxel pieces: apply through Grid0
+    DBuf<int64_t> rowptr;
+    DBuf<int32_t> col;
+    DBuf<double> val;
+    DBuf<float> val32;
+    DBuf<double> inv;                // inverse of each part's own block
+    DBuf<float> inv32;
+    DBuf<double> step;               // per piece: 4/3 / lambda_max(D^-1 K)
+
+    // reductions over each piece's parts
+    int64_t nchunks = 0;
+    DBuf<int64_t> chunk_lo;          // nchunks + 1 bounds
+    DBuf<int32_t> chunk_piece;
+    DBuf<int64_t> piece_chunk;       // per piece: first chunk; npieces + 1
+
+    // to the next level (absent at the last)
+    DBuf<int32_t> up;                // body at the next level, -1 where the piece tops out here
+    int64_t pnnz = 0;
+    DBuf<int64_t> prow;              // P: n rows
+    DBuf<int32_t> pcol;
+    DBuf<double> pval;
+    DBuf<float> pval32;
+    DBuf<int64_t> tptr;              // P transposed: coarse row c's entries tent[tptr[c]..tptr[c+1])
+    DBuf<int64_t> tent;              //   (index into pcol / pval), in fine-row order
+    DBuf<int32_t> trow;              //   and the fine row of each
+
+    // pieces solved directly at this level
+    std::vector<int32_t> top_h;
+    DBuf<int32_t> top;               // piece ids
+    DBuf<int64_t> kinv_off;          // per top piece: offset of its dense inverse
+    DBuf<double> kinv;
+    DBuf<int32_t> top_of_part;       // per part: 1 if its piece tops out here
+
+    // cycle work vectors (levels >= 1 keep r and z for the level above)
+    DBuf<double> r, x, left, z;
+    DBuf<float> r32, x32, left32, z32;
+};
+
+struct Batch {
+    int32_t npieces = 0;
+    std::vector<Level> levels;
+    Grid0 grid;                      // when level 0 is matrix-free
+    std::vector<int32_t> piece_levels;  // per piece: number of levels
+    std::vector<int32_t> piece_status;
+    DBuf<int32_t> status_d;          // per piece sc_status from device checks
+    std::vector<int64_t> node_count; // per piece: nodes of its lattice
+    DBuf<int64_t> node_start;        // per piece: first node (output motions)
+    DBuf<int32_t> part_node;         // per level-0 part: its node (within the piece)
+    DBuf<double> loads;              // level-0 right-hand side, 6 per part
+    DBuf<double> mass;               // per part (voxel pieces)
+    double setup_ms = 0;
+    int32_t base_level = 0;          // Lattice::level of level 0 (octree keys start one above)
+};
+
+struct Context;
+
+// --- grid.cu ------------------------------------------------------------------------
+// Build level 0 (numbering, cells, centres, sites, loads, assembled blocks for setup)
+// for voxel pieces already on the device.
+void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks);
+template <class T>
+void stencil_apply(Context& ctx, const Batch& b, const T* x, T* y, const int32_t* skip_row, const int32_t* done);
+template <class T>
+void stencil_residual(Context& ctx, const Batch& b, const T* x, const T* r, T* y, const int32_t* skip_row,
+                      const int32_t* done);
+void grid_cell_energy(Context& ctx, const Batch& b, const double* x, double* energy_cells);
+
+// --- lattice.cu -----------------------------------------------------------------------
+void lattice_level0(Context& ctx, Batch& b, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,
+                    const double* loads);
+
+// --- hierarchy.cu ---------------------------------------------------------------------
+void setup_chunks(Context& ctx, Level& L, int32_t npieces);
+void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt);
+void invert_blocks(Context& ctx, Level& L);
+void to_float(Context& ctx, const DBuf<double>& a, DBuf<float>& b);
+
+// --- cycle.cu -------------------------------------------------------------------------
+struct SolveStats {
+    std::vector<int64_t> iterations;
+    std::vector<int64_t> refinements;
+    std::vector<double> residual;
+    double work = 0;
+};
+void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st);
+void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st);
+template <class T>
+void level_apply(Context& ctx, const Batch& b, int l, const T* x, T* y);
+void seg_dot(Context& ctx, const Level& L, const double* a, const double* bb, double* out_per_piece);
+
+// Per-family kernel timing with CUDA events on the context's stream.
+struct Profiler {
+    uint32_t mask = 0;
+    struct Pending {
+        int fam;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    int64_t launches[SC_FAM_COUNT] = {};
+    double ms[SC_FAM_COUNT] = {};
+    double bytes[SC_FAM_COUNT] = {};
+    cudaEvent_t get();
+    void flush();
+    void reset();
+    ~Profiler();
+};
+
+struct Context;
+// Records a start event now and a stop event at scope exit, for family `fam`.
+struct ProfScope {
+    Context* c = nullptr;
+    int fam = 0;
+    double bytes = 0;
+    cudaEvent_t a = nullptr;
+    ProfScope(Context& ctx, int family, double algorithmic_bytes);
+    ~ProfScope();
+};
+
+struct Context {
+    int device = 0;
+    Profiler prof;
+    cudaStream_t stream = nullptr;
+    MemStats mem;
+    std::string last_error;
+    // scratch for reductions
+    DBuf<double> partial;
+    DBuf<double> scal;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    std::unique_ptr<Batch> last;     // the last solve's hierarchy (parity queries)
+    void* cub_scratch(size_t bytes);
+    ~Context();
+};
+
+}  // namespace sc

@@ -1,0 +1,255 @@
+"""GPU path against the oracle, through the C ABI: bit-exact numbering and hierarchy,
+operator values, motions, mixed precision, batches, general lattices, statuses."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import statics_cuda as sc
+from oracle import oracle as O
+
+from helpers import lattice_dict, oracle_lattice, piece, rel, z_loads
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# FP64 operator values differ from the oracle's only by summation order.
+OP_TOL64 = 1e-12
+OP_TOL32 = 2e-6
+# Displacements at 1e-8 relative residual: both solves are within ~kappa * 1e-8 of the
+# exact answer; the GPU's differs from the oracle's by far less.
+DISP_TOL = 1e-6
+
+
+def special_pieces():
+    out = []
+    st = np.zeros((1, 1, 2), np.uint8)
+    st[0, 0, 0], st[0, 0, 1] = 2, 1  # one free cell on the support
+    out.append(("one cell", st, np.ones(st.shape, np.float32)))
+    st = np.zeros((1, 1, 6), np.uint8)
+    st[0, 0, 0], st[0, 0, 1:] = 2, 1  # a column
+    out.append(("column", st, np.linspace(0.5, 2, st.size, dtype=np.float32).reshape(st.shape)))
+    st = np.zeros((5, 4, 3), np.uint8)
+    st[:, :, 0] = 2
+    st[1:4, 1:3, 1:] = 1  # a block, empty ring around it
+    out.append(("block", st, np.full(st.shape, 1.5, np.float32)))
+    st = np.zeros((4, 4, 4), np.uint8)
+    st[:, :, 0] = 2
+    st[:, :, 1] = 1
+    st[1, 1, 2] = 2  # a held cell in the middle of free ones
+    st[2, 2, 2:] = 1
+    out.append(("held inside", st, np.full(st.shape, 0.7, np.float32)))
+    return out
+
+
+@pytest.mark.parametrize("n,seed", [(8, 0), (12, 3), (16, 1), (20, 5)])
+def test_operator_matches_level_new_apply(solver, n, seed):
+    st, k = piece(n, seed, shape=(n, n + 3, n - 2))
+    lat = oracle_lattice(st, k)
+    _, parts = sc.grid_count(st)
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((parts, 6))
+    want = lat.level0_apply(x)
+    got = solver.grid_apply(st, k, x, sc.FP64)
+    assert rel(got, want) < OP_TOL64
+    got32 = solver.grid_apply(st, k, x, sc.MIXED)
+    assert rel(got32, want) < OP_TOL32
+
+
+@pytest.mark.parametrize("name,st,k", special_pieces(), ids=[p[0] for p in special_pieces()])
+def test_operator_special_pieces(solver, name, st, k):
+    lat = oracle_lattice(st, k)
+    _, parts = sc.grid_count(st)
+    x = np.random.default_rng(1).standard_normal((parts, 6))
+    assert rel(solver.grid_apply(st, k, x), lat.level0_apply(x)) < OP_TOL64
+
+
+def _solve_both(solver, st, k, tol, precision=sc.FP64):
+    lat = oracle_lattice(st, k)
+    loads, ex = z_loads(lat)
+    u_ref, info_ref = lat.motions(loads, tol=tol, hierarchy=True)
+    u, info = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=tol, precision=precision))
+    return lat, u_ref, info_ref, u, info
+
+
+@pytest.mark.parametrize("n,seed", [(16, 0), (16, 1), (24, 3), (32, 0), (32, 2)])
+def test_hierarchy_bit_exact_and_motions(solver, n, seed):
+    st, k = piece(n, seed)
+    lat, u_ref, ir, u, info = _solve_both(solver, st, k, 1e-8)
+    assert info["status"] == sc.OK
+    assert info["parts"] == ir["counts"]
+    assert info["blocks"][1:] == [2 * p + c for p, c in zip(ir["pairs"][1:], ir["counts"][1:])]
+    for l, up_ref in enumerate(ir["up"]):
+        up = solver.last_up(l, len(up_ref))
+        assert (up == up_ref).all(), f"level {l}"
+    assert np.allclose(info["steps"], ir["steps"], rtol=1e-9)
+    assert abs(info["iterations"] - ir["iterations"]) <= 1
+    assert rel(u, u_ref) < DISP_TOL
+    assert info["residual"] <= 1e-8 * 1.0001
+
+
+@pytest.mark.parametrize("name,st,k", special_pieces(), ids=[p[0] for p in special_pieces()])
+def test_motions_special_pieces(solver, name, st, k):
+    lat, u_ref, ir, u, info = _solve_both(solver, st, k, 1e-10)
+    assert info["parts"] == ir["counts"]
+    assert rel(u, u_ref) < 1e-8
+
+
+def test_mixed_precision_against_fp64(solver):
+    st, k = piece(32, 1)
+    lat = oracle_lattice(st, k)
+    loads, ex = z_loads(lat)
+    u_ref, _ = lat.motions(loads, tol=1e-12)
+    u64, i64 = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8))
+    u32, i32 = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8, precision=sc.MIXED))
+    assert i32["status"] == sc.OK
+    assert i32["residual"] <= 1e-8 * 1.0001
+    assert i32["refinements"] >= 1
+    assert rel(u64, u_ref) < DISP_TOL
+    assert rel(u32, u_ref) < DISP_TOL
+
+
+def test_golden_large(solver):
+    """Pieces whose oracle solve takes minutes, against its committed outputs."""
+    cases = [c for c in json.load(open(os.path.join(HERE, "golden", "oracle_pieces.json"))) if c["n"] >= 48]
+    for c in cases:
+        st, k = piece(c["n"], c["seed"])
+        u, info = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=c["tol"]))
+        assert info["parts"] == c["counts"], c["n"]
+        for l, h in enumerate(c["up_hash"]):
+            up = solver.last_up(l, c["counts"][l])
+            assert hashlib.sha256(up.astype(np.int32).tobytes()).hexdigest()[:16] == h
+        assert abs(info["iterations"] - c["iterations"]) <= 1
+        assert np.linalg.norm(u) == pytest.approx(c["u_norm"], rel=DISP_TOL)
+        idx = np.asarray(c["sample_idx"])
+        assert np.allclose(u.ravel()[idx], c["sample_u"], rtol=0, atol=DISP_TOL * c["u_norm"] / np.sqrt(u.size) * 50)
+
+
+def test_batch_matches_single_solves(solver):
+    rng = np.random.default_rng(7)
+    sizes = [16, 24, 32]
+    pieces = []
+    for i in range(6):
+        shape = tuple(int(v) for v in rng.choice(sizes, 3))
+        pieces.append(piece(0, 100 + i, shape=shape))
+    outs, infos = solver.solve_grid_batch(pieces, sc.options(max_iter=5000, tol=1e-8))
+    for (st, k), u, info in zip(pieces, outs, infos):
+        lat = oracle_lattice(st, k)
+        loads, _ = z_loads(lat)
+        u_ref, ir = lat.motions(loads, tol=1e-8)
+        assert info["parts"] == ir["counts"]
+        assert abs(info["iterations"] - ir["iterations"]) <= 1
+        assert rel(u, u_ref) < DISP_TOL
+
+
+def test_batch_mixed(solver):
+    pieces = [piece(0, 200 + i, shape=(16 + 8 * (i % 3), 24, 16 + 16 * (i % 2))) for i in range(8)]
+    outs, infos = solver.solve_grid_batch(pieces, sc.options(max_iter=5000, tol=1e-8, precision=sc.MIXED))
+    for (st, k), u, info in zip(pieces, outs, infos):
+        lat = oracle_lattice(st, k)
+        loads, _ = z_loads(lat)
+        u_ref, _ = lat.motions(loads, tol=1e-12)
+        assert info["residual"] <= 1e-8 * 1.0001
+        assert rel(u, u_ref) < DISP_TOL
+
+
+SCENES = [
+    ("cantilever", dict(kind="cantilever", mat=O.STONE, a=0.5, b=4.0), 0.43),
+    ("cantilever 6", dict(kind="cantilever", mat=O.STONE, a=0.5, b=6.0), 0.97),
+    ("portico", dict(kind="portico", a=1, b=0.5), 1.03),
+    ("tree 70", dict(kind="tree", a=8.0, b=-1.0, c=0.7), 3.3),
+]
+
+
+def _used_standing_gpu(solver, lat):
+    """bodies.rs:550-554 with the GPU's motions: gone = not joined to held."""
+    ex = lat.export()
+    nn = lat.n_nodes
+    # joined_to_held (bodies.rs:557-574)
+    nbr = [[] for _ in range(nn)]
+    for i, j in zip(ex["bi"], ex["bj"]):
+        nbr[i].append(j)
+        nbr[j].append(i)
+    held = ex["held"].astype(bool).copy()
+    stack = list(np.nonzero(held)[0])
+    while stack:
+        v = stack.pop()
+        for w in nbr[v]:
+            if not held[w]:
+                held[w] = True
+                stack.append(w)
+    gone = (~held).astype(np.uint8)
+    loads = np.zeros((nn, 6))
+    loads[:, 1] = -ex["m"] * 9.81
+    w = sc.Work()
+    u = solver.motions(lattice_dict(ex), None, gone, loads, w)
+    f = lat.moved(u)
+    f[(gone[ex["bi"]] == 1) | (gone[ex["bj"]] == 1)] = 0
+    # Bond::used (model.rs:123-129)
+    t = f / ex["a"][:, None]
+    sigma = (t * ex["n"]).sum(1)
+    tau2 = np.maximum((t * t).sum(1) - sigma ** 2, 0)
+    r = np.sqrt(sigma ** 2 / 4 + tau2)
+    s1, s3 = sigma / 2 + r, sigma / 2 - r
+    return u, w
+
+
+@pytest.mark.parametrize("name,kw,want", SCENES, ids=[s[0] for s in SCENES])
+def test_general_lattice_motions(solver, name, kw, want):
+    lat = O.Lattice.scene(**kw)
+    ex = lat.export()
+    loads = np.zeros((lat.n_nodes, 6))
+    loads[:, 1] = -ex["m"] * 9.81
+    u_ref, ir = lat.motions(loads, tol=1e-10, hierarchy=True)
+    w = sc.Work()
+    u = solver.motions(lattice_dict(ex), None, None, loads, w, sc.options(max_iter=5000, tol=1e-10))
+    assert w.status == sc.OK
+    assert w.info["parts"] == ir["counts"]
+    assert rel(u, u_ref) < 1e-7
+
+
+def test_general_lattice_alive_and_gone(solver):
+    lat = O.Lattice.scene("pendant", a=0)
+    ex = lat.export()
+    rng = np.random.default_rng(4)
+    alive = np.ones(lat.n_bonds, np.uint8)
+    beams = rng.choice(lat.n_bonds // 4, size=lat.n_bonds // 40, replace=False)
+    for b in beams:
+        alive[4 * b:4 * b + 4] = 0
+    gone = np.zeros(lat.n_nodes, np.uint8)
+    loads = np.zeros((lat.n_nodes, 6))
+    loads[:, 1] = -ex["m"] * 9.81
+    u_ref, ir = lat.motions(loads, alive=alive, gone=gone, tol=1e-10, hierarchy=True)
+    w = sc.Work()
+    u = solver.motions(lattice_dict(ex), alive, gone, loads, w, sc.options(max_iter=5000, tol=1e-10))
+    assert w.info["parts"] == ir["counts"]
+    assert rel(u, u_ref) < 1e-7
+
+
+def test_compliance_gradient(solver):
+    st, k = piece(12, 2)
+    C, grad, u, info = solver.compliance_grad(st, k, sc.options(max_iter=5000, tol=1e-12))
+    lat = oracle_lattice(st, k)
+    loads, ex = z_loads(lat)
+    u_ref, _ = lat.motions(loads, tol=1e-12)
+    assert C == pytest.approx(float((loads * u_ref).sum()), rel=1e-9)
+    energy = lat.cell_energy(u_ref, st.size).reshape(st.shape)
+    free = st == 1
+    want = np.where(free, -2 * energy / np.where(free, k, 1), 0)
+    assert rel(grad, want) < 1e-8
+
+
+def test_statuses(solver):
+    st, k = piece(12, 0)
+    u, info = solver.solve_grid(st, k, sc.options(tol=1e-8, max_iter=0))
+    assert info["status"] == sc.MAXITER
+    assert np.abs(u).max() == 0.0
+    bad = k.copy()
+    bad[st == 1] = np.nan
+    u, info = solver.solve_grid(st, bad, sc.options(max_iter=5000, tol=1e-8))
+    assert info["status"] in (sc.BREAKDOWN, sc.NOT_SPD)
+    with pytest.raises(sc.StaticsError) as e:
+        solver.solve_grid(st, k, sc.options(max_iter=5000, tol=-1.0))
+    assert e.value.status == sc.BAD_INPUT
