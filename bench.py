@@ -287,6 +287,23 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_probe(args):
+    """Only the level-0 stencil on the bench's piece (FP64 then FP32), two launches
+    each: the small command an ncu capture of that kernel runs."""
+    import numpy as np
+
+    import statics_cuda as sc
+    state, k = sc.generate_piece(N, N, N, args.seed, sc.K_UNIFORM)
+    _, parts = sc.grid_count(state)
+    x = np.random.default_rng(0).standard_normal((parts, 6))
+    solver = sc.Solver(0)
+    for prec in (sc.FP64, sc.MIXED):
+        for _ in range(2):
+            y = solver.grid_apply(state, k, x, prec)
+    print(json.dumps({"probe": "stencil", "parts": parts, "y_norm": float(np.linalg.norm(y))}))
+    solver.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -295,8 +312,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--probe", choices=["stencil"], help="run one kernel alone (for profiling)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.probe:
+        run_probe(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -50,6 +50,18 @@ template <>
 DBuf<double>& VZ<double>(Level& L) { return L.z; }
 template <>
 DBuf<float>& VZ<float>(Level& L) { return L.z32; }
+template <class T>
+static DBuf<T>& VT(Level& L);
+template <>
+DBuf<double>& VT<double>(Level& L) { return L.t; }
+template <>
+DBuf<float>& VT<float>(Level& L) { return L.t32; }
+template <class T>
+static DBuf<T>& VU(Level& L);
+template <>
+DBuf<double>& VU<double>(Level& L) { return L.u; }
+template <>
+DBuf<float>& VU<float>(Level& L) { return L.u32; }
 
 template <class T>
 void level_apply(Context& ctx, const Batch& b, int l, const T* x, T* y) {
@@ -78,6 +90,9 @@ static void alloc_cycle(Context& ctx, Batch& b) {
         if (l > 0) {
             ensure(ctx, VR<T>(L), n6);
             ensure(ctx, VZ<T>(L), n6);
+        } else if (L.matrix_free && b.levels.size() > 1) {
+            ensure(ctx, VT<T>(L), n6);
+            ensure(ctx, VU<T>(L), n6);
         }
     }
 }
@@ -103,7 +118,14 @@ template <class T>
 static void cycle(Context& ctx, Batch& b, int l, const T* r, T* z, const int32_t* done) {
     Level& L = b.levels[l];
     bool deepest = l + 1 == (int)b.levels.size();
-    if (!deepest) {
+    if (!deepest && l == 0 && L.matrix_free) {
+        // level 0 of voxel pieces: smoother and both transfers matrix-free
+        Level& C = b.levels[1];
+        T* x = VX<T>(L).get();
+        level0_down<T>(ctx, b, r, x, VL<T>(L).get(), VT<T>(L).get(), VU<T>(L).get(), VR<T>(C).get(), done);
+        cycle<T>(ctx, b, 1, VR<T>(C).get(), VZ<T>(C).get(), done);
+        level0_up<T>(ctx, b, r, x, VT<T>(L).get(), VZ<T>(C).get(), z, done);
+    } else if (!deepest) {
         const int32_t* skip = L.top_of_part.get();
         T* x = VX<T>(L).get();
         T* left = VL<T>(L).get();
@@ -361,6 +383,13 @@ struct CgState {
     }
 };
 
+// reduction scratch sized before a capture (a capture may not allocate)
+static void ensure_partial(Context& ctx, const Level& L) {
+    if ((int64_t)ctx.partial.size() < 2 * std::max<int64_t>(L.nchunks, 1) + 2048)
+        ctx.partial.alloc(2 * (L.nchunks + 1024) + 2048, ctx.stream, &ctx.mem);
+}
+static void prepare_top(const Level&) {}
+
 // two chunked dots (a.b and a.a) per piece
 template <class T>
 static void dot2(Context& ctx, const Level& L, const int32_t* done, const T* a, const T* b, double* oab, double* oaa) {
@@ -396,13 +425,66 @@ static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V*
     cycle<V>(ctx, b, 0, r, z, cg.s.done);
     SC_CK(cudaMemcpyAsync(p, z, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
     dot2<V>(ctx, L, cg.s.done, r, z, cg.s.rz, cg.s.rr);
+    // one iteration (bodies.rs:351-371), ending with the next iteration's check
+    auto body = [&]() {
+        if (L.matrix_free) {
+            stencil_apply<V>(ctx, b, p, ap, nullptr, cg.s.done);
+        } else {
+            ProfScope ps(ctx, fam_of<V>(SC_FAM_SPMV64), spmv_bytes<V>(L, 2));
+            spmv<V>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), VAL<V>(L), p, nullptr, ap, nullptr, nullptr,
+                    L.piece.get(), nullptr, cg.s.done);
+        }
+        dot2<V>(ctx, L, cg.s.done, p, ap, cg.s.pap, nullptr);
+        k_cg_alpha<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s);
+        SC_LAUNCH_CK();
+        if (L.nchunks > 0) {
+            k_axpy2<V, S><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
+                                                              cg.s.alpha, x, p, r, ap);
+            SC_LAUNCH_CK();
+        }
+        cycle<V>(ctx, b, 0, r, z, cg.s.done);
+        dot2<V>(ctx, L, cg.s.done, r, z, cg.s.next, cg.s.rr);
+        k_cg_beta<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.beta);
+        SC_LAUNCH_CK();
+        if (L.nchunks > 0) {
+            k_pupdate<V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
+                                                             cg.beta, p, z);
+            SC_LAUNCH_CK();
+        }
+        SC_CK(cudaMemsetAsync(cg.ndone.get(), 0, sizeof(int32_t), st));
+        k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
+        SC_LAUNCH_CK();
+    };
     int32_t* ndone_h = nullptr;
     SC_CK(cudaMallocHost((void**)&ndone_h, sizeof(int32_t)));
+    cudaGraphExec_t exec = nullptr;
     try {
-        for (int64_t it = 0;; it++) {
-            cg.ndone.zero();
-            k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
-            SC_LAUNCH_CK();
+        // Replaying a captured iteration saves ~50 launches an iteration; timing
+        // individual kernels (profiling) launches them one by one instead.
+        bool use_graph = ctx.prof.mask == 0;
+        if (use_graph) {
+            ensure_partial(ctx, L);
+            for (auto& lv : b.levels) prepare_top(lv);
+            cudaGraph_t graph = nullptr;
+            SC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            try {
+                body();
+            } catch (...) {
+                cudaStreamEndCapture(st, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            SC_CK(cudaStreamEndCapture(st, &graph));
+            cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            SC_CK(e);
+        }
+        SC_CK(cudaMemsetAsync(cg.ndone.get(), 0, sizeof(int32_t), st));
+        k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
+        SC_LAUNCH_CK();
+        // iterations run between looks at the done count (finished pieces' kernels return at once)
+        const int per_look = 4;
+        for (;;) {
             SC_CK(cudaMemcpyAsync(ndone_h, cg.ndone.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             SC_CK(cudaStreamSynchronize(st));
             if (*ndone_h >= np) break;
@@ -410,36 +492,19 @@ static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V*
                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count() >
                     timeout_ms)
                 throw Error(SC_TIMEOUT, "solve ran past its time limit");
-            // Ap, alpha
-            if (L.matrix_free) {
-                stencil_apply<V>(ctx, b, p, ap, nullptr, cg.s.done);
-            } else {
-                ProfScope ps(ctx, fam_of<V>(SC_FAM_SPMV64), spmv_bytes<V>(L, 2));
-                spmv<V>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), VAL<V>(L), p, nullptr, ap, nullptr, nullptr,
-                        L.piece.get(), nullptr, cg.s.done);
-            }
-            dot2<V>(ctx, L, cg.s.done, p, ap, cg.s.pap, nullptr);
-            k_cg_alpha<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s);
-            SC_LAUNCH_CK();
-            if (L.nchunks > 0) {
-                k_axpy2<V, S><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
-                                                                  cg.s.alpha, x, p, r, ap);
-                SC_LAUNCH_CK();
-            }
-            cycle<V>(ctx, b, 0, r, z, cg.s.done);
-            dot2<V>(ctx, L, cg.s.done, r, z, cg.s.next, cg.s.rr);
-            k_cg_beta<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.beta);
-            SC_LAUNCH_CK();
-            if (L.nchunks > 0) {
-                k_pupdate<V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
-                                                                 cg.beta, p, z);
-                SC_LAUNCH_CK();
+            for (int g = 0; g < per_look; g++) {
+                if (exec)
+                    SC_CK(cudaGraphLaunch(exec, st));
+                else
+                    body();
             }
         }
     } catch (...) {
+        if (exec) cudaGraphExecDestroy(exec);
         cudaFreeHost(ndone_h);
         throw;
     }
+    if (exec) cudaGraphExecDestroy(exec);
     cudaFreeHost(ndone_h);
 }
 
@@ -493,9 +558,10 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
     int np = b.npieces;
     for (size_t l = 0; l < b.levels.size(); l++) {
         Level& L = b.levels[l];
-        if (!(l == 0 && L.matrix_free)) to_float(ctx, L.val, L.val32);
-        to_float(ctx, L.inv, L.inv32);
+        if (L.val.size()) to_float(ctx, L.val, L.val32);
+        if (L.inv.size()) to_float(ctx, L.inv, L.inv32);
         if (L.pval.size()) to_float(ctx, L.pval, L.pval32);
+        if (L.mf_r.size()) to_float(ctx, L.mf_r, L.mf_r32);
     }
     alloc_cycle<float>(ctx, b);
     Level& L = b.levels[0];

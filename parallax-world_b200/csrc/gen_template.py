@@ -123,6 +123,13 @@ def emit(K, fac):
     w("};\nstatic const double JAC_L_HOST[3][6] = {\n")
     for _, lam in fac:
         w("  {" + ", ".join(lit(x) for x in lam) + "},\n")
+    w("};\n")
+    w("__constant__ double JAC_V_DEV[3][6][6] = {\n")
+    for V, _ in fac:
+        w("  {" + ", ".join("{" + ", ".join(lit(V[i, j]) for j in range(6)) + "}" for i in range(6)) + "},\n")
+    w("};\n__constant__ double JAC_L_DEV[3][6] = {\n")
+    for _, lam in fac:
+        w("  {" + ", ".join(lit(x) for x in lam) + "},\n")
     w("};\n\n")
     # stencil strips: y += sum_b T[slot][b] * xs[b], xs[b] the six node vectors of the cell
     for slot in range(6):
@@ -141,6 +148,18 @@ def emit(K, fac):
                 w(f"    s = fma(T({lit(v)}), x[{b}][{j}], s);\n")
             w(f"    acc[{i}] = s; }}\n")
         w("}\n\n")
+    # per-(slot, face) 6x6 blocks: acc += TPL block (slot, face) * x_face
+    w("template <int S, int F>\nstruct Blk;\n")
+    for slot in range(6):
+        for f in range(6):
+            w(f"template <>\nstruct Blk<{slot}, {f}> {{\n  template <class T>\n")
+            w("  __device__ __forceinline__ static void mac(const T (&x)[6], T (&acc)[6]) {\n")
+            for i in range(6):
+                terms = [(j, K[6 * slot + i, 6 * f + j]) for j in range(6) if K[6 * slot + i, 6 * f + j] != 0.0]
+                for j, v in terms:
+                    w(f"    acc[{i}] = fma(T({lit(v)}), x[{j}], acc[{i}]);\n")
+            w("  }\n};\n")
+    w("\n")
     nnz = int((K != 0).sum())
     w(f"constexpr int TPL_NNZ = {nnz};\n\n")
     w("}  // namespace sc\n")

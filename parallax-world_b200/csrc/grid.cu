@@ -40,6 +40,13 @@ __global__ void k_iota(int64_t n, int32_t* __restrict__ v) {
     if (i < n) v[i] = (int32_t)i;
 }
 
+constexpr int64_t STENCIL_TILE = 1024;
+
+__global__ void k_tile_axis_keys(int64_t n, const int8_t* __restrict__ axis, uint32_t* __restrict__ keys) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < n) keys[k] = (uint32_t)(((k / STENCIL_TILE) << 2) | (uint32_t)axis[k]);
+}
+
 struct Dims {
     int32_t nx, ny, nz, pad;
 };
@@ -334,71 +341,219 @@ __device__ __forceinline__ void store6(T* __restrict__ v, int64_t k, const T (&o
     }
 }
 
-// acc += k_C * strip_SLOT(x of cell C's faces, rotations scaled by s)
+// t += TPL block (SLOT, F) * x_F for faces F.., each face's six values loaded on its
+// own (rotations scaled by s) so few registers stay live.
+template <int SLOT, int F, class T>
+__device__ __forceinline__ void faces(const int32_t (&q)[6], const T* __restrict__ x, T s, T (&t)[6]) {
+    if constexpr (F < 6) {
+        if (q[F] >= 0) {
+            T xv[6];
+            load6<T>(x, q[F], xv);
+            xv[3] *= s;
+            xv[4] *= s;
+            xv[5] *= s;
+            Blk<SLOT, F>::mac(xv, t);
+        }
+        faces<SLOT, F + 1, T>(q, x, s, t);
+    }
+}
+
+// acc += k_C * (row strip SLOT of cell C's template) * (x of C's six faces)
 template <int SLOT, class T>
-__device__ __forceinline__ void cell_term(const int4* __restrict__ cell, int32_t C, const T* __restrict__ x, T s,
-                                          T (&acc)[6]) {
+__device__ __forceinline__ void cell_term(const int4* __restrict__ cell, int32_t C, T kc, const T* __restrict__ x,
+                                          T s, T (&acc)[6]) {
     int4 a = __ldg(cell + 2 * C), b = __ldg(cell + 2 * C + 1);
     int32_t q[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
-    T kc = (T)__int_as_float(b.z);
-    T xs[6][6];
-#pragma unroll
-    for (int f = 0; f < 6; f++) {
-        if (q[f] >= 0) {
-            load6<T>(x, q[f], xs[f]);
-            xs[f][3] *= s;
-            xs[f][4] *= s;
-            xs[f][5] *= s;
-        } else {
-#pragma unroll
-            for (int j = 0; j < 6; j++) xs[f][j] = T(0);
-        }
-    }
     T t[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    strip<SLOT, T>(xs, t);
+    faces<SLOT, 0, T>(q, x, s, t);
 #pragma unroll
     for (int i = 0; i < 6; i++) acc[i] = fma(kc, t[i], acc[i]);
 }
 
-// y = K x over the parts grouped by axis (perm). MODE 0: y = Kx. MODE 1: y = r - Kx.
+// D^-1 v for a face node on axis AX between cells of stiffness kA (lesser) and kB
+// (greater), spacing s: D = s Dm (kA M+ + kB M-) Dm with Dm = diag(1,1,1,s,s,s) and
+// kA M+ + kB M- = V^-T diag(kA lambda + kB) V^-1 (generalised eigenvectors of the two
+// face blocks, template_gen.cuh), so D^-1 v = (1/s) Dm^-1 V diag(1/(kA lambda + kB)) V' Dm^-1 v.
+template <int AX, class T>
+__device__ __forceinline__ void dinv(T kA, T kB, T s, const T (&v)[6], T (&y)[6]) {
+    T vt[6] = {v[0], v[1], v[2], v[3] / s, v[4] / s, v[5] / s};
+    T w[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < 6; j++) acc = fma((T)JAC_V_DEV[AX][j][i], vt[j], acc);
+        w[i] = acc / fma(kA, (T)JAC_L_DEV[AX][i], kB);
+    }
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < 6; j++) acc = fma((T)JAC_V_DEV[AX][i][j], w[j], acc);
+        y[i] = i < 3 ? acc / s : acc / (s * s);
+    }
+}
+
+// Epilogues of the stencil (Kx is the row's K x):
+//   ST_Y        y = Kx
+//   ST_RES      y = r - Kx
+//   ST_RES_JAC  y = r - Kx, y2 = D^-1 (r - Kx)
+//   ST_RES_W    y = r - w Kx                          (w the piece's smoother step)
+//   ST_PROLONG  y += x - w D^-1 Kx                    (x = P0 z; y accumulates)
+//   ST_SMOOTH   y = x + w D^-1 (r - Kx)
+enum { ST_Y = 0, ST_RES = 1, ST_RES_JAC = 2, ST_RES_W = 3, ST_PROLONG = 4, ST_SMOOTH = 5 };
+
+template <int AX, class T, int MODE>
+__device__ __forceinline__ void stencil_row(int32_t k, int32_t A, int32_t B, const int4* __restrict__ cell,
+                                            const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
+                                            T* __restrict__ y2, T s, T w) {
+    T kA = A >= 0 ? (T)__int_as_float(__ldg(&cell[2 * A + 1].z)) : T(0);
+    T kB = B >= 0 ? (T)__int_as_float(__ldg(&cell[2 * B + 1].z)) : T(0);
+    T acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    if (A >= 0) cell_term<2 * AX + 1, T>(cell, A, kA, x, s, acc);
+    if (B >= 0) cell_term<2 * AX, T>(cell, B, kB, x, s, acc);
+    T kx[6] = {acc[0] * s, acc[1] * s, acc[2] * s, acc[3] * s * s, acc[4] * s * s, acc[5] * s * s};
+    T o[6];
+    if constexpr (MODE == ST_Y) {
+        store6<T>(y, k, kx);
+    } else if constexpr (MODE == ST_RES) {
+        load6<T>(r, k, o);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] -= kx[j];
+        store6<T>(y, k, o);
+    } else if constexpr (MODE == ST_RES_JAC) {
+        load6<T>(r, k, o);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] -= kx[j];
+        store6<T>(y, k, o);
+        T d[6];
+        dinv<AX, T>(kA, kB, s, o, d);
+        store6<T>(y2, k, d);
+    } else if constexpr (MODE == ST_RES_W) {
+        load6<T>(r, k, o);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] = fma(-w, kx[j], o[j]);
+        store6<T>(y, k, o);
+    } else if constexpr (MODE == ST_PROLONG) {
+        T d[6], xv[6], acc2[6];
+        dinv<AX, T>(kA, kB, s, kx, d);
+        load6<T>(x, k, xv);
+        load6<T>(y, k, acc2);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] = acc2[j] + fma(-w, d[j], xv[j]);
+        store6<T>(y, k, o);
+    } else {
+        T rv[6], d[6], xv[6];
+        load6<T>(r, k, rv);
+#pragma unroll
+        for (int j = 0; j < 6; j++) rv[j] -= kx[j];
+        dinv<AX, T>(kA, kB, s, rv, d);
+        load6<T>(x, k, xv);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] = fma(w, d[j], xv[j]);
+        store6<T>(y, k, o);
+    }
+}
+
+// Level 0 applied matrix-free over the parts grouped by axis (perm).
 template <class T, int MODE>
-__global__ void __launch_bounds__(256) k_stencil(int64_t n_perm, const int32_t* __restrict__ perm, int64_t off1,
-                                                 int64_t off2, const int32_t* __restrict__ cella,
+__global__ void __launch_bounds__(256, 3) k_stencil(int64_t n_perm, const int32_t* __restrict__ perm,
+                                                 const int8_t* __restrict__ axis, const int32_t* __restrict__ cella,
                                                  const int32_t* __restrict__ cellb, const int4* __restrict__ cell,
                                                  const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
-                                                 T s, const int32_t* __restrict__ piece,
-                                                 const int32_t* __restrict__ skip_row, const int32_t* __restrict__ done) {
+                                                 T* __restrict__ y2, T s, const int32_t* __restrict__ piece,
+                                                 const double* __restrict__ step, const int32_t* __restrict__ skip_row,
+                                                 const int32_t* __restrict__ done) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n_perm) return;
     int32_t k = perm[i];
     if (skip_row && skip_row[k]) return;
-    if (done && done[piece[k]]) return;
+    int p = (done || step) ? piece[k] : 0;
+    if (done && done[p]) return;
+    T w = step ? (T)step[p] : T(0);
     int32_t A = cella[k], B = cellb[k];
-    T acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    if (i < off1) {
-        if (A >= 0) cell_term<1, T>(cell, A, x, s, acc);
-        if (B >= 0) cell_term<0, T>(cell, B, x, s, acc);
-    } else if (i < off2) {
-        if (A >= 0) cell_term<3, T>(cell, A, x, s, acc);
-        if (B >= 0) cell_term<2, T>(cell, B, x, s, acc);
-    } else {
-        if (A >= 0) cell_term<5, T>(cell, A, x, s, acc);
-        if (B >= 0) cell_term<4, T>(cell, B, x, s, acc);
-    }
-    T o[6];
-    o[0] = acc[0] * s;
-    o[1] = acc[1] * s;
-    o[2] = acc[2] * s;
-    o[3] = acc[3] * s * s;
-    o[4] = acc[4] * s * s;
-    o[5] = acc[5] * s * s;
-    if (MODE == 1) {
-        T rr[6];
-        load6<T>(r, k, rr);
+    int ax = axis[k];
+    if (ax == 0)
+        stencil_row<0, T, MODE>(k, A, B, cell, x, r, y, y2, s, w);
+    else if (ax == 1)
+        stencil_row<1, T, MODE>(k, A, B, cell, x, r, y, y2, s, w);
+    else
+        stencil_row<2, T, MODE>(k, A, B, cell, x, r, y, y2, s, w);
+}
+
+// x = w D^-1 r with D^-1 matrix-free (pre-smoothing, bodies.rs:386)
+template <class T>
+__global__ void __launch_bounds__(256) k_jacobi_mf(int64_t n, const int8_t* __restrict__ axis,
+                                                   const int32_t* __restrict__ cella, const int32_t* __restrict__ cellb,
+                                                   const int4* __restrict__ cell, const T* __restrict__ r,
+                                                   T* __restrict__ x, T s, const int32_t* __restrict__ piece,
+                                                   const double* __restrict__ step, const int32_t* __restrict__ skip_row,
+                                                   const int32_t* __restrict__ done) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (skip_row && skip_row[k]) return;
+    int p = piece[k];
+    if (done && done[p]) return;
+    T w = step ? (T)step[p] : T(1);
+    int32_t A = cella[k], B = cellb[k];
+    T kA = A >= 0 ? (T)__int_as_float(__ldg(&cell[2 * A + 1].z)) : T(0);
+    T kB = B >= 0 ? (T)__int_as_float(__ldg(&cell[2 * B + 1].z)) : T(0);
+    T rv[6], d[6];
+    load6<T>(r, (int32_t)k, rv);
+    int ax = axis[k];
+    if (ax == 0)
+        dinv<0, T>(kA, kB, s, rv, d);
+    else if (ax == 1)
+        dinv<1, T>(kA, kB, s, rv, d);
+    else
+        dinv<2, T>(kA, kB, s, rv, d);
 #pragma unroll
-        for (int j = 0; j < 6; j++) o[j] = rr[j] - o[j];
+    for (int j = 0; j < 6; j++) d[j] *= w;
+    store6<T>(x, k, d);
+}
+
+// rc[c] = sum over the parts k of body c of R_k' u_k, R_k' u = (u_t, u_w + r_k x u_t):
+// the rigid part P0' of the restriction (bodies.rs:239, 388-390)
+template <class T>
+__global__ void __launch_bounds__(256) k_p0t(int64_t nc, const int64_t* __restrict__ moff,
+                                             const int32_t* __restrict__ mem, const T* __restrict__ rvec,
+                                             const T* __restrict__ u, T* __restrict__ rc,
+                                             const int32_t* __restrict__ piece_c, const int32_t* __restrict__ done) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    if (done && done[piece_c[c]]) return;
+    T o[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    for (int64_t t = moff[c]; t < moff[c + 1]; t++) {
+        int32_t k = mem[t];
+        T uv[6];
+        load6<T>(u, k, uv);
+        T r0 = rvec[3 * (int64_t)k], r1 = rvec[3 * (int64_t)k + 1], r2 = rvec[3 * (int64_t)k + 2];
+        o[0] += uv[0];
+        o[1] += uv[1];
+        o[2] += uv[2];
+        o[3] += uv[3] + (r1 * uv[2] - r2 * uv[1]);
+        o[4] += uv[4] + (r2 * uv[0] - r0 * uv[2]);
+        o[5] += uv[5] + (r0 * uv[1] - r1 * uv[0]);
     }
-    store6<T>(y, k, o);
+    store6<T>(rc, c, o);
+}
+
+// e_k = R_k z_{up[k]} = (z_t + z_w x r_k, z_w): the rigid part P0 of the prolongation
+template <class T>
+__global__ void __launch_bounds__(256) k_p0(int64_t n, const int32_t* __restrict__ up, const T* __restrict__ rvec,
+                                            const T* __restrict__ z, T* __restrict__ e, const int32_t* __restrict__ piece,
+                                            const int32_t* __restrict__ skip_row, const int32_t* __restrict__ done) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (skip_row && skip_row[k]) return;
+    if (done && done[piece[k]]) return;
+    int32_t c = up[k];
+    T zv[6];
+    load6<T>(z, c, zv);
+    T r0 = rvec[3 * k], r1 = rvec[3 * k + 1], r2 = rvec[3 * k + 2];
+    T o[6] = {zv[0] + (zv[4] * r2 - zv[5] * r1), zv[1] + (zv[5] * r0 - zv[3] * r2), zv[2] + (zv[3] * r1 - zv[4] * r0),
+              zv[3], zv[4], zv[5]};
+    store6<T>(e, k, o);
 }
 
 // Strain energy of each free cell's 60 bonds at motions x: U = 1/2 x_c' K_c x_c with
@@ -437,16 +592,21 @@ static double stencil_bytes(const Batch& b, int vec_passes) {
     return (double)sizeof(T) * 6.0 * (double)b.levels[0].n * vec_passes + 4.0 * (double)g.ncells + G / 8.0;
 }
 
-template <class T>
-void stencil_apply(Context& ctx, const Batch& b, const T* x, T* y, const int32_t* skip_row, const int32_t* done) {
+template <class T, int MODE>
+static void launch_stencil(Context& ctx, const Batch& b, const T* x, const T* r, T* y, T* y2, const double* step,
+                           const int32_t* skip_row, const int32_t* done, int passes) {
     const Grid0& g = b.grid;
     const Level& L = b.levels[0];
     int64_t n = g.axis_off[3];
-    ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_STENCIL64 : SC_FAM_STENCIL32, stencil_bytes<T>(b, 2));
-    k_stencil<T, 0><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.perm.get(), g.axis_off[1], g.axis_off[2],
-                                                               g.cella.get(), g.cellb.get(), g.cell.get(), x,
-                                                               nullptr, y, (T)g.s, L.piece.get(), skip_row, done);
+    ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_STENCIL64 : SC_FAM_STENCIL32, stencil_bytes<T>(b, passes));
+    k_stencil<T, MODE><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.perm.get(), g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(), x, r, y,
+                                                                  y2, (T)g.s, L.piece.get(), step, skip_row, done);
     SC_LAUNCH_CK();
+}
+
+template <class T>
+void stencil_apply(Context& ctx, const Batch& b, const T* x, T* y, const int32_t* skip_row, const int32_t* done) {
+    launch_stencil<T, ST_Y>(ctx, b, x, nullptr, y, nullptr, nullptr, skip_row, done, 2);
 }
 template void stencil_apply<double>(Context&, const Batch&, const double*, double*, const int32_t*, const int32_t*);
 template void stencil_apply<float>(Context&, const Batch&, const float*, float*, const int32_t*, const int32_t*);
@@ -454,19 +614,68 @@ template void stencil_apply<float>(Context&, const Batch&, const float*, float*,
 template <class T>
 void stencil_residual(Context& ctx, const Batch& b, const T* x, const T* r, T* y, const int32_t* skip_row,
                       const int32_t* done) {
-    const Grid0& g = b.grid;
-    const Level& L = b.levels[0];
-    int64_t n = g.axis_off[3];
-    ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_STENCIL64 : SC_FAM_STENCIL32, stencil_bytes<T>(b, 3));
-    k_stencil<T, 1><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.perm.get(), g.axis_off[1], g.axis_off[2],
-                                                               g.cella.get(), g.cellb.get(), g.cell.get(), x, r, y,
-                                                               (T)g.s, L.piece.get(), skip_row, done);
-    SC_LAUNCH_CK();
+    launch_stencil<T, ST_RES>(ctx, b, x, r, y, nullptr, nullptr, skip_row, done, 3);
 }
 template void stencil_residual<double>(Context&, const Batch&, const double*, const double*, double*, const int32_t*,
                                        const int32_t*);
 template void stencil_residual<float>(Context&, const Batch&, const float*, const float*, float*, const int32_t*,
                                       const int32_t*);
+
+// Level 0's half of a V-cycle on the way up (bodies.rs:386-390), matrix-free:
+//   x = w D^-1 r;  left = r - K x;  t = D^-1 left;  u = left - w K t;  rc = P0' u
+// (P' = P0' (I - w K D^-1), P = (I - w D^-1 K) P0, bodies.rs:238-247).
+template <class T>
+void level0_down(Context& ctx, const Batch& b, const T* r, T* x, T* left, T* t, T* u, T* rc, const int32_t* done) {
+    const Grid0& g = b.grid;
+    const Level& L = b.levels[0];
+    const Level& C = b.levels[1];
+    const int32_t* skip = L.top_of_part.get();
+    double vb = (double)sizeof(T) * 6.0 * (double)L.n;
+    {
+        ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_SMOOTH64 : SC_FAM_SMOOTH32, 2 * vb + 8.0 * L.n);
+        k_jacobi_mf<T><<<grid_for(L.n, 256), 256, 0, ctx.stream>>>(L.n, g.axis.get(), g.cella.get(), g.cellb.get(),
+                                                                   g.cell.get(), r, x, (T)g.s, L.piece.get(),
+                                                                   L.step.get(), skip, done);
+        SC_LAUNCH_CK();
+    }
+    launch_stencil<T, ST_RES_JAC>(ctx, b, x, r, left, t, nullptr, skip, done, 4);
+    launch_stencil<T, ST_RES_W>(ctx, b, t, left, u, nullptr, L.step.get(), skip, done, 3);
+    {
+        ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_TRANSFER64 : SC_FAM_TRANSFER32, vb + (double)sizeof(T) * 3 * L.n +
+                     (double)sizeof(T) * 6 * C.n);
+        const T* rv = sizeof(T) == 8 ? (const T*)L.mf_r.get() : (const T*)L.mf_r32.get();
+        k_p0t<T><<<grid_for(C.n, 256), 256, 0, ctx.stream>>>(C.n, L.mem_off.get(), L.mem.get(), rv, u, rc,
+                                                             C.piece.get(), done);
+        SC_LAUNCH_CK();
+    }
+}
+
+// ... and on the way down (bodies.rs:392-401), matrix-free:
+//   e = P0 zc;  x += e - w D^-1 K e;  z = x + w D^-1 (r - K x)
+template <class T>
+void level0_up(Context& ctx, const Batch& b, const T* r, T* x, T* e, const T* zc, T* z, const int32_t* done) {
+    const Level& L = b.levels[0];
+    const int32_t* skip = L.top_of_part.get();
+    double vb = (double)sizeof(T) * 6.0 * (double)L.n;
+    {
+        ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_TRANSFER64 : SC_FAM_TRANSFER32, vb + (double)sizeof(T) * 3 * L.n +
+                     4.0 * L.n + (double)sizeof(T) * 6 * b.levels[1].n);
+        const T* rv = sizeof(T) == 8 ? (const T*)L.mf_r.get() : (const T*)L.mf_r32.get();
+        k_p0<T><<<grid_for(L.n, 256), 256, 0, ctx.stream>>>(L.n, L.up.get(), rv, zc, e, L.piece.get(), skip, done);
+        SC_LAUNCH_CK();
+    }
+    launch_stencil<T, ST_PROLONG>(ctx, b, e, nullptr, x, nullptr, L.step.get(), skip, done, 4);
+    launch_stencil<T, ST_SMOOTH>(ctx, b, x, r, z, nullptr, L.step.get(), skip, done, 3);
+}
+
+template void level0_down<double>(Context&, const Batch&, const double*, double*, double*, double*, double*, double*,
+                                  const int32_t*);
+template void level0_down<float>(Context&, const Batch&, const float*, float*, float*, float*, float*, float*,
+                                 const int32_t*);
+template void level0_up<double>(Context&, const Batch&, const double*, double*, double*, const double*, double*,
+                                const int32_t*);
+template void level0_up<float>(Context&, const Batch&, const float*, float*, float*, const float*, float*,
+                               const int32_t*);
 
 void grid_cell_energy(Context& ctx, const Batch& b, const double* x, double* energy_cells) {
     const Grid0& g = b.grid;
@@ -610,49 +819,53 @@ void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool
     k_cell_table<<<grid_for(nfree, 256), 256, 0, st>>>(nfree, cell_node6.get(), node_part.get(), g.cell_flat.get(),
                                                         gk.get(), g.cell.get());
     SC_LAUNCH_CK();
-    // parts grouped by axis (stable: ascending part id within an axis)
+    // parts in order, grouped by axis only within tiles of STENCIL_TILE parts: the
+    // stencil sweeps the piece once in part order (x neighbours stay in L2) while a
+    // warp mostly runs one axis' code
     {
         DBuf<int32_t> ids, ids_out;
         ids.alloc(n, st, ms);
         ids_out.alloc(n, st, ms);
-        DBuf<int8_t> ax_out;
-        ax_out.alloc(n, st, ms);
+        DBuf<uint32_t> keys, keys_out;
+        keys.alloc(n, st, ms);
+        keys_out.alloc(n, st, ms);
         k_iota<<<grid_for(n, 256), 256, 0, st>>>(n, ids.get());
         SC_LAUNCH_CK();
-        cub::DeviceRadixSort::SortPairs(nullptr, tb, g.axis.get(), ax_out.get(), ids.get(), ids_out.get(), n, 0, 2, st);
-        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, g.axis.get(), ax_out.get(), ids.get(),
-                                        ids_out.get(), n, 0, 2, st);
-        g.perm = std::move(ids_out);
-        std::vector<int8_t> axh = ax_out.to_host();
-        g.axis_off[0] = 0;
-        for (int a = 0; a < 3; a++) {
-            int64_t cnt = 0;
-            for (int8_t v : axh) cnt += (v == a);
-            g.axis_off[a + 1] = g.axis_off[a] + cnt;
-        }
-    }
-    // assembled blocks for the setup
-    L.rowptr.alloc(n + 1, st, ms);
-    {
-        DBuf<int64_t> cnt;
-        cnt.alloc(n + 1, st, ms);
-        SC_CK(cudaMemsetAsync(cnt.get() + n, 0, sizeof(int64_t), st));
-        k_row_count<<<grid_for(n, 256), 256, 0, st>>>(n, g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(),
-                                                      cnt.get());
+        k_tile_axis_keys<<<grid_for(n, 256), 256, 0, st>>>(n, g.axis.get(), keys.get());
         SC_LAUNCH_CK();
-        cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.get(), L.rowptr.get(), n + 1, st);
-        cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, cnt.get(), L.rowptr.get(), n + 1, st);
+        int end_bit = 2;
+        while (end_bit < 32 && ((uint64_t)1 << (end_bit - 2)) * STENCIL_TILE <= (uint64_t)n) end_bit++;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys_out.get(), ids.get(), ids_out.get(), n, 0,
+                                        end_bit, st);
+        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, keys.get(), keys_out.get(), ids.get(),
+                                        ids_out.get(), n, 0, end_bit, st);
+        g.perm = std::move(ids_out);
+        g.axis_off[0] = 0;
+        g.axis_off[1] = g.axis_off[2] = g.axis_off[3] = n;
     }
-    SC_CK(cudaMemcpyAsync(&L.nnzb, L.rowptr.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    SC_CK(cudaStreamSynchronize(st));
-    L.col.alloc(L.nnzb, st, ms);
-    L.val.alloc(36 * L.nnzb, st, ms);
-    k_row_fill<<<grid_for(n, 128), 128, 0, st>>>(n, g.s, g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(),
-                                                 L.rowptr.get(), L.col.get(), L.val.get());
-    SC_LAUNCH_CK();
+    // assembled blocks for the setup (the solve itself applies level 0 matrix-free)
+    if (keep_blocks) {
+        L.rowptr.alloc(n + 1, st, ms);
+        {
+            DBuf<int64_t> cnt;
+            cnt.alloc(n + 1, st, ms);
+            SC_CK(cudaMemsetAsync(cnt.get() + n, 0, sizeof(int64_t), st));
+            k_row_count<<<grid_for(n, 256), 256, 0, st>>>(n, g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(),
+                                                          cnt.get());
+            SC_LAUNCH_CK();
+            cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.get(), L.rowptr.get(), n + 1, st);
+            cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, cnt.get(), L.rowptr.get(), n + 1, st);
+        }
+        SC_CK(cudaMemcpyAsync(&L.nnzb, L.rowptr.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        SC_CK(cudaStreamSynchronize(st));
+        L.col.alloc(L.nnzb, st, ms);
+        L.val.alloc(36 * L.nnzb, st, ms);
+        k_row_fill<<<grid_for(n, 128), 128, 0, st>>>(n, g.s, g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(),
+                                                     L.rowptr.get(), L.col.get(), L.val.get());
+        SC_LAUNCH_CK();
+    }
     L.matrix_free = true;
     g.grid_off = std::move(goff);
-    (void)keep_blocks;
     SC_CK(cudaStreamSynchronize(st));
 }
 

@@ -748,13 +748,12 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     k_centroid<<<grid_for(nc, 128), 128, 0, st>>>(nc, moff.get(), mem_part.get(), F.centre.get(), F.site.get(),
                                                   F.piece.get(), C.centre.get(), C.site.get(), C.piece.get());
     SC_LAUNCH_CK();
-    mem_part.release();
     mem_body.release();
-    moff.release();
     DBuf<double> rvec;
     rvec.alloc(3 * n, st, ms);
     k_rvec<<<grid_for(n, 256), 256, 0, st>>>(n, F.up.get(), F.centre.get(), C.centre.get(), rvec.get());
     SC_LAUNCH_CK();
+    bool keep_mf = l == 0 && F.matrix_free;
 
     // --- P pattern and values
     DBuf<int64_t> cnt, off;
@@ -778,7 +777,15 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
                                                    rvec.get(), F.inv.get(), F.step.get(), F.piece.get(), F.prow.get(),
                                                    F.pcol.get(), F.pval.get());
     SC_LAUNCH_CK();
-    rvec.release();
+    if (keep_mf) {
+        F.mf_r = std::move(rvec);
+        F.mem_off = std::move(moff);
+        F.mem = std::move(mem_part);
+    } else {
+        rvec.release();
+        moff.release();
+        mem_part.release();
+    }
     // P transposed: entries sorted by column, stable (fine-row order within a column)
     {
         DBuf<int32_t> prow_of;
@@ -987,6 +994,21 @@ void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
         }
         build_top(ctx, b, l, tops);
         if (!more) break;
+    }
+    // a matrix-free level 0 keeps only what the solve reads: the assembled blocks, their
+    // inverses and the explicit prolongator served the setup alone
+    if (b.levels[0].matrix_free && b.levels.size() > 1) {
+        Level& L0 = b.levels[0];
+        L0.val.release();
+        L0.col.release();
+        L0.rowptr.release();
+        L0.inv.release();
+        L0.pval.release();
+        L0.pcol.release();
+        L0.prow.release();
+        L0.tptr.release();
+        L0.tent.release();
+        L0.trow.release();
     }
     b.piece_levels.assign(np, 0);
     for (size_t l = 0; l < b.levels.size(); l++)

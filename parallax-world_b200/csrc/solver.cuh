@@ -24,8 +24,8 @@ struct Grid0 {
     int64_t ncells = 0;
     double s = 0.125;           // spacing (statics/src/lattice.rs:16, 34-36)
     DBuf<int4> cell;            // 2 int4 per free cell: part ids of slots 0..5 (-1 held), k bits, 0
-    DBuf<int32_t> perm;         // parts grouped by axis, each group padded to a multiple of 32 with -1
-    int64_t axis_off[4] = {0, 0, 0, 0};
+    DBuf<int32_t> perm;         // parts in order, grouped by axis inside tiles of 1024 parts
+    int64_t axis_off[4] = {0, 0, 0, 0};  // axis_off[3]: parts in perm
     DBuf<int32_t> cella, cellb; // per part: its lesser cell (node is that cell's + face) and greater cell; -1 if not free
     DBuf<int8_t> axis;          // per part
     DBuf<int64_t> cell_flat;    // per free cell: its flat index in the batch's concatenated grids
@@ -74,9 +74,17 @@ struct Level {
     DBuf<double> kinv;
     DBuf<int32_t> top_of_part;       // per part: 1 if its piece tops out here
 
-    // cycle work vectors (levels >= 1 keep r and z for the level above)
-    DBuf<double> r, x, left, z;
-    DBuf<float> r32, x32, left32, z32;
+    // level 0 of voxel pieces: matrix-free transfers need each part's offset from its
+    // body's centroid and the bodies' member lists (parts in order)
+    DBuf<double> mf_r;
+    DBuf<float> mf_r32;
+    DBuf<int64_t> mem_off;
+    DBuf<int32_t> mem;
+
+    // cycle work vectors (levels >= 1 keep r and z for the level above; level 0 of
+    // voxel pieces also t and u)
+    DBuf<double> r, x, left, z, t, u;
+    DBuf<float> r32, x32, left32, z32, t32, u32;
 };
 
 struct Batch {
@@ -107,6 +115,10 @@ template <class T>
 void stencil_residual(Context& ctx, const Batch& b, const T* x, const T* r, T* y, const int32_t* skip_row,
                       const int32_t* done);
 void grid_cell_energy(Context& ctx, const Batch& b, const double* x, double* energy_cells);
+template <class T>
+void level0_down(Context& ctx, const Batch& b, const T* r, T* x, T* left, T* t, T* u, T* rc, const int32_t* done);
+template <class T>
+void level0_up(Context& ctx, const Batch& b, const T* r, T* x, T* e, const T* zc, T* z, const int32_t* done);
 
 // --- lattice.cu -----------------------------------------------------------------------
 void lattice_level0(Context& ctx, Batch& b, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,
