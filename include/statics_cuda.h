@@ -195,6 +195,27 @@ int64_t sc_launches(void);
 /* The CUDA stream (cudaStream_t) the context launches on. */
 sc_status sc_context_stream(sc_context* ctx, void** stream);
 
+/* ---------------------------------------------------------------------------
+ * Compliance without device allocation. No counterpart in the reference.
+ *
+ * For callers that must not have the library allocate device memory: an engine that
+ * owns the GPU's memory through its own arena, code running while its caller captures
+ * a CUDA graph, or a per-frame loop that cannot afford cudaMalloc's implicit device
+ * synchronisation. It computes C = f . u (n_values doubles each, device pointers; e.g.
+ * the loads and the motions of sc_solve_grid, node order) into *compliance (a device
+ * pointer), on `stream` (a cudaStream_t; NULL = the legacy default stream), with the
+ * solver's deterministic chunked sum, and allocates nothing: its partial sums live in
+ * one 512 KB array inside the library, reserved on every GPU that loads it until the
+ * process exits. At most SC_NOALLOC_MAX_VALUES values (SC_BAD_INPUT beyond).
+ * The first call on a device looks that array up for the device (do it before any
+ * stream capture). Every call shares the array: calls whose kernels may overlap on the
+ * GPU race and can return wrong sums, so order them on one stream. Asynchronous:
+ * *compliance is ready when `stream` reaches this point.
+ * ------------------------------------------------------------------------- */
+#define SC_NOALLOC_MAX_VALUES (8192LL * 65536LL)
+sc_status sc_compliance_noalloc(const double* loads, const double* motions, int64_t n_values, double* compliance,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,6 +112,8 @@ def lib():
         L.sc_launches.restype = C.c_int64
         L.sc_launches.argtypes = []
         L.sc_context_stream.argtypes = [P, C.POINTER(P)]
+        L.sc_compliance_noalloc.argtypes = [P, P, C.c_int64, P, P]
+        L.sc_compliance_noalloc.restype = C.c_int
         for name in ("sc_profile", "sc_profile_read", "sc_context_stream"):
             getattr(L, name).restype = C.c_int
         for name in ("sc_create", "sc_generate_piece", "sc_grid_count", "sc_solve_grid", "sc_solve_grid_batch",
@@ -159,6 +161,18 @@ def make_grid(state: np.ndarray, k: np.ndarray, g_over_e=0.4, rho=512.0, gravity
 def launches() -> int:
     """Kernels the library has launched in this process."""
     return int(lib().sc_launches())
+
+
+NOALLOC_MAX_VALUES = 8192 * 65536
+
+
+def compliance_noalloc(loads_ptr: int, motions_ptr: int, n_values: int, out_ptr: int, stream: int = 0) -> int:
+    """C = f . u of two device arrays into a device double, allocating no device memory
+    (sc_compliance_noalloc). For callers that cannot let the library allocate: engines
+    that own the GPU's memory, code inside a graph capture, frame loops. Returns the
+    status; the result is ready when `stream` gets there."""
+    return int(lib().sc_compliance_noalloc(C.c_void_p(loads_ptr), C.c_void_p(motions_ptr), n_values,
+                                           C.c_void_p(out_ptr), C.c_void_p(stream or None)))
 
 
 def grid_count(state: np.ndarray):
