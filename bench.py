@@ -31,6 +31,7 @@ METRIC = "DOF·iters/s & solves/s to 1e-8 rel residual: mixed vs FP64 GPU vs CPU
 N = 128
 TOL = 1e-8
 SAMPLE_N, SAMPLE_SEED = 48, 5  # the CPU legs' bounded sample
+EDGES = (16, 24, 32, 48, 64)   # edge lengths of the batched pieces
 
 
 def peaks():
@@ -39,6 +40,11 @@ def peaks():
         return float(m["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def rank_seed(base, rank):
+    """Each rank solves its own piece: weak scaling, no collective on the data path."""
+    return base + rank
 
 
 def workload(seed):
@@ -96,7 +102,8 @@ def max_over_ranks(v, world):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -184,7 +191,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     solver = sc.Solver(local)
-    seed = args.seed + rank
+    seed = rank_seed(args.seed, rank)
     state, k = sc.generate_piece(N, N, N, seed, sc.K_UNIFORM)
     n_nodes, n_parts = sc.grid_count(state)
     st_d = torch.from_numpy(state).cuda()
@@ -276,6 +283,8 @@ def run_ours(args):
         "clocks": clk,
         "peak_hbm_bytes": infos_m[-1]["peak_bytes"],
     }
+    if not args.no_batch:
+        line["batch"] = batch_section(solver, sc, rank, world, args)
     if rank == 0 and world == 1 and not args.no_cpu:
         s = cpu_sample()
         line["cpu_baseline"] = cpu_baseline_obj(s, dof * it_64)
@@ -288,12 +297,21 @@ def run_ours(args):
 
 
 def run_probe(args):
-    """Only the level-0 stencil on the bench's piece (FP64 then FP32), two launches
-    each: the small command an ncu capture of that kernel runs."""
+    """One kernel or one solve alone, for profiling: `stencil` applies the level-0
+    stencil to the bench's piece (FP64 then FP32, two launches each); `solve` runs one
+    FP64 and one mixed solve of it."""
     import numpy as np
 
     import statics_cuda as sc
     state, k = sc.generate_piece(N, N, N, args.seed, sc.K_UNIFORM)
+    if args.probe == "solve":
+        solver = sc.Solver(0)
+        for prec in (sc.FP64, sc.MIXED):
+            _, info = solver.solve_grid(state, k, sc.options(tol=TOL, precision=prec))
+            print(json.dumps({"probe": "solve", "precision": prec, "iterations": info["iterations"],
+                              "setup_ms": info["setup_ms"], "solve_ms": info["solve_ms"]}))
+        solver.close()
+        return
     _, parts = sc.grid_count(state)
     x = np.random.default_rng(0).standard_normal((parts, 6))
     solver = sc.Solver(0)
@@ -304,6 +322,58 @@ def run_probe(args):
     solver.close()
 
 
+def batch_section(solver, sc, rank, world, args):
+    """Many pieces of uneven size: BATCH pieces whose edges are drawn from EDGES per axis
+    (seeded per rank), solved by the autotuned mixed-precision batched solve; against the
+    plain FP64 drop-in solving them one call at a time (a seeded sample of them)."""
+    import numpy as np
+    import torch
+
+    from statics_cuda import autotune
+    rng = np.random.default_rng(777 + rank)
+    pieces = []
+    for i in range(args.batch):
+        nx, ny, nz = (int(v) for v in rng.choice(EDGES, 3))
+        pieces.append(sc.generate_piece(nx, ny, nz, 10_000 + args.batch * rank + i, sc.K_UNIFORM))
+    dof = sum(6 * sc.grid_count(p[0])[1] for p in pieces)
+    t = time.perf_counter()
+    settings = autotune.choose(solver, pieces, sc.MIXED, TOL)
+    tune_s = time.perf_counter() - t
+    stream = torch.cuda.ExternalStream(solver.stream())
+    autotune.solve_batch(solver, pieces[: min(8, len(pieces))], sc.MIXED, TOL, settings=settings)  # warm-up
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _, infos = autotune.solve_batch(solver, pieces, sc.MIXED, TOL, settings=settings)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_b = max_over_ranks(e0.elapsed_time(e1), world)
+    sample = pieces[: min(args.batch_sample, len(pieces))]
+    opt64 = sc.options(tol=TOL, precision=sc.FP64)
+    solver.solve_grid(*sample[0], opt64)  # warm-up
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for st, k in sample:
+        solver.solve_grid(st, k, opt64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_1 = max_over_ranks(e0.elapsed_time(e1), world)
+    batched = world * len(pieces) / (ms_b / 1000.0)
+    single = world * len(sample) / (ms_1 / 1000.0)
+    bad = sum(1 for i in infos if i["status"] != 0 or i["residual"] > TOL * 1.0001)
+    return {"workload": f"{len(pieces)} pieces per rank, edges from {list(EDGES)} per axis, seeds 10000+; "
+                        f"value noise period 8 thr 0.5, k U[0.5,2], tol {TOL:g}",
+            "pieces": len(pieces), "dof": dof, "mixed_batched_solves_per_s": batched,
+            "fp64_single_solves_per_s": single, "fp64_single_sample": len(sample),
+            "speedup_batched_mixed_vs_fp64_single": batched / single,
+            "mixed_batched_ms": ms_b, "iterations_mean": float(np.mean([i["iterations"] for i in infos])),
+            "pieces_not_converged": bad, "autotune": {str(k): {"sweeps": v["sweeps"], "tile": v["tile"]}
+                                                       for k, v in settings.items()},
+            "autotune_seconds": tune_s}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -312,7 +382,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--probe", choices=["stencil"], help="run one kernel alone (for profiling)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-pieces section")
+    ap.add_argument("--batch", type=int, default=512, help="pieces in the batched section")
+    ap.add_argument("--batch-sample", type=int, default=64, help="pieces the one-at-a-time FP64 leg solves")
+    ap.add_argument("--probe", choices=["stencil", "solve"], help="run one kernel or one solve alone (profiling)")
     args = ap.parse_args()
     if args.probe:
         run_probe(args)

@@ -46,6 +46,9 @@ typedef struct sc_options {
                           reference does 1 (bodies.rs:386, 397-401) */
     double inner_tol;  /* SC_MIXED: relative residual each FP32 inner solve stops at */
     int64_t timeout_ms;/* wall-clock bound of one call; 0 = none */
+    int32_t tile;      /* voxel pieces: parts per stencil tile (the window in which parts are
+                          grouped by axis); 0 = 1024 */
+    int32_t reserved;
 } sc_options;
 
 /* The reference's constants (tol 1e-6, FEW 64, cap 100000, one sweep), FP64. */
@@ -97,6 +100,8 @@ typedef struct sc_grid {
     double rho;           /* density; 512 gives a level-0 cell (0.125 m) a mass of 1 */
     double gravity[3];    /* load per unit mass, e.g. {0, 0, -1} */
     int32_t on_device;    /* state and k are device pointers */
+    const double* loads;  /* optional: 6 per node (node order), used instead of mass * gravity;
+                             host memory, or device memory when on_device */
 } sc_grid;
 
 /* Seeded synthetic piece: value noise of period 8, threshold 0.5, bottom z layer held,

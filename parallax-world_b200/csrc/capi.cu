@@ -152,6 +152,9 @@ void check_options(const sc_options& o) {
     require(o.max_iter >= 0, SC_BAD_INPUT, "max_iter must be non-negative");
     require(o.few >= 1, SC_BAD_INPUT, "few must be at least 1");
     require(o.precision == SC_FP64 || o.precision == SC_MIXED, SC_BAD_INPUT, "unknown precision");
+    require(o.sweeps >= 1 && o.sweeps <= 8, SC_BAD_INPUT, "sweeps must be 1 to 8");
+    require(o.tile == 0 || (o.tile >= 32 && o.tile <= (1 << 20) && (o.tile & (o.tile - 1)) == 0), SC_BAD_INPUT,
+            "tile must be 0 or a power of two from 32");
 }
 
 // The reference's Work for a solve of one piece: parts + pairs per level apply
@@ -208,6 +211,7 @@ void read_steps(Context& ctx, const Batch& b, int piece, sc_solve_info* info) {
 
 // Solves a batch already at level 0; returns per-piece statuses.
 sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st, double& solve_ms) {
+    b.sweeps = opt.sweeps;
     build_hierarchy(ctx, b, opt);
     auto t0 = std::chrono::steady_clock::now();
     if (opt.precision == SC_MIXED)
@@ -238,6 +242,8 @@ void sc_default_options(sc_options* o) {
     o->sweeps = 1;
     o->inner_tol = 1e-4;
     o->timeout_ms = 0;
+    o->tile = 0;
+    o->reserved = 0;
 }
 
 const char* sc_status_string(sc_status s) {
@@ -322,7 +328,7 @@ sc_status sc_solve_grid(sc_context* ctx, const sc_grid* g, const sc_options* opt
         check_options(*opt);
         auto b = std::make_unique<Batch>();
         c.mem.peak = c.mem.now;
-        grid_level0(c, *b, {*g}, true);
+        grid_level0(c, *b, {*g}, true, opt->tile);
         int64_t nodes = b->node_count[0];
         require(capacity >= 6 * nodes, SC_BAD_INPUT, "motions buffer holds fewer than 6 * n_nodes values");
         DBuf<double> x;
@@ -349,6 +355,10 @@ sc_status sc_solve_grid(sc_context* ctx, const sc_grid* g, const sc_options* opt
     return s != SC_OK ? s : solve_status;
 }
 
+// Pieces per batched solve are grouped so that a group's hierarchy setup stays within
+// device memory: at most this many grid cells a group (a 128^3 piece is 2.1 M).
+static const int64_t BATCH_CELLS = 5LL << 20;
+
 sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, const sc_options* opt,
                               double* const* motions, sc_solve_info* infos) {
     if (n <= 0 || !grids || !opt || !motions) return SC_BAD_INPUT;
@@ -356,37 +366,55 @@ sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, 
     sc_status s = guarded(ctx, [&] {
         Context& c = ctx->c;
         check_options(*opt);
-        std::vector<sc_grid> gs(grids, grids + n);
-        for (auto& g : gs) check_grid(g);
-        auto b = std::make_unique<Batch>();
+        std::vector<sc_grid> all(grids, grids + n);
+        for (auto& g : all) check_grid(g);
         c.mem.peak = c.mem.now;
-        grid_level0(c, *b, gs, true);
-        DBuf<double> x;
-        SolveStats st;
-        double solve_ms = 0;
-        solve_status = solve_batch(c, *b, *opt, x, st, solve_ms);
-        int64_t total = 0;
-        std::vector<int64_t> start(n + 1, 0);
-        for (int p = 0; p < n; p++) start[p + 1] = start[p] + b->node_count[p];
-        total = start[n];
-        DBuf<double> out;
-        out.alloc(6 * std::max<int64_t>(total, 1), c.stream, &c.mem);
-        out.zero();
-        const Level& L = b->levels[0];
-        k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(),
-                                                             b->part_node.get(), x.get(), out.get());
-        SC_LAUNCH_CK();
-        for (int p = 0; p < n; p++)
-            if (motions[p])
-                SC_CK(cudaMemcpyAsync(motions[p], out.get() + 6 * start[p], 6 * b->node_count[p] * sizeof(double),
-                                      cudaMemcpyDeviceToHost, c.stream));
-        SC_CK(cudaStreamSynchronize(c.stream));
-        if (infos)
-            for (int p = 0; p < n; p++) {
-                fill_info(*b, p, st, infos + p, solve_ms, c.mem.peak);
-                read_steps(c, *b, p, infos + p);
+        int first = 0;
+        while (first < n) {
+            // the next group: consecutive pieces up to the cell budget (at least one)
+            int last = first;
+            int64_t cells = 0;
+            while (last < n) {
+                int64_t gc = (int64_t)all[last].nx * all[last].ny * all[last].nz;
+                if (last > first && cells + gc > BATCH_CELLS) break;
+                cells += gc;
+                last++;
             }
-        c.last = std::move(b);
+            std::vector<sc_grid> gs(all.begin() + first, all.begin() + last);
+            int m = last - first;
+            auto b = std::make_unique<Batch>();
+            grid_level0(c, *b, gs, true, opt->tile);
+            DBuf<double> x;
+            SolveStats st;
+            double solve_ms = 0;
+            sc_status gsts = solve_batch(c, *b, *opt, x, st, solve_ms);
+            solve_status = std::max(solve_status, gsts);
+            std::vector<int64_t> start(m + 1, 0);
+            for (int p = 0; p < m; p++) start[p + 1] = start[p] + b->node_count[p];
+            int64_t total = start[m];
+            DBuf<double> out;
+            out.alloc(6 * std::max<int64_t>(total, 1), c.stream, &c.mem);
+            out.zero();
+            const Level& L = b->levels[0];
+            k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(),
+                                                                 b->part_node.get(), x.get(), out.get());
+            SC_LAUNCH_CK();
+            for (int p = 0; p < m; p++)
+                if (motions[first + p])
+                    SC_CK(cudaMemcpyAsync(motions[first + p], out.get() + 6 * start[p],
+                                          6 * b->node_count[p] * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+            SC_CK(cudaStreamSynchronize(c.stream));
+            if (infos) {
+                for (int p = 0; p < m; p++) fill_info(*b, p, st, infos + first + p, solve_ms, c.mem.peak);
+                for (size_t l = 0; l < b->levels.size() && l < SC_MAX_LEVELS; l++) {
+                    std::vector<double> steps = b->levels[l].step.to_host();
+                    for (int p = 0; p < m; p++)
+                        if ((int)l < infos[first + p].levels) infos[first + p].steps[l] = steps[p];
+                }
+            }
+            c.last = std::move(b);
+            first = last;
+        }
     });
     return s != SC_OK ? s : solve_status;
 }
@@ -402,7 +430,7 @@ sc_status sc_compliance_grad(sc_context* ctx, const sc_grid* g, const sc_options
         require(!g->on_device, SC_BAD_INPUT, "sc_compliance_grad takes host grids");
         auto b = std::make_unique<Batch>();
         c.mem.peak = c.mem.now;
-        grid_level0(c, *b, {*g}, true);
+        grid_level0(c, *b, {*g}, true, opt->tile);
         int64_t nodes = b->node_count[0];
         require(!motions || capacity >= 6 * nodes, SC_BAD_INPUT, "motions buffer too small");
         DBuf<double> x;
@@ -452,7 +480,7 @@ sc_status sc_grid_apply(sc_context* ctx, const sc_grid* g, int32_t precision, co
         Context& c = ctx->c;
         check_grid(*g);
         Batch b;
-        grid_level0(c, b, {*g}, false);
+        grid_level0(c, b, {*g}, false, 0);
         const Level& L = b.levels[0];
         int64_t n6 = 6 * L.n;
         DBuf<double> x, y;

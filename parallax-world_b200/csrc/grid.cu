@@ -42,9 +42,18 @@ __global__ void k_iota(int64_t n, int32_t* __restrict__ v) {
 
 constexpr int64_t STENCIL_TILE = 1024;
 
-__global__ void k_tile_axis_keys(int64_t n, const int8_t* __restrict__ axis, uint32_t* __restrict__ keys) {
+__global__ void k_tile_axis_keys(int64_t n, int64_t tile, const int8_t* __restrict__ axis, uint32_t* __restrict__ keys) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k < n) keys[k] = (uint32_t)(((k / STENCIL_TILE) << 2) | (uint32_t)axis[k]);
+    if (k < n) keys[k] = (uint32_t)(((k / tile) << 2) | (uint32_t)axis[k]);
+}
+
+// the stencil's per-slot record: part, lesser cell, greater cell, axis
+__global__ void k_slots(int64_t n, const int32_t* __restrict__ perm, const int32_t* __restrict__ cella,
+                        const int32_t* __restrict__ cellb, const int8_t* __restrict__ axis, int4* __restrict__ slots) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int32_t k = perm[i];
+    slots[i] = make_int4(k, cella[k], cellb[k], (int)axis[k]);
 }
 
 struct Dims {
@@ -194,15 +203,40 @@ __global__ void k_part_data(int64_t nnodes, int np, const int64_t* __restrict__ 
     loads[6 * k + 5] = 0.0;
 }
 
-__global__ void k_cell_table(int64_t ncells, const int64_t* __restrict__ cell_node6, const int32_t* __restrict__ node_part,
-                             const int64_t* __restrict__ cell_flat, const float* __restrict__ gk, int4* __restrict__ cell) {
+// per free cell: its six faces' parts (-1 held), k, and bit a set when its +a
+// neighbour is free
+__global__ void k_cell_table(int np, const int64_t* __restrict__ goff, const Dims* __restrict__ dims,
+                             const uint8_t* __restrict__ st, int64_t ncells, const int64_t* __restrict__ cell_node6,
+                             const int32_t* __restrict__ node_part, const int64_t* __restrict__ cell_flat,
+                             const float* __restrict__ gk, int4* __restrict__ cell) {
     int64_t ci = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (ci >= ncells) return;
     int32_t q[6];
     for (int s = 0; s < 6; s++) q[s] = node_part[cell_node6[6 * ci + s]];
-    float k = gk[cell_flat[ci]];
+    int64_t c = cell_flat[ci];
+    float k = gk[c];
+    int p = find_piece(goff, np, c);
+    Dims d = dims[p];
+    int64_t l = c - goff[p];
+    int z = (int)(l % d.nz), y = (int)(l / d.nz % d.ny), x = (int)(l / ((int64_t)d.nz * d.ny));
+    const uint8_t* sp = st + goff[p];
+    int nbr = (is_free(sp, d, x + 1, y, z) ? 1 : 0) | (is_free(sp, d, x, y + 1, z) ? 2 : 0) |
+              (is_free(sp, d, x, y, z + 1) ? 4 : 0);
     cell[2 * ci] = make_int4(q[0], q[1], q[2], q[3]);
-    cell[2 * ci + 1] = make_int4(q[4], q[5], __float_as_int(k), 0);
+    cell[2 * ci + 1] = make_int4(q[4], q[5], __float_as_int(k), nbr);
+}
+
+__global__ void k_gridmap(int64_t ncell, const int64_t* __restrict__ free_flag, const int64_t* __restrict__ cell_index,
+                          int32_t* __restrict__ gridmap) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c < ncell) gridmap[c] = free_flag[c] ? (int32_t)cell_index[c] : -1;
+}
+
+__global__ void k_node_loads(int64_t n, const int32_t* __restrict__ part_node, const double* __restrict__ node_loads,
+                             double* __restrict__ loads) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    for (int q = 0; q < 6; q++) loads[6 * k + q] = node_loads[6 * (int64_t)part_node[k] + q];
 }
 
 __global__ void k_cell_flat(int64_t ncell, const int64_t* __restrict__ free_flag, const int64_t* __restrict__ cell_index,
@@ -341,31 +375,38 @@ __device__ __forceinline__ void store6(T* __restrict__ v, int64_t k, const T (&o
     }
 }
 
-// t += TPL block (SLOT, F) * x_F for faces F.., each face's six values loaded on its
-// own (rotations scaled by s) so few registers stay live.
+// t += sum over the six faces F of TPL block (SLOT, F) * x_F. The six faces' loads are
+// issued together, branch-free (a held face reads the part's own x and is masked to
+// zero), so a thread waits for one round of gathers per cell.
 template <int SLOT, int F, class T>
-__device__ __forceinline__ void faces(const int32_t (&q)[6], const T* __restrict__ x, T s, T (&t)[6]) {
+__device__ __forceinline__ void face_macs(const T (&xs)[6][6], T (&t)[6]) {
     if constexpr (F < 6) {
-        if (q[F] >= 0) {
-            T xv[6];
-            load6<T>(x, q[F], xv);
-            xv[3] *= s;
-            xv[4] *= s;
-            xv[5] *= s;
-            Blk<SLOT, F>::mac(xv, t);
-        }
-        faces<SLOT, F + 1, T>(q, x, s, t);
+        Blk<SLOT, F>::mac(xs[F], t);
+        face_macs<SLOT, F + 1, T>(xs, t);
     }
 }
 
 // acc += k_C * (row strip SLOT of cell C's template) * (x of C's six faces)
 template <int SLOT, class T>
-__device__ __forceinline__ void cell_term(const int4* __restrict__ cell, int32_t C, T kc, const T* __restrict__ x,
-                                          T s, T (&acc)[6]) {
-    int4 a = __ldg(cell + 2 * C), b = __ldg(cell + 2 * C + 1);
+__device__ __forceinline__ void cell_term(int4 a, int4 b, int32_t self, T kc, const T* __restrict__ x, T s,
+                                          T (&acc)[6]) {
     int32_t q[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+    T xs[6][6];
+#pragma unroll
+    for (int f = 0; f < 6; f++) load6<T>(x, q[f] >= 0 ? q[f] : self, xs[f]);
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        T m = q[f] >= 0 ? T(1) : T(0);
+        T ms = m * s;
+        xs[f][0] *= m;
+        xs[f][1] *= m;
+        xs[f][2] *= m;
+        xs[f][3] *= ms;
+        xs[f][4] *= ms;
+        xs[f][5] *= ms;
+    }
     T t[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    faces<SLOT, 0, T>(q, x, s, t);
+    face_macs<SLOT, 0, T>(xs, t);
 #pragma unroll
     for (int i = 0; i < 6; i++) acc[i] = fma(kc, t[i], acc[i]);
 }
@@ -404,14 +445,14 @@ __device__ __forceinline__ void dinv(T kA, T kB, T s, const T (&v)[6], T (&y)[6]
 enum { ST_Y = 0, ST_RES = 1, ST_RES_JAC = 2, ST_RES_W = 3, ST_PROLONG = 4, ST_SMOOTH = 5 };
 
 template <int AX, class T, int MODE>
-__device__ __forceinline__ void stencil_row(int32_t k, int32_t A, int32_t B, const int4* __restrict__ cell,
+__device__ __forceinline__ void stencil_row(int32_t k, int32_t A, int32_t B, int4 a0, int4 a1, int4 b0, int4 b1,
                                             const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
                                             T* __restrict__ y2, T s, T w) {
-    T kA = A >= 0 ? (T)__int_as_float(__ldg(&cell[2 * A + 1].z)) : T(0);
-    T kB = B >= 0 ? (T)__int_as_float(__ldg(&cell[2 * B + 1].z)) : T(0);
+    T kA = A >= 0 ? (T)__int_as_float(a1.z) : T(0);
+    T kB = B >= 0 ? (T)__int_as_float(b1.z) : T(0);
     T acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    if (A >= 0) cell_term<2 * AX + 1, T>(cell, A, kA, x, s, acc);
-    if (B >= 0) cell_term<2 * AX, T>(cell, B, kB, x, s, acc);
+    if (A >= 0) cell_term<2 * AX + 1, T>(a0, a1, k, kA, x, s, acc);
+    if (B >= 0) cell_term<2 * AX, T>(b0, b1, k, kB, x, s, acc);
     T kx[6] = {acc[0] * s, acc[1] * s, acc[2] * s, acc[3] * s * s, acc[4] * s * s, acc[5] * s * s};
     T o[6];
     if constexpr (MODE == ST_Y) {
@@ -457,28 +498,263 @@ __device__ __forceinline__ void stencil_row(int32_t k, int32_t A, int32_t B, con
 
 // Level 0 applied matrix-free over the parts grouped by axis (perm).
 template <class T, int MODE>
-__global__ void __launch_bounds__(256, 3) k_stencil(int64_t n_perm, const int32_t* __restrict__ perm,
-                                                 const int8_t* __restrict__ axis, const int32_t* __restrict__ cella,
-                                                 const int32_t* __restrict__ cellb, const int4* __restrict__ cell,
+__global__ void __launch_bounds__(256, 2) k_stencil(int64_t n_perm, const int4* __restrict__ slots,
+                                                 const int4* __restrict__ cell,
                                                  const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
                                                  T* __restrict__ y2, T s, const int32_t* __restrict__ piece,
                                                  const double* __restrict__ step, const int32_t* __restrict__ skip_row,
                                                  const int32_t* __restrict__ done) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n_perm) return;
-    int32_t k = perm[i];
+    int4 sl = __ldg(slots + i);  // part, lesser cell, greater cell, axis
+    int32_t k = sl.x, A = sl.y, B = sl.z;
     if (skip_row && skip_row[k]) return;
     int p = (done || step) ? piece[k] : 0;
     if (done && done[p]) return;
     T w = step ? (T)step[p] : T(0);
-    int32_t A = cella[k], B = cellb[k];
-    int ax = axis[k];
-    if (ax == 0)
-        stencil_row<0, T, MODE>(k, A, B, cell, x, r, y, y2, s, w);
-    else if (ax == 1)
-        stencil_row<1, T, MODE>(k, A, B, cell, x, r, y, y2, s, w);
+    int32_t Ac = A >= 0 ? A : 0, Bc = B >= 0 ? B : 0;
+    int4 a0 = __ldg(cell + 2 * Ac), a1 = __ldg(cell + 2 * Ac + 1);
+    int4 b0 = __ldg(cell + 2 * Bc), b1 = __ldg(cell + 2 * Bc + 1);
+    if (sl.w == 0)
+        stencil_row<0, T, MODE>(k, A, B, a0, a1, b0, b1, x, r, y, y2, s, w);
+    else if (sl.w == 1)
+        stencil_row<1, T, MODE>(k, A, B, a0, a1, b0, b1, x, r, y, y2, s, w);
     else
-        stencil_row<2, T, MODE>(k, A, B, cell, x, r, y, y2, s, w);
+        stencil_row<2, T, MODE>(k, A, B, a0, a1, b0, b1, x, r, y, y2, s, w);
+}
+
+// ---- the plane-pencil stencil ------------------------------------------------------
+// A block owns a PTY x PTZ tile of (y, z) cells of one piece and walks PSX planes of x.
+// Each free cell's six faces are gathered once per plane and all six of its template
+// strips computed (Y_s = k * strip_s * x~, s = slot): its +y / +z strips go to shared
+// memory for the neighbour threads, its +x strip stays in a register for the next plane.
+// Every part is written once, by its greater cell (the - face; a + face only where the
+// greater cell is not free): Kx of the part on the face between cells L and G along axis
+// a is Y_L[2a+1] + Y_G[2a]. A warp of the block recomputes the +y strips of the row
+// before the tile and one the +z strips of the column before it; the first plane's +x
+// strips come from recomputing the plane before the segment. So a cell is gathered
+// about 1 + 1/PSX + 1/PTY + 1/PTZ times instead of six (once per part that touches it).
+constexpr int PTY = 8, PTZ = 32, PSX = 16;
+constexpr int PENCIL_THREADS = (PTY + 2) * 32;  // 8 tile warps, a +y halo warp, a +z halo warp
+
+struct PencilTile {
+    int32_t piece, x0, y0, z0;
+};
+struct PieceGeo {
+    int32_t nx, ny, nz, pad;
+    int64_t goff;  // first flat cell of the piece
+};
+
+// Y[slot] += k * strip(slot) * x~ for all six slots
+template <int SLOT, class T>
+__device__ __forceinline__ void slot_out(const T (&xs)[6][6], T kc, T s, T (&y)[6]) {
+    T t[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    face_macs<SLOT, 0, T>(xs, t);
+    y[0] = kc * t[0] * s;
+    y[1] = kc * t[1] * s;
+    y[2] = kc * t[2] * s;
+    y[3] = kc * t[3] * s * s;
+    y[4] = kc * t[4] * s * s;
+    y[5] = kc * t[5] * s * s;
+}
+
+template <class T>
+__device__ __forceinline__ void gather_cell(int4 a, int4 b, const T* __restrict__ x, T s, T (&xs)[6][6]) {
+    int32_t q[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+#pragma unroll
+    for (int f = 0; f < 6; f++) load6<T>(x, q[f] >= 0 ? q[f] : 0, xs[f]);
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        T m = q[f] >= 0 ? T(1) : T(0);
+        T ms = m * s;
+        xs[f][0] *= m;
+        xs[f][1] *= m;
+        xs[f][2] *= m;
+        xs[f][3] *= ms;
+        xs[f][4] *= ms;
+        xs[f][5] *= ms;
+    }
+}
+
+// the part's epilogue given its Kx, its axis and the stiffness of its lesser / greater cell
+template <int AX, class T, int MODE>
+__device__ __forceinline__ void pencil_finish(int32_t q, const T (&kx)[6], T kA, T kB, T s, T w,
+                                              const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
+                                              T* __restrict__ y2) {
+    T o[6];
+    if constexpr (MODE == ST_Y) {
+        store6<T>(y, q, kx);
+    } else if constexpr (MODE == ST_RES) {
+        load6<T>(r, q, o);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] -= kx[j];
+        store6<T>(y, q, o);
+    } else if constexpr (MODE == ST_RES_JAC) {
+        load6<T>(r, q, o);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] -= kx[j];
+        store6<T>(y, q, o);
+        T d[6];
+        dinv<AX, T>(kA, kB, s, o, d);
+        store6<T>(y2, q, d);
+    } else if constexpr (MODE == ST_RES_W) {
+        load6<T>(r, q, o);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] = fma(-w, kx[j], o[j]);
+        store6<T>(y, q, o);
+    } else if constexpr (MODE == ST_PROLONG) {
+        T d[6], xv[6], acc2[6];
+        dinv<AX, T>(kA, kB, s, kx, d);
+        load6<T>(x, q, xv);
+        load6<T>(y, q, acc2);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] = acc2[j] + fma(-w, d[j], xv[j]);
+        store6<T>(y, q, o);
+    } else {
+        T rv[6], d[6], xv[6];
+        load6<T>(r, q, rv);
+#pragma unroll
+        for (int j = 0; j < 6; j++) rv[j] -= kx[j];
+        dinv<AX, T>(kA, kB, s, rv, d);
+        load6<T>(x, q, xv);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o[j] = fma(w, d[j], xv[j]);
+        store6<T>(y, q, o);
+    }
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(PENCIL_THREADS, 2) k_stencil_pencil(
+    const PencilTile* __restrict__ tiles, const PieceGeo* __restrict__ geo, const int32_t* __restrict__ gridmap,
+    const int4* __restrict__ cell, const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
+    T* __restrict__ y2, T s, const double* __restrict__ step, const int32_t* __restrict__ skip_row,
+    const int32_t* __restrict__ done) {
+    // shared (dynamic): +y and +z strips and k of every tile position and the halo row /
+    // column, indexed [ty + 1][tz + 1]; the tile cells' three - strips
+    extern __shared__ __align__(16) unsigned char pencil_smem[];
+    T(*py)[PTZ + 1][6] = reinterpret_cast<T(*)[PTZ + 1][6]>(pencil_smem);
+    T(*pz)[PTZ + 1][6] = py + (PTY + 1);
+    T(*kk)[PTZ + 1] = reinterpret_cast<T(*)[PTZ + 1]>(pz + (PTY + 1));
+    T(*ym)[PTZ][3][6] = reinterpret_cast<T(*)[PTZ][3][6]>(kk + (PTY + 1));
+    const PencilTile tl = tiles[blockIdx.x];
+    if (done && done[tl.piece]) return;
+    const PieceGeo g = geo[tl.piece];
+    const T w = step ? (T)step[tl.piece] : T(0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // this thread's (ty, tz) in [-1, PTY) x [-1, PTZ); role 0 tile, 1 +y halo, 2 +z halo
+    int ty, tz, role;
+    if (warp < PTY) {
+        ty = warp;
+        tz = lane;
+        role = 0;
+    } else if (warp == PTY) {
+        ty = -1;
+        tz = lane;
+        role = 1;
+    } else {
+        ty = lane < PTY ? lane : PTY;  // lanes past the column idle
+        tz = -1;
+        role = 2;
+    }
+    const int yy = tl.y0 + ty, zz = tl.z0 + tz;
+    const bool inside = ty < PTY && yy >= 0 && yy < g.ny && zz >= 0 && zz < g.nz;
+    T prevx[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    T prevk = T(0);
+    const int xend = min(tl.x0 + PSX, g.nx);
+    for (int xx = tl.x0 - 1; xx < xend; xx++) {
+        // the cell here, if free
+        int32_t C = -1;
+        if (inside && xx >= 0) C = gridmap[g.goff + ((int64_t)xx * g.ny + yy) * g.nz + zz];
+        int4 a = make_int4(-1, -1, -1, -1), b = make_int4(-1, -1, 0, 0);
+        T kc = T(0);
+        if (C >= 0) {
+            a = __ldg(cell + 2 * C);
+            b = __ldg(cell + 2 * C + 1);
+            kc = (T)__int_as_float(b.z);
+        }
+        T y1[6];
+        if (C >= 0) {
+            T xs[6][6];
+            gather_cell<T>(a, b, x, s, xs);
+            if (role == 0 && xx >= tl.x0) {
+                T t[6];
+                slot_out<0, T>(xs, kc, s, t);
+#pragma unroll
+                for (int j = 0; j < 6; j++) ym[ty][tz][0][j] = t[j];
+                slot_out<2, T>(xs, kc, s, t);
+#pragma unroll
+                for (int j = 0; j < 6; j++) ym[ty][tz][1][j] = t[j];
+                slot_out<4, T>(xs, kc, s, t);
+#pragma unroll
+                for (int j = 0; j < 6; j++) ym[ty][tz][2][j] = t[j];
+            }
+            if (role == 0) slot_out<1, T>(xs, kc, s, y1);
+            if (xx >= tl.x0 && role != 2) {
+                T t3[6];
+                slot_out<3, T>(xs, kc, s, t3);
+#pragma unroll
+                for (int j = 0; j < 6; j++) py[ty + 1][tz + 1][j] = t3[j];
+            }
+            if (xx >= tl.x0 && role != 1) {
+                T t5[6];
+                slot_out<5, T>(xs, kc, s, t5);
+#pragma unroll
+                for (int j = 0; j < 6; j++) pz[ty + 1][tz + 1][j] = t5[j];
+            }
+        } else if (xx >= tl.x0 && ty < PTY) {
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                if (role != 2) py[ty + 1][tz + 1][j] = T(0);
+                if (role != 1) pz[ty + 1][tz + 1][j] = T(0);
+            }
+        }
+        if (xx >= tl.x0 && ty < PTY) kk[ty + 1][tz + 1] = kc;
+        __syncthreads();
+        if (xx >= tl.x0 && role == 0 && C >= 0) {
+            int32_t q[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+            int nbr = b.w;  // bit a: the +a neighbour is free
+            // - faces: Kx = Y_L[2a+1] + Y_C[2a]
+            if (q[0] >= 0 && !(skip_row && skip_row[q[0]])) {
+                T kx[6];
+#pragma unroll
+                for (int j = 0; j < 6; j++) kx[j] = prevx[j] + ym[ty][tz][0][j];
+                pencil_finish<0, T, MODE>(q[0], kx, prevk, kc, s, w, x, r, y, y2);
+            }
+            if (q[2] >= 0 && !(skip_row && skip_row[q[2]])) {
+                T kx[6];
+#pragma unroll
+                for (int j = 0; j < 6; j++) kx[j] = py[ty][tz + 1][j] + ym[ty][tz][1][j];
+                pencil_finish<1, T, MODE>(q[2], kx, kk[ty][tz + 1], kc, s, w, x, r, y, y2);
+            }
+            if (q[4] >= 0 && !(skip_row && skip_row[q[4]])) {
+                T kx[6];
+#pragma unroll
+                for (int j = 0; j < 6; j++) kx[j] = pz[ty + 1][tz][j] + ym[ty][tz][2][j];
+                pencil_finish<2, T, MODE>(q[4], kx, kk[ty + 1][tz], kc, s, w, x, r, y, y2);
+            }
+            // + faces whose greater cell is not free: Kx = Y_C[2a+1]
+            if (!(nbr & 1) && q[1] >= 0 && !(skip_row && skip_row[q[1]]))
+                pencil_finish<0, T, MODE>(q[1], y1, kc, T(0), s, w, x, r, y, y2);
+            if (!(nbr & 2) && q[3] >= 0 && !(skip_row && skip_row[q[3]])) {
+                T t[6];
+#pragma unroll
+                for (int j = 0; j < 6; j++) t[j] = py[ty + 1][tz + 1][j];
+                pencil_finish<1, T, MODE>(q[3], t, kc, T(0), s, w, x, r, y, y2);
+            }
+            if (!(nbr & 4) && q[5] >= 0 && !(skip_row && skip_row[q[5]])) {
+                T t[6];
+#pragma unroll
+                for (int j = 0; j < 6; j++) t[j] = pz[ty + 1][tz + 1][j];
+                pencil_finish<2, T, MODE>(q[5], t, kc, T(0), s, w, x, r, y, y2);
+            }
+        }
+        if (role == 0) {
+#pragma unroll
+            for (int j = 0; j < 6; j++) prevx[j] = C >= 0 ? y1[j] : T(0);
+            prevk = kc;
+        }
+        __syncthreads();
+    }
 }
 
 // x = w D^-1 r with D^-1 matrix-free (pre-smoothing, bodies.rs:386)
@@ -599,8 +875,23 @@ static void launch_stencil(Context& ctx, const Batch& b, const T* x, const T* r,
     const Level& L = b.levels[0];
     int64_t n = g.axis_off[3];
     ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_STENCIL64 : SC_FAM_STENCIL32, stencil_bytes<T>(b, passes));
-    k_stencil<T, MODE><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.perm.get(), g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(), x, r, y,
-                                                                  y2, (T)g.s, L.piece.get(), step, skip_row, done);
+    if (g.pencil) {
+        // one piece per block: the step and done flag are the block's piece's
+        size_t smem = sizeof(T) * ((size_t)2 * (PTY + 1) * (PTZ + 1) * 6 + (size_t)(PTY + 1) * (PTZ + 1) +
+                                   (size_t)PTY * PTZ * 18);
+        static bool attr_set[2][8] = {};
+        if (!attr_set[sizeof(T) == 8][MODE]) {
+            SC_CK(cudaFuncSetAttribute(k_stencil_pencil<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+            attr_set[sizeof(T) == 8][MODE] = true;
+        }
+        k_stencil_pencil<T, MODE><<<(unsigned)g.ntiles, PENCIL_THREADS, smem, ctx.stream>>>(
+            reinterpret_cast<const PencilTile*>(g.tiles.get()), reinterpret_cast<const PieceGeo*>(g.geo.get()),
+            g.gridmap.get(), g.cell.get(), x, r, y, y2, (T)g.s, step, skip_row, done);
+        SC_LAUNCH_CK();
+        return;
+    }
+    k_stencil<T, MODE><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.slots.get(), g.cell.get(), x, r, y, y2, (T)g.s, L.piece.get(), step, skip_row, done);
     SC_LAUNCH_CK();
 }
 
@@ -638,6 +929,10 @@ void level0_down(Context& ctx, const Batch& b, const T* r, T* x, T* left, T* t, 
                                                                    L.step.get(), skip, done);
         SC_LAUNCH_CK();
     }
+    for (int sweep = 1; sweep < b.sweeps; sweep++) {  // further pre-smoothing sweeps
+        level0_smooth<T>(ctx, b, r, x, t, done);
+        SC_CK(cudaMemcpyAsync(x, t, 6 * L.n * sizeof(T), cudaMemcpyDeviceToDevice, ctx.stream));
+    }
     launch_stencil<T, ST_RES_JAC>(ctx, b, x, r, left, t, nullptr, skip, done, 4);
     launch_stencil<T, ST_RES_W>(ctx, b, t, left, u, nullptr, L.step.get(), skip, done, 3);
     {
@@ -665,8 +960,21 @@ void level0_up(Context& ctx, const Batch& b, const T* r, T* x, T* e, const T* zc
         SC_LAUNCH_CK();
     }
     launch_stencil<T, ST_PROLONG>(ctx, b, e, nullptr, x, nullptr, L.step.get(), skip, done, 4);
+    for (int sweep = 1; sweep < b.sweeps; sweep++) {  // further post-smoothing sweeps
+        launch_stencil<T, ST_SMOOTH>(ctx, b, x, r, e, nullptr, L.step.get(), skip, done, 3);
+        SC_CK(cudaMemcpyAsync(x, e, 6 * L.n * sizeof(T), cudaMemcpyDeviceToDevice, ctx.stream));
+    }
     launch_stencil<T, ST_SMOOTH>(ctx, b, x, r, z, nullptr, L.step.get(), skip, done, 3);
 }
+
+// z = x + w D^-1 (r - K x): one more block-Jacobi sweep
+template <class T>
+void level0_smooth(Context& ctx, const Batch& b, const T* r, const T* x, T* z, const int32_t* done) {
+    const Level& L = b.levels[0];
+    launch_stencil<T, ST_SMOOTH>(ctx, b, x, r, z, nullptr, L.step.get(), L.top_of_part.get(), done, 3);
+}
+template void level0_smooth<double>(Context&, const Batch&, const double*, const double*, double*, const int32_t*);
+template void level0_smooth<float>(Context&, const Batch&, const float*, const float*, float*, const int32_t*);
 
 template void level0_down<double>(Context&, const Batch&, const double*, double*, double*, double*, double*, double*,
                                   const int32_t*);
@@ -685,7 +993,8 @@ void grid_cell_energy(Context& ctx, const Batch& b, const double* x, double* ene
 
 // Builds level 0 of a batch of voxel pieces. The grids' state/k are uploaded (or
 // copied device to device) into one concatenated array.
-void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks) {
+void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks, int32_t tile) {
+    const int64_t TILE = tile > 0 ? tile : STENCIL_TILE;
     cudaStream_t st = ctx.stream;
     MemStats* ms = &ctx.mem;
     int np = (int)grids.size();
@@ -811,13 +1120,50 @@ void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool
         b.part_node.get(), g.axis.get(), L.site.get(), L.centre.get(), g.cella.get(), g.cellb.get(), b.mass.get(),
         b.loads.get());
     SC_LAUNCH_CK();
+    // caller loads instead of mass * gravity (node order) where given
+    for (int p = 0; p < np; p++) {
+        if (!grids[p].loads) continue;
+        DBuf<double> nl;
+        nl.alloc(6 * std::max<int64_t>(b.node_count[p], 1), st, ms);
+        SC_CK(cudaMemcpyAsync(nl.get(), grids[p].loads, 6 * b.node_count[p] * sizeof(double),
+                              grids[p].on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+        int64_t k0 = L.pstart[p], cnt = L.pstart[p + 1] - k0;
+        if (cnt > 0) {
+            k_node_loads<<<grid_for(cnt, 256), 256, 0, st>>>(cnt, b.part_node.get() + k0, nl.get(),
+                                                             b.loads.get() + 6 * k0);
+            SC_LAUNCH_CK();
+        }
+    }
     // cell table
     g.cell_flat.alloc(std::max<int64_t>(nfree, 1), st, ms);
     k_cell_flat<<<grid_for(ncell, 256), 256, 0, st>>>(ncell, freef.get(), cell_index.get(), g.cell_flat.get());
     SC_LAUNCH_CK();
     g.cell.alloc(2 * std::max<int64_t>(nfree, 1), st, ms);
-    k_cell_table<<<grid_for(nfree, 256), 256, 0, st>>>(nfree, cell_node6.get(), node_part.get(), g.cell_flat.get(),
-                                                        gk.get(), g.cell.get());
+    k_cell_table<<<grid_for(nfree, 256), 256, 0, st>>>(np, goff_d.get(), dims_d.get(), gst.get(), nfree,
+                                                        cell_node6.get(), node_part.get(), g.cell_flat.get(), gk.get(),
+                                                        g.cell.get());
+    SC_LAUNCH_CK();
+    // the pencil stencil's grid map and tiles
+    g.gridmap.alloc(ncell, st, ms);
+    k_gridmap<<<grid_for(ncell, 256), 256, 0, st>>>(ncell, freef.get(), cell_index.get(), g.gridmap.get());
+    {
+        std::vector<PencilTile> tiles;
+        std::vector<PieceGeo> geo(np);
+        for (int p = 0; p < np; p++) {
+            const Dims& d = dims[p];
+            geo[p] = PieceGeo{d.nx, d.ny, d.nz, 0, goff[p]};
+            for (int x0 = 0; x0 < d.nx; x0 += PSX)
+                for (int y0 = 0; y0 < d.ny; y0 += PTY)
+                    for (int z0 = 0; z0 < d.nz; z0 += PTZ) tiles.push_back(PencilTile{p, x0, y0, z0});
+        }
+        g.ntiles = (int64_t)tiles.size();
+        g.tiles.alloc(tiles.size() * sizeof(PencilTile), st, ms);
+        SC_CK(cudaMemcpyAsync(g.tiles.get(), tiles.data(), tiles.size() * sizeof(PencilTile), cudaMemcpyHostToDevice, st));
+        g.geo.alloc(geo.size() * sizeof(PieceGeo), st, ms);
+        SC_CK(cudaMemcpyAsync(g.geo.get(), geo.data(), geo.size() * sizeof(PieceGeo), cudaMemcpyHostToDevice, st));
+        SC_CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
+    }
+    g.pencil = tile == 0;
     SC_LAUNCH_CK();
     // parts in order, grouped by axis only within tiles of STENCIL_TILE parts: the
     // stencil sweeps the piece once in part order (x neighbours stay in L2) while a
@@ -831,10 +1177,10 @@ void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool
         keys_out.alloc(n, st, ms);
         k_iota<<<grid_for(n, 256), 256, 0, st>>>(n, ids.get());
         SC_LAUNCH_CK();
-        k_tile_axis_keys<<<grid_for(n, 256), 256, 0, st>>>(n, g.axis.get(), keys.get());
+        k_tile_axis_keys<<<grid_for(n, 256), 256, 0, st>>>(n, TILE, g.axis.get(), keys.get());
         SC_LAUNCH_CK();
         int end_bit = 2;
-        while (end_bit < 32 && ((uint64_t)1 << (end_bit - 2)) * STENCIL_TILE <= (uint64_t)n) end_bit++;
+        while (end_bit < 32 && ((uint64_t)1 << (end_bit - 2)) * (uint64_t)TILE <= (uint64_t)n) end_bit++;
         cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys_out.get(), ids.get(), ids_out.get(), n, 0,
                                         end_bit, st);
         cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, keys.get(), keys_out.get(), ids.get(),
@@ -842,6 +1188,10 @@ void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool
         g.perm = std::move(ids_out);
         g.axis_off[0] = 0;
         g.axis_off[1] = g.axis_off[2] = g.axis_off[3] = n;
+        g.slots.alloc(n, st, ms);
+        k_slots<<<grid_for(n, 256), 256, 0, st>>>(n, g.perm.get(), g.cella.get(), g.cellb.get(), g.axis.get(),
+                                                   g.slots.get());
+        SC_LAUNCH_CK();
     }
     // assembled blocks for the setup (the solve itself applies level 0 matrix-free)
     if (keep_blocks) {

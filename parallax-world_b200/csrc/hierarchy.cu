@@ -210,16 +210,23 @@ __global__ void k_count_KP(int64_t n, const int64_t* __restrict__ rowptr, const 
         }
     cnt[k] = c;
 }
+// candidates of K P row k: (k, col of P_qf) for each block K_kq and each block P_qf,
+// contribution (entry of K_kq << 32 | entry of P_qf)
 __global__ void k_fill_KP(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
-                          const int32_t* __restrict__ up, const int64_t* __restrict__ off, uint64_t* __restrict__ keys) {
+                          const int32_t* __restrict__ up, const int64_t* __restrict__ off, uint64_t* __restrict__ keys,
+                          uint64_t* __restrict__ vals) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (up[k] < 0) return;
     int64_t o = off[k];
     for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
         int32_t q = col[e];
-        for (int64_t f = prow[q]; f < prow[q + 1]; f++) keys[o++] = ((uint64_t)k << 32) | (uint32_t)pcol[f];
+        for (int64_t f = prow[q]; f < prow[q + 1]; f++) {
+            keys[o] = ((uint64_t)k << 32) | (uint32_t)pcol[f];
+            vals[o] = ((uint64_t)e << 32) | (uint64_t)f;
+            o++;
+        }
     }
 }
 // per P entry (k, c): the columns d >= c of KP row k
@@ -232,16 +239,22 @@ __global__ void k_count_C(int64_t n, const int64_t* __restrict__ prow, const int
         cnt[e] = kprow[k + 1] - lb;
     }
 }
+// candidates of the upper P'KP: (c, d) for each entry (k, c) of P and each block
+// (k, d >= c) of K P, contribution (entry of P << 32 | entry of KP)
 __global__ void k_fill_C(int64_t n, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
                          const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol,
-                         const int64_t* __restrict__ off, uint64_t* __restrict__ keys) {
+                         const int64_t* __restrict__ off, uint64_t* __restrict__ keys, uint64_t* __restrict__ vals) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     for (int64_t e = prow[k]; e < prow[k + 1]; e++) {
         int32_t c = pcol[e];
         int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], c);
         int64_t o = off[e];
-        for (int64_t f = lb; f < kprow[k + 1]; f++) keys[o++] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)kpcol[f];
+        for (int64_t f = lb; f < kprow[k + 1]; f++) {
+            keys[o] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)kpcol[f];
+            vals[o] = ((uint64_t)e << 32) | (uint64_t)f;
+            o++;
+        }
     }
 }
 __global__ void k_unpack_pattern(int64_t m, const uint64_t* __restrict__ keys, int32_t* __restrict__ col,
@@ -345,47 +358,45 @@ __global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restr
     }
 }
 
-__global__ void __launch_bounds__(256) k_num_KP(int64_t n, const int64_t* __restrict__ rowptr,
-                                                const int32_t* __restrict__ col, const double* __restrict__ val,
-                                                const int32_t* __restrict__ up, const int64_t* __restrict__ prow,
-                                                const int32_t* __restrict__ pcol, const double* __restrict__ pval,
-                                                const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol,
-                                                double* __restrict__ kpval) {
-    int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (k >= n) return;
-    int lane = threadIdx.x & 31;
-    if (up[k] < 0) return;
-    int64_t q0 = kprow[k], q1 = kprow[k + 1];
-    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
-        int32_t o = col[e];
-        for (int64_t f = prow[o]; f < prow[o + 1]; f++) {
-            int64_t pos = lower_bound_i32(kpcol, q0, q1, pcol[f]);
-            warp_block_mac<false, false>(lane, val + 36 * e, pval + 36 * f, nullptr, kpval + 36 * pos);
-            __syncwarp();
-        }
+
+
+// Every output block of a product as the ordered sum of its contributions: after the
+// symbolic sort, output block q's contributions are vals[seg[q] .. seg[q+1]), each the
+// pair (a << 32 | b) of a left block and a right block, in the order the candidates were
+// generated (a stable sort), so the sum is deterministic. 36 threads per output block,
+// one per entry; the left operand transposed when TA.
+constexpr int SUM_GROUPS = 8;  // output blocks per thread block (8 * 36 threads)
+template <bool TA>
+__global__ void __launch_bounds__(36 * SUM_GROUPS) k_sum_products(int64_t nout, const int64_t* __restrict__ seg,
+                                                                  const uint64_t* __restrict__ vals,
+                                                                  const double* __restrict__ A,
+                                                                  const double* __restrict__ B,
+                                                                  double* __restrict__ out) {
+    int g = threadIdx.x / 36, e = threadIdx.x % 36;
+    int64_t q = (int64_t)blockIdx.x * SUM_GROUPS + g;
+    if (q >= nout) return;
+    int r = e / 6, c = e % 6;
+    double acc = 0.0;
+    for (int64_t i = seg[q]; i < seg[q + 1]; i++) {
+        uint64_t v = vals[i];
+        const double* a = A + 36 * (int64_t)(v >> 32);
+        const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; j++) s = fma(TA ? a[j * 6 + r] : a[r * 6 + j], bb[j * 6 + c], s);
+        acc += s;
     }
+    out[36 * q + e] = acc;
 }
 
-__global__ void __launch_bounds__(256) k_num_C(int64_t nc, const int64_t* __restrict__ tptr,
-                                               const int64_t* __restrict__ tent, const int32_t* __restrict__ trow,
-                                               const double* __restrict__ pval, const int64_t* __restrict__ kprow,
-                                               const int32_t* __restrict__ kpcol, const double* __restrict__ kpval,
-                                               const int64_t* __restrict__ crow, const int32_t* __restrict__ ccol,
-                                               double* __restrict__ cval) {
-    int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (c >= nc) return;
-    int lane = threadIdx.x & 31;
-    int64_t c0 = crow[c], c1 = crow[c + 1];
-    for (int64_t t = tptr[c]; t < tptr[c + 1]; t++) {
-        int64_t e = tent[t];
-        int32_t k = trow[t];
-        int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], (int32_t)c);
-        for (int64_t f = lb; f < kprow[k + 1]; f++) {
-            int64_t pos = lower_bound_i32(ccol, c0, c1, kpcol[f]);
-            warp_block_mac<true, false>(lane, pval + 36 * e, kpval + 36 * f, nullptr, cval + 36 * pos);
-            __syncwarp();
-        }
-    }
+// P' as its own block rows: block t = transpose of P's block tent[t]
+__global__ void k_transpose_gather(int64_t m, const int64_t* __restrict__ tent, const double* __restrict__ pval,
+                                   double* __restrict__ ptval) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= 36 * m) return;
+    int64_t t = i / 36;
+    int e = (int)(i % 36), r = e / 6, c = e % 6;
+    ptval[i] = pval[36 * tent[t] + c * 6 + r];
 }
 
 // full symmetric storage: entry i of the full pattern copies upper entry src[i] & mask,
@@ -573,6 +584,71 @@ void keys_to_csr(Context& ctx, DBuf<uint64_t>& keys, int64_t nkeys, int64_t nrow
     k_offsets_from_sorted<<<grid_for(nnz + 1, 256), 256, 0, st>>>(nnz, rows.get(), nrows, rowptr.get());
     SC_LAUNCH_CK();
     (void)ncols;
+}
+
+__global__ void k_seg_flags(int64_t m, const uint64_t* __restrict__ keys, int64_t* __restrict__ flag) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+__global__ void k_seg_starts(int64_t m, const uint64_t* __restrict__ keys, const int64_t* __restrict__ flag,
+                             const int64_t* __restrict__ idx, int64_t* __restrict__ seg, int32_t* __restrict__ col,
+                             int32_t* __restrict__ row) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    if (flag[i]) {
+        int64_t u = idx[i];
+        seg[u] = i;
+        col[u] = (int32_t)(keys[i] & 0xffffffffu);
+        row[u] = (int32_t)(keys[i] >> 32);
+    }
+}
+
+// The same, keeping each candidate's contribution (a << 32 | b): the pattern in CSR,
+// and for every stored block the range seg[q] .. seg[q+1] of its contributions in
+// `vals` (sorted by output block, candidate order kept within one).
+void keys_to_csr_with(Context& ctx, DBuf<uint64_t>& keys, DBuf<uint64_t>& vin, int64_t nkeys, int64_t nrows,
+                      DBuf<int64_t>& rowptr, DBuf<int32_t>& col, int64_t& nnz, DBuf<int64_t>& seg,
+                      DBuf<uint64_t>& vals) {
+    cudaStream_t st = ctx.stream;
+    MemStats* ms = &ctx.mem;
+    DBuf<uint64_t> sorted;
+    sorted.alloc(std::max<int64_t>(nkeys, 1), st, ms);
+    vals.alloc(std::max<int64_t>(nkeys, 1), st, ms);
+    int end_bit = 32 + bits_for(nrows);
+    size_t tb = 0;
+    if (nkeys > 0) {
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), sorted.get(), vin.get(), vals.get(), nkeys, 0, end_bit,
+                                        st);
+        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, keys.get(), sorted.get(), vin.get(), vals.get(), nkeys,
+                                        0, end_bit, st);
+    }
+    keys.release();
+    vin.release();
+    DBuf<int64_t> flag, idx;
+    flag.alloc(nkeys + 1, st, ms);
+    idx.alloc(nkeys + 1, st, ms);
+    SC_CK(cudaMemsetAsync(flag.get() + nkeys, 0, sizeof(int64_t), st));
+    if (nkeys > 0) {
+        k_seg_flags<<<grid_for(nkeys, 256), 256, 0, st>>>(nkeys, sorted.get(), flag.get());
+        SC_LAUNCH_CK();
+    }
+    exclusive_scan(ctx, flag.get(), idx.get(), nkeys + 1);
+    nnz = d2h_i64(ctx, idx.get() + nkeys);
+    seg.alloc(nnz + 1, st, ms);
+    col.alloc(std::max<int64_t>(nnz, 1), st, ms);
+    DBuf<int32_t> rows;
+    rows.alloc(std::max<int64_t>(nnz, 1), st, ms);
+    if (nkeys > 0) {
+        k_seg_starts<<<grid_for(nkeys, 256), 256, 0, st>>>(nkeys, sorted.get(), flag.get(), idx.get(), seg.get(),
+                                                          col.get(), rows.get());
+        SC_LAUNCH_CK();
+    }
+    SC_CK(cudaMemcpyAsync(seg.get() + nnz, &nkeys, sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    rowptr.alloc(nrows + 1, st, ms);
+    k_offsets_from_sorted<<<grid_for(nnz + 1, 256), 256, 0, st>>>(nnz, rows.get(), nrows, rowptr.get());
+    SC_LAUNCH_CK();
+    SC_CK(cudaStreamSynchronize(st));  // nkeys (a host value) was copied asynchronously
 }
 
 }  // namespace
@@ -811,6 +887,13 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         // trow[t] = row of entry tent[t]
         gather_i32(ctx, F.pnnz, F.tent.get(), prow_of.get(), F.trow.get());
     }
+    // the restriction's blocks, contiguous by coarse row (a matrix-free level 0 needs none)
+    if (!keep_mf) {
+        F.ptval.alloc(36 * std::max<int64_t>(F.pnnz, 1), st, ms);
+        k_transpose_gather<<<grid_for(36 * F.pnnz, 256), 256, 0, st>>>(F.pnnz, F.tent.get(), F.pval.get(),
+                                                                       F.ptval.get());
+        SC_LAUNCH_CK();
+    }
     // --- K P
     DBuf<int64_t> kprow;
     DBuf<int32_t> kpcol;
@@ -819,24 +902,27 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     SC_LAUNCH_CK();
     exclusive_scan(ctx, cnt.get(), off.get(), n + 1);
     tot = d2h_i64(ctx, off.get() + n);
-    {
-        DBuf<uint64_t> keys;
-        keys.alloc(std::max<int64_t>(tot, 1), st, ms);
-        k_fill_KP<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.prow.get(), F.pcol.get(),
-                                                    F.up.get(), off.get(), keys.get());
-        SC_LAUNCH_CK();
-        keys_to_csr(ctx, keys, tot, n, nc, kprow, kpcol, kpnnz);
-    }
     DBuf<double> kpval;
-    kpval.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
-    kpval.zero();
-    k_num_KP<<<grid_for(n * 32, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.val.get(), F.up.get(),
-                                                    F.prow.get(), F.pcol.get(), F.pval.get(), kprow.get(), kpcol.get(),
-                                                    kpval.get());
-    SC_LAUNCH_CK();
+    {
+        DBuf<uint64_t> keys, vin, vals;
+        DBuf<int64_t> seg;
+        keys.alloc(std::max<int64_t>(tot, 1), st, ms);
+        vin.alloc(std::max<int64_t>(tot, 1), st, ms);
+        k_fill_KP<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.prow.get(), F.pcol.get(),
+                                                    F.up.get(), off.get(), keys.get(), vin.get());
+        SC_LAUNCH_CK();
+        keys_to_csr_with(ctx, keys, vin, tot, n, kprow, kpcol, kpnnz, seg, vals);
+        kpval.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
+        if (kpnnz > 0) {
+            k_sum_products<false><<<(unsigned)((kpnnz + SUM_GROUPS - 1) / SUM_GROUPS), 36 * SUM_GROUPS, 0, st>>>(
+                kpnnz, seg.get(), vals.get(), F.val.get(), F.pval.get(), kpval.get());
+            SC_LAUNCH_CK();
+        }
+    }
     // --- P' K P, upper triangle (d >= c)
     DBuf<int64_t> urow;
     DBuf<int32_t> ucol;
+    DBuf<double> uval;
     int64_t unnz = 0;
     {
         DBuf<int64_t> ecnt, eoff;
@@ -847,20 +933,21 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         SC_LAUNCH_CK();
         exclusive_scan(ctx, ecnt.get(), eoff.get(), F.pnnz + 1);
         tot = d2h_i64(ctx, eoff.get() + F.pnnz);
-        DBuf<uint64_t> keys;
+        DBuf<uint64_t> keys, vin, vals;
+        DBuf<int64_t> seg;
         keys.alloc(std::max<int64_t>(tot, 1), st, ms);
+        vin.alloc(std::max<int64_t>(tot, 1), st, ms);
         k_fill_C<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), F.pcol.get(), kprow.get(), kpcol.get(), eoff.get(),
-                                                   keys.get());
+                                                   keys.get(), vin.get());
         SC_LAUNCH_CK();
-        keys_to_csr(ctx, keys, tot, nc, nc, urow, ucol, unnz);
+        keys_to_csr_with(ctx, keys, vin, tot, nc, urow, ucol, unnz, seg, vals);
+        uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
+        if (unnz > 0) {
+            k_sum_products<true><<<(unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS), 36 * SUM_GROUPS, 0, st>>>(
+                unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get());
+            SC_LAUNCH_CK();
+        }
     }
-    DBuf<double> uval;
-    uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
-    uval.zero();
-    k_num_C<<<grid_for(nc * 32, 256), 256, 0, st>>>(nc, F.tptr.get(), F.tent.get(), F.trow.get(), F.pval.get(),
-                                                    kprow.get(), kpcol.get(), kpval.get(), urow.get(), ucol.get(),
-                                                    uval.get());
-    SC_LAUNCH_CK();
     kpval.release();
     kprow.release();
     kpcol.release();

@@ -25,6 +25,12 @@ struct Grid0 {
     double s = 0.125;           // spacing (statics/src/lattice.rs:16, 34-36)
     DBuf<int4> cell;            // 2 int4 per free cell: part ids of slots 0..5 (-1 held), k bits, 0
     DBuf<int32_t> perm;         // parts in order, grouped by axis inside tiles of 1024 parts
+    DBuf<int4> slots;           // per perm slot: part, lesser cell, greater cell, axis
+    bool pencil = true;         // the plane-pencil stencil (tile 0) or the per-slot one
+    DBuf<int32_t> gridmap;      // per grid cell: its free-cell index or -1
+    DBuf<uint8_t> tiles;        // pencil tiles (piece, x0, y0, z0)
+    DBuf<uint8_t> geo;          // per piece: dims and first flat cell
+    int64_t ntiles = 0;
     int64_t axis_off[4] = {0, 0, 0, 0};  // axis_off[3]: parts in perm
     DBuf<int32_t> cella, cellb; // per part: its lesser cell (node is that cell's + face) and greater cell; -1 if not free
     DBuf<int8_t> axis;          // per part
@@ -66,6 +72,8 @@ struct Level {
     DBuf<int64_t> tptr;              // P transposed: coarse row c's entries tent[tptr[c]..tptr[c+1])
     DBuf<int64_t> tent;              //   (index into pcol / pval), in fine-row order
     DBuf<int32_t> trow;              //   and the fine row of each
+    DBuf<double> ptval;              // P' blocks in that order (restriction as a block-sparse product)
+    DBuf<float> ptval32;
 
     // pieces solved directly at this level
     std::vector<int32_t> top_h;
@@ -101,6 +109,7 @@ struct Batch {
     DBuf<double> mass;               // per part (voxel pieces)
     double setup_ms = 0;
     int32_t base_level = 0;          // Lattice::level of level 0 (octree keys start one above)
+    int32_t sweeps = 1;              // block-Jacobi sweeps before and after each coarse correction
 };
 
 struct Context;
@@ -108,7 +117,7 @@ struct Context;
 // --- grid.cu ------------------------------------------------------------------------
 // Build level 0 (numbering, cells, centres, sites, loads, assembled blocks for setup)
 // for voxel pieces already on the device.
-void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks);
+void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks, int32_t tile);
 template <class T>
 void stencil_apply(Context& ctx, const Batch& b, const T* x, T* y, const int32_t* skip_row, const int32_t* done);
 template <class T>
@@ -119,6 +128,8 @@ template <class T>
 void level0_down(Context& ctx, const Batch& b, const T* r, T* x, T* left, T* t, T* u, T* rc, const int32_t* done);
 template <class T>
 void level0_up(Context& ctx, const Batch& b, const T* r, T* x, T* e, const T* zc, T* z, const int32_t* done);
+template <class T>
+void level0_smooth(Context& ctx, const Batch& b, const T* r, const T* x, T* z, const int32_t* done);
 
 // --- lattice.cu -----------------------------------------------------------------------
 void lattice_level0(Context& ctx, Batch& b, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,

@@ -46,7 +46,8 @@ class StaticsError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_int64), ("few", C.c_int64), ("precision", C.c_int32),
-                ("sweeps", C.c_int32), ("inner_tol", C.c_double), ("timeout_ms", C.c_int64)]
+                ("sweeps", C.c_int32), ("inner_tol", C.c_double), ("timeout_ms", C.c_int64), ("tile", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class SolveInfo(C.Structure):
@@ -67,7 +68,7 @@ class SolveInfo(C.Structure):
 class Grid(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("state", C.c_void_p), ("k", C.c_void_p),
                 ("g_over_e", C.c_double), ("rho", C.c_double), ("gravity", C.c_double * 3),
-                ("on_device", C.c_int32)]
+                ("on_device", C.c_int32), ("loads", C.c_void_p)]
 
 
 class LatticeC(C.Structure):
@@ -127,12 +128,13 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def options(tol=1e-6, max_iter=100000, few=64, precision=FP64, sweeps=1, inner_tol=1e-4, timeout_ms=0) -> Options:
+def options(tol=1e-6, max_iter=100000, few=64, precision=FP64, sweeps=1, inner_tol=1e-4, timeout_ms=0,
+            tile=0) -> Options:
     """The reference's constants by default (bodies.rs:430-432, 351)."""
     o = Options()
     lib().sc_default_options(C.byref(o))
     o.tol, o.max_iter, o.few, o.precision = tol, max_iter, few, precision
-    o.sweeps, o.inner_tol, o.timeout_ms = sweeps, inner_tol, timeout_ms
+    o.sweeps, o.inner_tol, o.timeout_ms, o.tile = sweeps, inner_tol, timeout_ms, tile
     return o
 
 
@@ -146,7 +148,8 @@ def generate_piece(nx: int, ny: int, nz: int, seed: int, k_dist: int = K_UNIFORM
     return state, k
 
 
-def make_grid(state: np.ndarray, k: np.ndarray, g_over_e=0.4, rho=512.0, gravity=(0.0, 0.0, -1.0)) -> Grid:
+def make_grid(state: np.ndarray, k: np.ndarray, g_over_e=0.4, rho=512.0, gravity=(0.0, 0.0, -1.0),
+              loads: np.ndarray | None = None) -> Grid:
     nx, ny, nz = state.shape
     g = Grid()
     g.nx, g.ny, g.nz = nx, ny, nz
@@ -154,7 +157,8 @@ def make_grid(state: np.ndarray, k: np.ndarray, g_over_e=0.4, rho=512.0, gravity
     g.g_over_e, g.rho = g_over_e, rho
     g.gravity[0], g.gravity[1], g.gravity[2] = gravity
     g.on_device = 0
-    g._keep = (state, k)
+    g.loads = _ptr(loads)
+    g._keep = (state, k, loads)
     return g
 
 
@@ -247,11 +251,14 @@ class Solver:
         return d
 
     # ---- voxel pieces -------------------------------------------------------------
-    def solve_grid(self, state, k, opt: Options | None = None, gravity=(0.0, 0.0, -1.0), rho=512.0):
-        """Motions of every node of a voxel piece (n_nodes x 6, reference node order)."""
+    def solve_grid(self, state, k, opt: Options | None = None, gravity=(0.0, 0.0, -1.0), rho=512.0, loads=None):
+        """Motions of every node of a voxel piece (n_nodes x 6, reference node order);
+        `loads` (n_nodes x 6) replaces mass * gravity when given."""
         state = np.ascontiguousarray(state, np.uint8)
         k = np.ascontiguousarray(k, np.float32)
-        g = make_grid(state, k, rho=rho, gravity=gravity)
+        if loads is not None:
+            loads = np.ascontiguousarray(loads, np.float64)
+        g = make_grid(state, k, rho=rho, gravity=gravity, loads=loads)
         n_nodes, _ = grid_count(state)
         out = np.zeros((max(n_nodes, 1), 6))
         info = SolveInfo()
