@@ -4,9 +4,11 @@
 Workload (one step): one full solve -- hierarchy setup plus preconditioned conjugate
 gradients to 1e-8 relative residual -- of a seeded synthetic 128^3 piece (value noise of
 period 8, threshold 0.5, bottom layer held, k uniform in [0.5, 2], load -1 along z per
-unit mass). `value` is solves/s with the piece already in HBM (mixed precision: FP32
-operators inside FP64 iterative refinement); `fp64` is the same for the plain FP64
-solve; `e2e` is the C-ABI call with host buffers (copies inside the timed region).
+unit mass). `value` is solves/s with the piece already in HBM (mixed precision: FP64
+conjugate gradients preconditioned by the V-cycle in FP32); `fp64` is the same for the
+plain FP64 solve and `mixed_fp32_krylov` for the all-FP32 Krylov recurrence with FP64
+residual replacement; `e2e` is the C-ABI call with host buffers (copies inside the
+timed region).
 Each rank solves its own piece (seed + rank): weak scaling, no collective on the data
 path. The working set (vectors ~0.1-0.2 GB each, coarse operators GBs) exceeds the
 126 MB L2, so no flush is needed between steps.
@@ -202,13 +204,14 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(solver.stream())
     hbm, hbm_kind = peaks()
 
-    def timed(precision, steps, warmup, mask):
+    def timed(precision, steps, warmup):
+        """K solves on the solver's stream, CUDA events around them, profiling off (the
+        CG iterations run as CUDA graphs)."""
         opt = sc.options(tol=TOL, precision=precision)
         for _ in range(warmup):
             solver.solve_grid_device(grid, opt, out_d.data_ptr(), out_d.numel())
         barrier(world)
         torch.cuda.synchronize()
-        solver.profile(mask)
         l0 = sc.launches()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -217,20 +220,32 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier(world)
         ms = max_over_ranks(e0.elapsed_time(e1), world)
+        return ms, infos, sc.launches() - l0
+
+    def profiled(precision, mask):
+        """One more solve of the same workload with per-launch CUDA events on the
+        solver's stream for the kernel families in `mask` (kernels launched one by one)."""
+        opt = sc.options(tol=TOL, precision=precision)
+        barrier(world)
+        torch.cuda.synchronize()
+        solver.profile(mask)
+        solver.solve_grid_device(grid, opt, out_d.data_ptr(), out_d.numel())
+        torch.cuda.synchronize()
         prof = solver.profile_read()
         solver.profile(0)
-        return ms, infos, sc.launches() - l0, prof
+        return prof
 
-    # which kernel family dominates a mixed solve (all families timed once)
-    _, _, _, prof_all = timed(sc.MIXED, 1, max(1, args.warmup // 2), (1 << 9) - 1)
-    dominant = max(prof_all, key=lambda f: prof_all[f]["ms"])
-    fam = sc.FAM_NAMES.index(dominant)
-    stencil = "stencil32"
-    mask = (1 << fam) | (1 << sc.FAM_NAMES.index(stencil))
     clocks = Clocks(local)
-    ms_mixed, infos_m, launches, prof = timed(sc.MIXED, args.steps, args.warmup, mask)
+    ms_mixed, infos_m, launches = timed(sc.MIXED, args.steps, args.warmup)
     clk = clocks.stop()
-    ms_64, infos_64, _, prof64 = timed(sc.FP64, args.steps, max(1, args.warmup // 2), 1 << sc.FAM_STENCIL64)
+    ms_64, infos_64, _ = timed(sc.FP64, args.steps, max(3, args.warmup // 2))
+    ms_k, infos_k, _ = timed(sc.MIXED_FP32_KRYLOV, args.steps, max(3, args.warmup // 2))
+    # which kernel family dominates a mixed solve, and each family's time per launch
+    all_fams = (1 << len(sc.FAM_NAMES)) - 1
+    prof = profiled(sc.MIXED, all_fams)
+    prof64 = profiled(sc.FP64, all_fams)
+    dominant = max(prof, key=lambda f: prof[f]["ms"])
+    stencil = "stencil32"
 
     # e2e through the C ABI with host buffers
     barrier(world)
@@ -265,7 +280,7 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": ms_mixed / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 operators in f64 refinement", "data": "synthetic", "config": workload(args.seed),
+        "dtype": "f64 CG, f32 V-cycle", "data": "synthetic", "config": workload(args.seed),
         "dof": dof, "iterations": it_m, "refinements": infos_m[-1]["refinements"],
         "levels": infos_m[-1]["parts"], "residual": infos_m[-1]["residual"],
         "setup_ms": statistics.mean(i["setup_ms"] for i in infos_m), "solve_ms": solve_ms_m,
@@ -274,9 +289,16 @@ def run_ours(args):
                  "iterations": it_64, "solve_ms": solve_ms_64,
                  "dof_iters_per_s": world * dof * it_64 / (solve_ms_64 / 1000.0),
                  "residual": infos_64[-1]["residual"], "stencil_roofline": roof(prof64, "stencil64")},
+        "mixed_fp32_krylov": {"value": world * K / (ms_k / 1000.0), "unit": "solves/s", "ms_per_step": ms_k / K,
+                              "iterations": infos_k[-1]["iterations"],
+                              "refinements": infos_k[-1]["refinements"],
+                              "solve_ms": statistics.mean(i["solve_ms"] for i in infos_k),
+                              "residual": infos_k[-1]["residual"]},
         "roofline": roof(prof, dominant),
         "stencil_roofline": roof(prof, stencil),
-        "kernel_share": {f: round(prof_all[f]["ms"], 3) for f in prof_all if prof_all[f]["launches"]},
+        "kernel_ms": {f: round(prof[f]["ms"], 3) for f in prof if prof[f]["launches"]},
+        "roofline_method": "per-launch CUDA events on the solver's stream during one profiled solve of the same "
+                           "workload after the timed region (the timed region runs CUDA graphs, no events)",
         "e2e": {"value": world * K / (ms_e2e / 1000.0), "unit": "solves/s",
                 "h2d_bytes_per_step": int(state.nbytes + k.nbytes), "d2h_bytes_per_step": int(8 * 6 * n_nodes)},
         "gpu_launches": launches,
@@ -298,15 +320,81 @@ def run_ours(args):
 
 def run_probe(args):
     """One kernel or one solve alone, for profiling: `stencil` applies the level-0
-    stencil to the bench's piece (FP64 then FP32, two launches each); `solve` runs one
-    FP64 and one mixed solve of it."""
+    stencil to the bench's piece (FP64 then FP32, two launches each); `solve` runs FP64,
+    mixed, FP64, mixed solves of it (SC_TIMING=1 prints the setup's phases)."""
     import numpy as np
 
     import statics_cuda as sc
+    if args.probe == "large":
+        # the large configuration: a 256^3 piece, lognormal k (mu 0, sigma 0.5) clipped to
+        # [0.1, 10]; mixed-precision forward solve plus the compliance adjoint, checked
+        # against the FP64 solve's gradient (the FP64 GPU solve is the oracle at this size,
+        # validated against the CPU oracle up to 128^3 by the parity tests)
+        import numpy as np
+        n = args.large_n
+        st, k = sc.generate_piece(n, n, n, args.seed, sc.K_LOGNORMAL)
+        nodes, parts = sc.grid_count(st)
+        solver = sc.Solver(0)
+        out = {"probe": "large", "grid": [n, n, n], "free_cells": int((st == sc.CELL_FREE).sum()),
+               "dof": 6 * parts, "tol": TOL}
+        res = {}
+        for name, prec, tol in (("mixed", sc.MIXED, TOL), ("fp64", sc.FP64, 1e-10)):
+            t = time.perf_counter()
+            C, grad, u, info = solver.compliance_grad(st, k, sc.options(tol=tol, precision=prec, max_iter=20000))
+            wall = time.perf_counter() - t
+            res[name] = grad
+            out[name] = {"tol": tol, "status": info["status"], "iterations": info["iterations"],
+                         "residual": info["residual"], "setup_ms": info["setup_ms"], "solve_ms": info["solve_ms"],
+                         "time_to_tol_ms": info["setup_ms"] + info["solve_ms"], "wall_s_with_copies": wall,
+                         "peak_hbm_bytes": info["peak_bytes"], "levels": info["parts"], "compliance": C}
+            print(json.dumps({name: out[name]}), flush=True)
+        g, g64 = res["mixed"].ravel(), res["fp64"].ravel()
+        free = st.ravel() == sc.CELL_FREE
+        err = np.abs(g[free] - g64[free])
+        out["grad_err"] = {"max_abs_over_max": float(err.max() / np.abs(g64[free]).max()),
+                           "l2_rel": float(np.linalg.norm(err) / np.linalg.norm(g64[free])),
+                           "max_rel_per_voxel": float((err / np.abs(g64[free])).max())}
+        print(json.dumps(out), flush=True)
+        solver.close()
+        return
+    if args.probe == "batch":
+        pieces = batch_pieces(sc, args.batch, 0)
+        solver = sc.Solver(0)
+        names = {sc.FP64: "fp64", sc.MIXED: "mixed", sc.MIXED_FP32_KRYLOV: "mixed_fp32_krylov"}
+        slow = None
+        for prec in (sc.MIXED, sc.MIXED, sc.MIXED_FP32_KRYLOV, sc.FP64):
+            opt = sc.options(tol=TOL, precision=prec, max_iter=20000)
+            t = time.perf_counter()
+            _, infos = solver.solve_grid_batch(pieces, opt)
+            dt = time.perf_counter() - t
+            groups = sorted({(i["setup_ms"], i["solve_ms"]) for i in infos})
+            print(json.dumps({"probe": "batch", "pieces": len(pieces), "precision": names[prec],
+                              "seconds": dt, "groups": len(groups),
+                              "setup_ms": sum(g[0] for g in groups), "solve_ms": sum(g[1] for g in groups),
+                              "iterations_max": max(i["iterations"] for i in infos),
+                              "iterations_mean": sum(i["iterations"] for i in infos) / len(infos),
+                              "bad": sum(1 for i in infos if i["status"] != 0)}), flush=True)
+            if slow is None:
+                slow = sorted(range(len(infos)), key=lambda i: -infos[i]["iterations"])[:4]
+        for i in slow:
+            st, k = pieces[i]
+            alone = {}
+            for prec in (sc.MIXED, sc.MIXED_FP32_KRYLOV, sc.FP64):
+                _, inf = solver.solve_grid(st, k, sc.options(tol=TOL, precision=prec, max_iter=20000))
+                alone[names[prec]] = {"status": inf["status"], "iterations": inf["iterations"],
+                                      "residual": inf["residual"]}
+            print(json.dumps({"piece": i, "shape": list(st.shape), "parts": inf["parts"][:inf["levels"]],
+                              "steps": inf["steps"][:inf["levels"]], "alone": alone}), flush=True)
+        t = time.perf_counter()
+        for st, k in pieces[:32]:
+            solver.solve_grid(st, k, sc.options(tol=TOL, precision=sc.FP64))
+        print(json.dumps({"probe": "fp64 single", "pieces": 32, "seconds": time.perf_counter() - t}), flush=True)
+        solver.close()
+        return
     state, k = sc.generate_piece(N, N, N, args.seed, sc.K_UNIFORM)
     if args.probe == "solve":
         solver = sc.Solver(0)
-        for prec in (sc.FP64, sc.MIXED):
+        for prec in (sc.FP64, sc.MIXED, sc.MIXED_FP32_KRYLOV, sc.FP64, sc.MIXED, sc.MIXED_FP32_KRYLOV):
             _, info = solver.solve_grid(state, k, sc.options(tol=TOL, precision=prec))
             print(json.dumps({"probe": "solve", "precision": prec, "iterations": info["iterations"],
                               "setup_ms": info["setup_ms"], "solve_ms": info["solve_ms"]}))
@@ -322,6 +410,17 @@ def run_probe(args):
     solver.close()
 
 
+def batch_pieces(sc, count, rank):
+    """`count` pieces with edges drawn from EDGES per axis, seeded per rank."""
+    import numpy as np
+    rng = np.random.default_rng(777 + rank)
+    pieces = []
+    for i in range(count):
+        nx, ny, nz = (int(v) for v in rng.choice(EDGES, 3))
+        pieces.append(sc.generate_piece(nx, ny, nz, 10_000 + count * rank + i, sc.K_UNIFORM))
+    return pieces
+
+
 def batch_section(solver, sc, rank, world, args):
     """Many pieces of uneven size: BATCH pieces whose edges are drawn from EDGES per axis
     (seeded per rank), solved by the autotuned mixed-precision batched solve; against the
@@ -330,11 +429,7 @@ def batch_section(solver, sc, rank, world, args):
     import torch
 
     from statics_cuda import autotune
-    rng = np.random.default_rng(777 + rank)
-    pieces = []
-    for i in range(args.batch):
-        nx, ny, nz = (int(v) for v in rng.choice(EDGES, 3))
-        pieces.append(sc.generate_piece(nx, ny, nz, 10_000 + args.batch * rank + i, sc.K_UNIFORM))
+    pieces = batch_pieces(sc, args.batch, rank)
     dof = sum(6 * sc.grid_count(p[0])[1] for p in pieces)
     t = time.perf_counter()
     settings = autotune.choose(solver, pieces, sc.MIXED, TOL)
@@ -363,13 +458,15 @@ def batch_section(solver, sc, rank, world, args):
     batched = world * len(pieces) / (ms_b / 1000.0)
     single = world * len(sample) / (ms_1 / 1000.0)
     bad = sum(1 for i in infos if i["status"] != 0 or i["residual"] > TOL * 1.0001)
+    retried = sum(1 for i in infos if i.get("retried"))
+    groups = len({autotune.size_class(p[0]) for p in pieces})
     return {"workload": f"{len(pieces)} pieces per rank, edges from {list(EDGES)} per axis, seeds 10000+; "
                         f"value noise period 8 thr 0.5, k U[0.5,2], tol {TOL:g}",
             "pieces": len(pieces), "dof": dof, "mixed_batched_solves_per_s": batched,
             "fp64_single_solves_per_s": single, "fp64_single_sample": len(sample),
             "speedup_batched_mixed_vs_fp64_single": batched / single,
             "mixed_batched_ms": ms_b, "iterations_mean": float(np.mean([i["iterations"] for i in infos])),
-            "pieces_not_converged": bad, "autotune": {str(k): {"sweeps": v["sweeps"], "tile": v["tile"]}
+            "pieces_not_converged": bad, "pieces_retried": retried, "size_classes": groups, "autotune": {str(k): {"sweeps": v["sweeps"], "tile": v["tile"]}
                                                        for k, v in settings.items()},
             "autotune_seconds": tune_s}
 
@@ -385,7 +482,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-pieces section")
     ap.add_argument("--batch", type=int, default=512, help="pieces in the batched section")
     ap.add_argument("--batch-sample", type=int, default=64, help="pieces the one-at-a-time FP64 leg solves")
-    ap.add_argument("--probe", choices=["stencil", "solve"], help="run one kernel or one solve alone (profiling)")
+    ap.add_argument("--large-n", type=int, default=256, help="edge of the --probe large piece")
+    ap.add_argument("--probe", choices=["stencil", "solve", "batch", "large"], help="run one kernel or one solve alone (profiling)")
     args = ap.parse_args()
     if args.probe:
         run_probe(args)

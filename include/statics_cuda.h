@@ -34,20 +34,25 @@ typedef enum sc_status {
 
 enum { SC_CELL_EMPTY = 0, SC_CELL_FREE = 1, SC_CELL_HELD = 2 };
 enum { SC_K_UNIFORM = 0, SC_K_LOGNORMAL = 1 };
-enum { SC_FP64 = 0, SC_MIXED = 1 };
+enum { SC_FP64 = 0, SC_MIXED = 1, SC_MIXED_FP32_KRYLOV = 2 };
 
 typedef struct sc_options {
     double tol;        /* stop at ||r|| <= tol ||b||; reference 1e-6 (bodies.rs:432) */
     int64_t max_iter;  /* CG iteration cap; reference 100000 (bodies.rs:351) */
     int64_t few;       /* coarsen while a piece has more parts than this; reference 64 (bodies.rs:430) */
-    int32_t precision; /* SC_FP64: the reference's algorithm in FP64. SC_MIXED: FP32 operators
-                          inside FP64 iterative refinement */
+    int32_t precision; /* SC_FP64: the reference's algorithm in FP64. SC_MIXED: FP64 conjugate
+                          gradients (vectors, operator, dots, scalars) preconditioned by the V-cycle
+                          in FP32 (stencil, smoother, transfers, coarse operators; FP64 top solve).
+                          SC_MIXED_FP32_KRYLOV: one CG with FP32 vectors and stencil as well, FP64
+                          dots and scalars, and the FP64 true residual replacing the FP32 one every
+                          few iterations (reliable updates) */
     int32_t sweeps;    /* block-Jacobi sweeps before and after each coarse correction; the
                           reference does 1 (bodies.rs:386, 397-401) */
-    double inner_tol;  /* SC_MIXED: relative residual each FP32 inner solve stops at */
+    double inner_tol;  /* unused (kept for layout) */
     int64_t timeout_ms;/* wall-clock bound of one call; 0 = none */
-    int32_t tile;      /* voxel pieces: parts per stencil tile (the window in which parts are
-                          grouped by axis); 0 = 1024 */
+    int32_t tile;      /* voxel pieces, level-0 stencil: a power of two >= 32 is the window of
+                          parts grouped by axis for the per-part stencil; 0 = that stencil with
+                          1024; 1 = the plane-pencil stencil (cells staged in shared memory) */
     int32_t reserved;
 } sc_options;
 
@@ -66,8 +71,8 @@ const char* sc_status_string(sc_status s);
 /* What a solve did. */
 #define SC_MAX_LEVELS 24
 typedef struct sc_solve_info {
-    int64_t iterations;      /* CG iterations (SC_MIXED: inner iterations, all refinement steps) */
-    int64_t refinements;     /* SC_MIXED: FP64 true-residual refinement steps */
+    int64_t iterations;      /* CG iterations */
+    int64_t refinements;     /* SC_MIXED_FP32_KRYLOV: FP64 true-residual replacements */
     int32_t levels;          /* levels of the hierarchy, level 0 included */
     int32_t status;          /* sc_status of the solve (batched solves: of this piece) */
     int64_t parts[SC_MAX_LEVELS];   /* parts per level */

@@ -4,6 +4,9 @@
 
 #include <chrono>
 #include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "kernels.cuh"
@@ -14,6 +17,40 @@ struct sc_context {
 };
 
 namespace sc {
+
+PhaseTimer::PhaseTimer(Context& c) : ctx(c) {
+    const char* e = std::getenv("SC_TIMING");
+    on = e && e[0] == '1';
+    t = std::chrono::steady_clock::now();
+    alloc_ms0 = c.mem.alloc_ms;
+    allocs0 = c.mem.allocs;
+}
+
+void PhaseTimer::note(const char* fmt, ...) {
+    if (!on) return;
+    va_list ap;
+    va_start(ap, fmt);
+    std::fprintf(stderr, "[sc] ");
+    std::vfprintf(stderr, fmt, ap);
+    std::fprintf(stderr, "\n");
+    va_end(ap);
+}
+
+void PhaseTimer::mark(const char* phase) {
+    if (!on) return;
+    SC_CK(cudaStreamSynchronize(ctx.stream));
+    auto now = std::chrono::steady_clock::now();
+    cudaMemPool_t pool;
+    uint64_t reserved = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx.device) == cudaSuccess)
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    std::fprintf(stderr, "[sc] %-22s %9.2f ms  alloc %8.2f ms (%lld)  held %6.2f GB  peak %6.2f GB  pool %6.2f GB\n",
+                 phase, std::chrono::duration<double, std::milli>(now - t).count(), ctx.mem.alloc_ms - alloc_ms0,
+                 (long long)(ctx.mem.allocs - allocs0), ctx.mem.now / 1e9, ctx.mem.peak / 1e9, reserved / 1e9);
+    t = now;
+    alloc_ms0 = ctx.mem.alloc_ms;
+    allocs0 = ctx.mem.allocs;
+}
 
 std::atomic<int64_t> g_launches{0};
 
@@ -92,6 +129,7 @@ Context::~Context() {
     partial.release();
     scal.release();
     if (cub_tmp) cudaFreeAsync(cub_tmp, stream);
+    mem.trim(stream);
     if (stream) {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
@@ -151,10 +189,11 @@ void check_options(const sc_options& o) {
     require(o.tol >= 0 && std::isfinite(o.tol), SC_BAD_INPUT, "tol must be finite and non-negative");
     require(o.max_iter >= 0, SC_BAD_INPUT, "max_iter must be non-negative");
     require(o.few >= 1, SC_BAD_INPUT, "few must be at least 1");
-    require(o.precision == SC_FP64 || o.precision == SC_MIXED, SC_BAD_INPUT, "unknown precision");
+    require(o.precision == SC_FP64 || o.precision == SC_MIXED || o.precision == SC_MIXED_FP32_KRYLOV, SC_BAD_INPUT,
+            "unknown precision");
     require(o.sweeps >= 1 && o.sweeps <= 8, SC_BAD_INPUT, "sweeps must be 1 to 8");
-    require(o.tile == 0 || (o.tile >= 32 && o.tile <= (1 << 20) && (o.tile & (o.tile - 1)) == 0), SC_BAD_INPUT,
-            "tile must be 0 or a power of two from 32");
+    require(o.tile == 0 || o.tile == 1 || (o.tile >= 32 && o.tile <= (1 << 20) && (o.tile & (o.tile - 1)) == 0), SC_BAD_INPUT,
+            "tile must be 0, 1 or a power of two from 32");
 }
 
 // The reference's Work for a solve of one piece: parts + pairs per level apply
@@ -215,6 +254,8 @@ sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double
     build_hierarchy(ctx, b, opt);
     auto t0 = std::chrono::steady_clock::now();
     if (opt.precision == SC_MIXED)
+        pcg_fp32_cycle(ctx, b, opt, x, st);
+    else if (opt.precision == SC_MIXED_FP32_KRYLOV)
         pcg_mixed(ctx, b, opt, x, st);
     else
         pcg_fp64(ctx, b, opt, x, st);
@@ -327,6 +368,8 @@ sc_status sc_solve_grid(sc_context* ctx, const sc_grid* g, const sc_options* opt
         check_grid(*g);
         check_options(*opt);
         auto b = std::make_unique<Batch>();
+        c.last.reset();  // the previous solve's hierarchy is not kept through this one
+        SC_CK(cudaStreamSynchronize(c.stream));
         c.mem.peak = c.mem.now;
         grid_level0(c, *b, {*g}, true, opt->tile);
         int64_t nodes = b->node_count[0];
@@ -368,6 +411,8 @@ sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, 
         check_options(*opt);
         std::vector<sc_grid> all(grids, grids + n);
         for (auto& g : all) check_grid(g);
+        c.last.reset();  // the previous solve's hierarchy is not kept through this one
+        SC_CK(cudaStreamSynchronize(c.stream));
         c.mem.peak = c.mem.now;
         int first = 0;
         while (first < n) {
@@ -382,6 +427,7 @@ sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, 
             }
             std::vector<sc_grid> gs(all.begin() + first, all.begin() + last);
             int m = last - first;
+            c.last.reset();
             auto b = std::make_unique<Batch>();
             grid_level0(c, *b, gs, true, opt->tile);
             DBuf<double> x;
@@ -429,6 +475,8 @@ sc_status sc_compliance_grad(sc_context* ctx, const sc_grid* g, const sc_options
         check_options(*opt);
         require(!g->on_device, SC_BAD_INPUT, "sc_compliance_grad takes host grids");
         auto b = std::make_unique<Batch>();
+        c.last.reset();  // the previous solve's hierarchy is not kept through this one
+        SC_CK(cudaStreamSynchronize(c.stream));
         c.mem.peak = c.mem.now;
         grid_level0(c, *b, {*g}, true, opt->tile);
         int64_t nodes = b->node_count[0];
@@ -534,6 +582,8 @@ sc_status sc_motions(sc_context* ctx, const sc_lattice* lat, const uint8_t* aliv
                         lat->bond_j[b] < lat->n_nodes,
                     SC_BAD_INPUT, "bond end out of range");
         auto b = std::make_unique<Batch>();
+        c.last.reset();  // the previous solve's hierarchy is not kept through this one
+        SC_CK(cudaStreamSynchronize(c.stream));
         c.mem.peak = c.mem.now;
         lattice_level0(c, *b, *lat, alive, gone, loads);
         DBuf<double> x;

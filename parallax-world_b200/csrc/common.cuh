@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <cstdint>
+#include <algorithm>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -37,20 +40,63 @@ inline void require(bool ok, sc_status s, const std::string& msg) {
     if (!ok) throw Error(s, msg);
 }
 
-// Device memory accounting of one context: what is held now and at most.
+// Device memory of one context: what is held now and at most, the host time spent in
+// the driver's allocate and free calls, and a cache of released blocks. Every buffer of a
+// context lives on the context's one stream, so a released block can be handed to the
+// next request on that stream at once (stream order keeps the old and new users apart),
+// as cudaFreeAsync / cudaMallocAsync would, but without calling the driver, whose
+// allocation calls were measured at milliseconds each: repeated solves of similar sizes
+// then allocate nothing. Requests are rounded up to size classes (1/8 steps of their
+// power of two, at least 512 bytes) so that similar sizes share blocks, and the cache
+// keeps at most twice the largest amount ever held at once; beyond that a released block
+// goes back to the pool.
 struct MemStats {
-    int64_t now = 0, peak = 0;
+    int64_t now = 0, peak = 0, top = 0;
+    double alloc_ms = 0;
+    int64_t allocs = 0;
+    std::multimap<size_t, void*> cache;  // block bytes -> block
+    size_t cached = 0;
     void add(int64_t b) {
         now += b;
         if (now > peak) peak = now;
+        if (now > top) top = now;
+    }
+    static size_t size_class(size_t bytes) {
+        if (bytes <= 512) return 512;
+        size_t p2 = size_t(1) << (63 - __builtin_clzll((unsigned long long)(bytes - 1)));  // < bytes <= 2 p2
+        size_t step = std::max<size_t>(p2 / 8, 512);
+        return (bytes + step - 1) / step * step;
+    }
+    // a cached block of exactly this size class, or null
+    void* take(size_t bytes) {
+        auto it = cache.find(bytes);
+        if (it == cache.end()) return nullptr;
+        void* p = it->second;
+        cached -= bytes;
+        cache.erase(it);
+        return p;
+    }
+    bool give(void* p, size_t bytes) {
+        if (cached + bytes > 2 * (size_t)top) return false;
+        cache.emplace(bytes, p);
+        cached += bytes;
+        return true;
+    }
+    // frees every cached block (stream-ordered on s)
+    void trim(cudaStream_t s) {
+        for (auto& kv : cache) cudaFreeAsync(kv.second, s);
+        cache.clear();
+        cached = 0;
     }
 };
 
-// A stream-ordered device array (cudaMallocAsync from the device's pool).
+// A device array on a context's stream: from the context's block cache, else from the
+// device's pool (cudaMallocAsync); released into the cache, else to the pool.
 template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t n = 0;
+    size_t bytes = 0;  // the block's size (at least n * sizeof(T))
     cudaStream_t s = nullptr;
     MemStats* stats = nullptr;
 
@@ -63,10 +109,12 @@ struct DBuf {
             release();
             p = o.p;
             n = o.n;
+            bytes = o.bytes;
             s = o.s;
             stats = o.stats;
             o.p = nullptr;
             o.n = 0;
+            o.bytes = 0;
         }
         return *this;
     }
@@ -74,20 +122,55 @@ struct DBuf {
 
     void release() {
         if (p) {
-            cudaFreeAsync(p, s);
-            if (stats) stats->now -= (int64_t)(n * sizeof(T));
+            if (stats) {
+                stats->now -= (int64_t)bytes;
+                if (!stats->give(p, bytes)) {
+                    auto t0 = std::chrono::steady_clock::now();
+                    cudaFreeAsync(p, s);
+                    stats->alloc_ms +=
+                        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                }
+            } else {
+                cudaFreeAsync(p, s);
+            }
         }
         p = nullptr;
         n = 0;
+        bytes = 0;
     }
     void alloc(size_t count, cudaStream_t stream, MemStats* st) {
         release();
         s = stream;
         stats = st;
         n = count;
-        if (count) {
-            SC_CK(cudaMallocAsync((void**)&p, count * sizeof(T), stream));
-            if (stats) stats->add((int64_t)(count * sizeof(T)));
+        if (!count) return;
+        size_t want = count * sizeof(T);
+        if (stats) {
+            want = MemStats::size_class(want);
+            if (void* q = stats->take(want)) {
+                p = static_cast<T*>(q);
+                bytes = want;
+                stats->add((int64_t)bytes);
+                return;
+            }
+        }
+        auto t0 = std::chrono::steady_clock::now();
+        cudaError_t e = cudaMallocAsync((void**)&p, want, stream);
+        if (e == cudaErrorMemoryAllocation && stats && stats->cached) {
+            cudaGetLastError();  // out of memory with blocks cached: give them back and retry
+            stats->trim(stream);
+            e = cudaMallocAsync((void**)&p, want, stream);
+        }
+        if (e != cudaSuccess) {
+            p = nullptr;
+            n = 0;
+            SC_CK(e);
+        }
+        bytes = want;
+        if (stats) {
+            stats->add((int64_t)bytes);
+            stats->alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            stats->allocs++;
         }
     }
     void zero() {

@@ -4,6 +4,8 @@
 // FP64 iterative refinement.
 #include <chrono>
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace sc {
@@ -265,6 +267,28 @@ __global__ void k_cg_beta(int np, CgScalars s, double* beta) {
     s.iters[p] += 1;
 }
 
+// beta for a preconditioner applied in lower precision (not exactly symmetric): the
+// Polak-Ribiere form (z', r' - r) / (z, r) = -alpha (z', Ap) / (z, r), which equals
+// next / rz when the preconditioner is symmetric; rz = next; counts the iteration
+__global__ void k_cg_beta_flex(int np, CgScalars s, const double* __restrict__ zap, double* beta) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np || s.done[p]) return;
+    beta[p] = -s.alpha[p] * zap[p] / s.rz[p];
+    s.rz[p] = s.next[p];
+    s.iters[p] += 1;
+}
+
+// b = a in another precision for the pieces not done, one block per chunk
+template <class A, class B>
+__global__ void __launch_bounds__(256) k_cast_chunks(const int64_t* __restrict__ chunk_lo,
+                                                     const int32_t* __restrict__ cpiece, const int32_t* __restrict__ done,
+                                                     const A* __restrict__ a, B* __restrict__ b) {
+    int c = blockIdx.x;
+    if (done && done[cpiece[c]]) return;
+    int64_t lo = 6 * chunk_lo[c], hi = 6 * chunk_lo[c + 1];
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) b[i] = (B)a[i];
+}
+
 // x += alpha p; r -= alpha Ap (bodies.rs:357-362), one block per chunk
 template <class V, class S>
 __global__ void __launch_bounds__(256) k_axpy2(const int64_t* __restrict__ chunk_lo, const int32_t* __restrict__ cpiece,
@@ -361,6 +385,7 @@ struct CgState {
     DBuf<int32_t> ndone;
     CgScalars s{};
     double* beta = nullptr;
+    double* zap = nullptr;  // (z, Ap) for the Polak-Ribiere beta
     int np = 0;
     void init(Context& ctx, int npieces, int32_t* status) {
         np = npieces;
@@ -380,6 +405,7 @@ struct CgState {
         s.next = q + 5 * np;
         s.alpha = q + 6 * np;
         beta = q + 7 * np;
+        zap = q + 8 * np;
         s.done = flags.get();
         s.iters = iters.get();
         s.status = status;
@@ -416,21 +442,41 @@ static void dot2(Context& ctx, const Level& L, const int32_t* done, const T* a, 
 }
 
 // PCG with per-piece scalars on level 0. V is the vector type of p, r, z, Ap; S the
-// type of x. On return x holds the solution of K x = rhs for each piece.
-template <class V, class S>
+// type of x; P the precision of the V-cycle preconditioner (with rp, zp its vectors when
+// it differs from V). On return x holds the solution of K x = rhs for each piece.
+template <class V, class S, class P = V>
 static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V* ap, double tol, int64_t max_iter,
                 CgState& cg, int64_t timeout_ms, std::chrono::steady_clock::time_point t_start,
-                const int32_t* start_done = nullptr) {
+                const int32_t* start_done = nullptr, P* rp = nullptr, P* zp = nullptr) {
     Level& L = b.levels[0];
     cudaStream_t st = ctx.stream;
     int np = b.npieces;
     int64_t n6 = 6 * L.n;
+    constexpr bool same = std::is_same<V, P>::value;
+    // z = M r
+    auto precondition = [&]() {
+        if constexpr (same) {
+            cycle<V>(ctx, b, 0, r, z, cg.s.done);
+        } else {
+            if (L.nchunks > 0) {
+                k_cast_chunks<V, P><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(),
+                                                                          cg.s.done, r, rp);
+                SC_LAUNCH_CK();
+            }
+            cycle<P>(ctx, b, 0, rp, zp, cg.s.done);
+            if (L.nchunks > 0) {
+                k_cast_chunks<P, V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(),
+                                                                          cg.s.done, zp, z);
+                SC_LAUNCH_CK();
+            }
+        }
+    };
     SC_CK(cudaMemsetAsync(x, 0, n6 * sizeof(S), st));
     SC_CK(cudaMemcpyAsync(r, rhs, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
     dot2<V>(ctx, L, nullptr, rhs, rhs, cg.s.bb, nullptr);
     k_cg_init<<<grid_for(np, 128), 128, 0, st>>>(np, tol, cg.s, start_done);
     SC_LAUNCH_CK();
-    cycle<V>(ctx, b, 0, r, z, cg.s.done);
+    precondition();
     SC_CK(cudaMemcpyAsync(p, z, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
     dot2<V>(ctx, L, cg.s.done, r, z, cg.s.rz, cg.s.rr);
     // one iteration (bodies.rs:351-371), ending with the next iteration's check
@@ -450,9 +496,14 @@ static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V*
                                                               cg.s.alpha, x, p, r, ap);
             SC_LAUNCH_CK();
         }
-        cycle<V>(ctx, b, 0, r, z, cg.s.done);
+        precondition();
         dot2<V>(ctx, L, cg.s.done, r, z, cg.s.next, cg.s.rr);
-        k_cg_beta<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.beta);
+        if constexpr (same) {
+            k_cg_beta<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.beta);
+        } else {
+            dot2<V>(ctx, L, cg.s.done, ap, z, cg.zap, nullptr);
+            k_cg_beta_flex<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.zap, cg.beta);
+        }
         SC_LAUNCH_CK();
         if (L.nchunks > 0) {
             k_pupdate<V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
@@ -642,10 +693,7 @@ __global__ void k_mixed_true(int np, int64_t max_iter, CgScalars s, const int32_
 // `period` iterations and whenever the FP32 residual claims convergence, and there the
 // true residual b - K x is recomputed by the FP64 stencil and replaces the FP32 one
 // (reliable updates): the FP64 iterative refinement. The dense top solve is FP64.
-void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& stats) {
-    auto t0 = std::chrono::steady_clock::now();
-    cudaStream_t st = ctx.stream;
-    int np = b.npieces;
+static void float_operators(Context& ctx, Batch& b) {
     for (size_t l = 0; l < b.levels.size(); l++) {
         Level& L = b.levels[l];
         if (L.val.size()) to_float(ctx, L.val, L.val32);
@@ -654,6 +702,41 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
         if (L.ptval.size()) to_float(ctx, L.ptval, L.ptval32);
         if (L.mf_r.size()) to_float(ctx, L.mf_r, L.mf_r32);
     }
+}
+
+// FP64 conjugate gradients (vectors, operator, dots and scalars in FP64) preconditioned
+// by the V-cycle in FP32 (stencil, smoother, transfers and coarse operators with FP32
+// accumulation; the dense top solve FP64). The FP32 cycle is not exactly symmetric, so
+// beta takes the Polak-Ribiere form.
+void pcg_fp32_cycle(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    float_operators(ctx, b);
+    alloc_cycle<float>(ctx, b);
+    Level& L = b.levels[0];
+    int64_t n6 = 6 * L.n;
+    x.alloc(n6, ctx.stream, &ctx.mem);
+    DBuf<double> r, z, p, ap;
+    for (auto* v : {&r, &z, &p, &ap}) v->alloc(n6, ctx.stream, &ctx.mem);
+    DBuf<float> r32, z32;
+    r32.alloc(n6, ctx.stream, &ctx.mem);
+    z32.alloc(n6, ctx.stream, &ctx.mem);
+    CgState cg;
+    cg.init(ctx, b.npieces, b.status_d.get());
+    pcg<double, double, float>(ctx, b, b.loads.get(), x.get(), r.get(), z.get(), p.get(), ap.get(), opt.tol,
+                               opt.max_iter, cg, opt.timeout_ms, t0, nullptr, r32.get(), z32.get());
+    std::vector<int64_t> it(b.npieces);
+    cg.iters.download(it.data(), b.npieces);
+    SC_CK(cudaStreamSynchronize(ctx.stream));
+    stats.iterations = it;
+    stats.refinements.assign(b.npieces, 0);
+    true_residual(ctx, b, x.get(), stats.residual);
+}
+
+void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t st = ctx.stream;
+    int np = b.npieces;
+    float_operators(ctx, b);
     alloc_cycle<float>(ctx, b);
     Level& L = b.levels[0];
     int64_t n6 = 6 * L.n;

@@ -16,6 +16,7 @@
 // read x and write y (2 * 6 * w per part) plus the cell table (32 B per free cell).
 #include <cub/cub.cuh>
 
+#include "level0_blocks.cuh"
 #include "solver.cuh"
 #include "template_gen.cuh"
 
@@ -270,13 +271,14 @@ __global__ void k_row_count(int64_t n, const int8_t* __restrict__ axis, const in
     cnt[k] = c;
 }
 
-__global__ void k_row_fill(int64_t n, double s, const int8_t* __restrict__ axis, const int32_t* __restrict__ cella,
+// The level-0 pattern of row k (its own block and every part sharing a cell with it,
+// columns sorted) with each block's origin in the cell template (level0_blocks.cuh).
+__global__ void k_row_fill(int64_t n, const int32_t* __restrict__ cella,
                            const int32_t* __restrict__ cellb, const int4* __restrict__ cell,
-                           const int64_t* __restrict__ rowptr, int32_t* __restrict__ col, double* __restrict__ val) {
+                           const int64_t* __restrict__ rowptr, int32_t* __restrict__ col, uint8_t* __restrict__ desc) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
-    int ax = axis[k];
-    // gather (column, cell side, slot of column, slot of k)
+    // gather (column, cell side, slot of column)
     int32_t cols[11];
     int8_t sideof[11], slotof[11];
     int m = 0;
@@ -313,28 +315,16 @@ __global__ void k_row_fill(int64_t n, double s, const int8_t* __restrict__ axis,
         slotof[j + 1] = l0;
     }
     int64_t base = rowptr[k];
-    int32_t CA = cella[k], CB = cellb[k];
-    double kA = CA >= 0 ? (double)__int_as_float(cell[2 * CA + 1].z) : 0.0;
-    double kB = CB >= 0 ? (double)__int_as_float(cell[2 * CB + 1].z) : 0.0;
-    int slA = 2 * ax + 1, slB = 2 * ax;
     for (int e = 0; e < m; e++) {
         col[base + e] = cols[e];
-        double* blk = val + 36 * (base + e);
-        for (int i = 0; i < 6; i++)
-            for (int j = 0; j < 6; j++) {
-                double v;
-                if (sideof[e] < 0) {
-                    v = 0.0;
-                    if (CA >= 0) v += kA * tpl_scaled(6 * slA + i, 6 * slA + j, s);
-                    if (CB >= 0) v += kB * tpl_scaled(6 * slB + i, 6 * slB + j, s);
-                } else if (sideof[e] == 0) {
-                    v = kA * tpl_scaled(6 * slA + i, 6 * slotof[e] + j, s);
-                } else {
-                    v = kB * tpl_scaled(6 * slB + i, 6 * slotof[e] + j, s);
-                }
-                blk[6 * i + j] = v;
-            }
+        desc[base + e] = sideof[e] < 0 ? K0_DIAG : (uint8_t)((sideof[e] << 3) | slotof[e]);
     }
+}
+
+// the cell template at spacing s (entry (i, j) times s, and s again for each rotation index)
+__global__ void k_scaled_template(double s, double* __restrict__ out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < 36 * 36) out[e] = tpl_scaled(e / 36, e % 36, s);
 }
 
 // ---- the matrix-free stencil ---------------------------------------------------------
@@ -994,7 +984,8 @@ void grid_cell_energy(Context& ctx, const Batch& b, const double* x, double* ene
 // Builds level 0 of a batch of voxel pieces. The grids' state/k are uploaded (or
 // copied device to device) into one concatenated array.
 void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks, int32_t tile) {
-    const int64_t TILE = tile > 0 ? tile : STENCIL_TILE;
+    const int64_t TILE = tile > 1 ? tile : STENCIL_TILE;
+    PhaseTimer pt(ctx);
     cudaStream_t st = ctx.stream;
     MemStats* ms = &ctx.mem;
     int np = (int)grids.size();
@@ -1163,7 +1154,7 @@ void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool
         SC_CK(cudaMemcpyAsync(g.geo.get(), geo.data(), geo.size() * sizeof(PieceGeo), cudaMemcpyHostToDevice, st));
         SC_CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
     }
-    g.pencil = tile == 0;
+    g.pencil = tile == 1;
     SC_LAUNCH_CK();
     // parts in order, grouped by axis only within tiles of STENCIL_TILE parts: the
     // stencil sweeps the piece once in part order (x neighbours stay in L2) while a
@@ -1209,14 +1200,18 @@ void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool
         SC_CK(cudaMemcpyAsync(&L.nnzb, L.rowptr.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         SC_CK(cudaStreamSynchronize(st));
         L.col.alloc(L.nnzb, st, ms);
-        L.val.alloc(36 * L.nnzb, st, ms);
-        k_row_fill<<<grid_for(n, 128), 128, 0, st>>>(n, g.s, g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(),
-                                                     L.rowptr.get(), L.col.get(), L.val.get());
+        L.desc.alloc(L.nnzb, st, ms);
+        k_row_fill<<<grid_for(n, 128), 128, 0, st>>>(n, g.cella.get(), g.cellb.get(), g.cell.get(),
+                                                     L.rowptr.get(), L.col.get(), L.desc.get());
+        SC_LAUNCH_CK();
+        g.tpl_s.alloc(36 * 36, st, ms);
+        k_scaled_template<<<grid_for(36 * 36, 256), 256, 0, st>>>(g.s, g.tpl_s.get());
         SC_LAUNCH_CK();
     }
     L.matrix_free = true;
     g.grid_off = std::move(goff);
     SC_CK(cudaStreamSynchronize(st));
+    pt.mark("level 0 (grid)");
 }
 
 }  // namespace sc

@@ -17,6 +17,7 @@
 #include <chrono>
 
 #include "kernels.cuh"
+#include "level0_blocks.cuh"
 
 namespace sc {
 
@@ -32,6 +33,22 @@ __global__ void k_find_diag_invert(int64_t n, const int64_t* __restrict__ rowptr
     bool ok = e < rowptr[k + 1] && col[e] == (int32_t)k;
     double tmp[36];
     if (ok) ok = invert6(val + 36 * e, tmp);
+    if (!ok) {
+        for (int i = 0; i < 36; i++) tmp[i] = 0.0;
+        if (status) atomicMax(status + piece[k], (int)SC_BREAKDOWN);
+    }
+    for (int i = 0; i < 36; i++) inv[36 * k + i] = tmp[i];
+}
+
+// the same for a matrix-free level 0: each part's own block from the cell template
+__global__ void k_diag_invert_k0(int64_t n, K0View v, double* __restrict__ inv, const int32_t* __restrict__ piece,
+                                 int32_t* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    K0Row row = k0_row(v, k);
+    double blk[36], tmp[36];
+    for (int t = 0; t < 36; t++) blk[t] = k0_entry(v.tpl_s, row, K0_DIAG, t / 6, t % 6);
+    bool ok = invert6(blk, tmp);
     if (!ok) {
         for (int i = 0; i < 36; i++) tmp[i] = 0.0;
         if (status) atomicMax(status + piece[k], (int)SC_BREAKDOWN);
@@ -191,78 +208,72 @@ __global__ void k_count_P(int64_t n, const int64_t* __restrict__ rowptr, const i
     cnt[k] = up[k] >= 0 ? rowptr[k + 1] - rowptr[k] : 0;
 }
 __global__ void k_fill_P(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
-                         const int32_t* __restrict__ up, const int64_t* __restrict__ off, uint64_t* __restrict__ keys) {
+                         const int32_t* __restrict__ up, const int64_t* __restrict__ off, uint64_t* __restrict__ keys,
+                         int cb) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (up[k] < 0) return;
     int64_t o = off[k];
-    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) keys[o++] = ((uint64_t)k << 32) | (uint32_t)up[col[e]];
+    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) keys[o++] = ((uint64_t)k << cb) | (uint32_t)up[col[e]];
 }
-__global__ void k_count_KP(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+// candidates of K P, per block K_kq (entry e of K, row krow[e]): one per block P_qf,
+// (k, col of P_qf) with contribution (e << 32 | f). Entries are laid out in entry order,
+// so the list is row by row, K's columns in order, then P's.
+__global__ void k_count_KP(int64_t nnz, const int32_t* __restrict__ krow, const int32_t* __restrict__ col,
                            const int64_t* __restrict__ prow, const int32_t* __restrict__ up, int64_t* __restrict__ cnt) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    int64_t c = 0;
-    if (up[k] >= 0)
-        for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
-            int32_t o = col[e];
-            c += prow[o + 1] - prow[o];
-        }
-    cnt[k] = c;
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    int32_t q = col[e];
+    cnt[e] = up[krow[e]] >= 0 ? prow[q + 1] - prow[q] : 0;
 }
-// candidates of K P row k: (k, col of P_qf) for each block K_kq and each block P_qf,
-// contribution (entry of K_kq << 32 | entry of P_qf)
-__global__ void k_fill_KP(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+__global__ void k_fill_KP(int64_t nnz, const int32_t* __restrict__ krow, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
                           const int32_t* __restrict__ up, const int64_t* __restrict__ off, uint64_t* __restrict__ keys,
-                          uint64_t* __restrict__ vals) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n) return;
+                          uint64_t* __restrict__ vals, int cb) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    int32_t k = krow[e];
     if (up[k] < 0) return;
-    int64_t o = off[k];
-    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
-        int32_t q = col[e];
-        for (int64_t f = prow[q]; f < prow[q + 1]; f++) {
-            keys[o] = ((uint64_t)k << 32) | (uint32_t)pcol[f];
-            vals[o] = ((uint64_t)e << 32) | (uint64_t)f;
-            o++;
-        }
+    int32_t q = col[e];
+    int64_t o = off[e];
+    for (int64_t f = prow[q]; f < prow[q + 1]; f++, o++) {
+        keys[o] = ((uint64_t)(uint32_t)k << cb) | (uint32_t)pcol[f];
+        vals[o] = ((uint64_t)e << 32) | (uint64_t)f;
     }
 }
-// per P entry (k, c): the columns d >= c of KP row k
-__global__ void k_count_C(int64_t n, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+// per P entry e = (k, c), k = prow_of[e]: the columns d >= c of KP row k
+__global__ void k_count_C(int64_t pnnz, const int32_t* __restrict__ prow_of, const int32_t* __restrict__ pcol,
                           const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol, int64_t* __restrict__ cnt) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    for (int64_t e = prow[k]; e < prow[k + 1]; e++) {
-        int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], pcol[e]);
-        cnt[e] = kprow[k + 1] - lb;
-    }
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= pnnz) return;
+    int32_t k = prow_of[e];
+    int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], pcol[e]);
+    cnt[e] = kprow[k + 1] - lb;
 }
 // candidates of the upper P'KP: (c, d) for each entry (k, c) of P and each block
 // (k, d >= c) of K P, contribution (entry of P << 32 | entry of KP)
-__global__ void k_fill_C(int64_t n, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+__global__ void k_fill_C(int64_t pnnz, const int32_t* __restrict__ prow_of, const int32_t* __restrict__ pcol,
                          const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol,
-                         const int64_t* __restrict__ off, uint64_t* __restrict__ keys, uint64_t* __restrict__ vals) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    for (int64_t e = prow[k]; e < prow[k + 1]; e++) {
-        int32_t c = pcol[e];
-        int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], c);
-        int64_t o = off[e];
-        for (int64_t f = lb; f < kprow[k + 1]; f++) {
-            keys[o] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)kpcol[f];
-            vals[o] = ((uint64_t)e << 32) | (uint64_t)f;
-            o++;
-        }
+                         const int64_t* __restrict__ off, uint64_t* __restrict__ keys, uint64_t* __restrict__ vals,
+                         int cb) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= pnnz) return;
+    int32_t k = prow_of[e];
+    int32_t c = pcol[e];
+    int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], c);
+    int64_t o = off[e];
+    for (int64_t f = lb; f < kprow[k + 1]; f++, o++) {
+        keys[o] = ((uint64_t)(uint32_t)c << cb) | (uint32_t)kpcol[f];
+        vals[o] = ((uint64_t)e << 32) | (uint64_t)f;
     }
 }
+// keys are (row << cb | col)
 __global__ void k_unpack_pattern(int64_t m, const uint64_t* __restrict__ keys, int32_t* __restrict__ col,
-                                 int32_t* __restrict__ row) {
+                                 int32_t* __restrict__ row, int cb) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= m) return;
-    col[i] = (int32_t)(keys[i] & 0xffffffffu);
-    row[i] = (int32_t)(keys[i] >> 32);
+    col[i] = (int32_t)(keys[i] & ((uint64_t(1) << cb) - 1));
+    row[i] = (int32_t)(keys[i] >> cb);
 }
 
 // ---- numeric products, one warp per output row ----------------------------------------
@@ -305,22 +316,36 @@ __device__ __forceinline__ void warp_block_mac(int lane, const double* __restric
 }
 
 // S[k][pos(up[o])] += K_ko R_o over the row; then P_k = delta R_k - step D_k^-1 S.
+// K0: level 0 of voxel pieces, blocks made from the cell template (val unused).
+template <bool K0>
 __global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restrict__ rowptr,
                                                const int32_t* __restrict__ col, const double* __restrict__ val,
-                                               const int32_t* __restrict__ up, const double* __restrict__ rvec,
-                                               const double* __restrict__ inv, const double* __restrict__ step,
-                                               const int32_t* __restrict__ piece, const int64_t* __restrict__ prow,
-                                               const int32_t* __restrict__ pcol, double* __restrict__ pval) {
+                                               K0View k0, const int32_t* __restrict__ up,
+                                               const double* __restrict__ rvec, const double* __restrict__ inv,
+                                               const double* __restrict__ step, const int32_t* __restrict__ piece,
+                                               const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+                                               double* __restrict__ pval) {
+    __shared__ double blk_s[8][36];  // K0: the warp's current block
     int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (k >= n) return;
     int lane = threadIdx.x & 31;
     if (up[k] < 0) return;
+    double* blk = blk_s[(threadIdx.x >> 5) & 7];
+    K0Row row{};
+    if (K0) row = k0_row(k0, k);
     int64_t p0 = prow[k], p1 = prow[k + 1];
     for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
         int32_t o = col[e];
         int64_t pos = lower_bound_i32(pcol, p0, p1, up[o]);
         double rv[3] = {rvec[3 * (int64_t)o], rvec[3 * (int64_t)o + 1], rvec[3 * (int64_t)o + 2]};
-        warp_block_mac<false, true>(lane, val + 36 * e, nullptr, rv, pval + 36 * pos);
+        const double* A = val + 36 * e;
+        if (K0) {
+            uint8_t d = k0.desc[e];
+            for (int t = lane; t < 36; t += 32) blk[t] = k0_entry(k0.tpl_s, row, d, t / 6, t % 6);
+            __syncwarp();
+            A = blk;
+        }
+        warp_block_mac<false, true>(lane, A, nullptr, rv, pval + 36 * pos);
         __syncwarp();
     }
     double st = step[piece[k]];
@@ -365,28 +390,91 @@ __global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restr
 // pair (a << 32 | b) of a left block and a right block, in the order the candidates were
 // generated (a stable sort), so the sum is deterministic. 36 threads per output block,
 // one per entry; the left operand transposed when TA.
-constexpr int SUM_GROUPS = 8;  // output blocks per thread block (8 * 36 threads)
-template <bool TA>
-__global__ void __launch_bounds__(36 * SUM_GROUPS) k_sum_products(int64_t nout, const int64_t* __restrict__ seg,
-                                                                  const uint64_t* __restrict__ vals,
-                                                                  const double* __restrict__ A,
-                                                                  const double* __restrict__ B,
-                                                                  double* __restrict__ out) {
-    int g = threadIdx.x / 36, e = threadIdx.x % 36;
-    int64_t q = (int64_t)blockIdx.x * SUM_GROUPS + g;
-    if (q >= nout) return;
-    int r = e / 6, c = e % 6;
-    double acc = 0.0;
-    for (int64_t i = seg[q]; i < seg[q + 1]; i++) {
-        uint64_t v = vals[i];
-        const double* a = A + 36 * (int64_t)(v >> 32);
-        const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j < 6; j++) s = fma(TA ? a[j * 6 + r] : a[r * 6 + j], bb[j * 6 + c], s);
-        acc += s;
+constexpr int SUM_GROUPS = 32;  // output blocks per thread block, 6 threads each
+constexpr int SUM_THREADS = 6 * SUM_GROUPS;
+// out[q] = sum over q's contributions (a << 32 | b) of op(A_a) B_b, op = transpose when TA.
+// Six threads per output block, thread c owning its column c: each reads the whole left
+// block (the same addresses across the six, one transaction) and its column of the
+// right one, so a contribution costs 42 loads a thread instead of 12 for each of 36
+// threads. Every entry is summed over the contributions in list order, each
+// contribution's six products first, as a one-thread-per-entry sum would.
+// K0 (K P on a matrix-free level 0): A_a is block a of the level-0 pattern, made from the
+// cell template (krow gives its row); A is unused, and blocks stay resident, striding
+// over the outputs (the template is staged once per block).
+template <bool TA, bool K0>
+__global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, const int64_t* __restrict__ seg,
+                                                             const uint64_t* __restrict__ vals,
+                                                             const double* __restrict__ A,
+                                                             const double* __restrict__ B, double* __restrict__ out,
+                                                             K0View k0, const int32_t* __restrict__ krow) {
+    __shared__ double T[K0 ? 36 * 36 : 1];
+    if (K0) {
+        for (int t = threadIdx.x; t < 36 * 36; t += blockDim.x) T[t] = k0.tpl_s[t];
+        __syncthreads();
     }
-    out[36 * q + e] = acc;
+    const int g = threadIdx.x / 6, c = threadIdx.x % 6;
+    for (int64_t q = (int64_t)blockIdx.x * SUM_GROUPS + g; q < nout; q += K0 ? (int64_t)gridDim.x * SUM_GROUPS : nout) {
+        int64_t i = seg[q];
+        const int64_t end = seg[q + 1];
+        K0Row row{};
+        if (K0 && i < end) row = k0_row(k0, krow[vals[i] >> 32]);
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        // one contribution's operands: column c of its right block, and its left block
+        // (or, K0, the block's template descriptor)
+        struct Ops {
+            double bc[6];
+            double av[K0 ? 1 : 36];
+            uint8_t d;
+        };
+        auto load = [&](uint64_t v, Ops& o) {
+            const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
+#pragma unroll
+            for (int j = 0; j < 6; j++) o.bc[j] = bb[j * 6 + c];
+            if (K0) {
+                o.d = k0.desc[v >> 32];
+            } else {
+                const double2* a2 = reinterpret_cast<const double2*>(A + 36 * (int64_t)(v >> 32));
+#pragma unroll
+                for (int t = 0; t < 18; t++) {
+                    double2 w = a2[t];
+                    o.av[2 * t] = w.x;
+                    o.av[2 * t + 1] = w.y;
+                }
+            }
+        };
+        // acc(r) += sum_j op(A)(r, j) B(j, c)
+        auto add = [&](const Ops& o) {
+#pragma unroll
+            for (int r = 0; r < 6; r++) {
+                double s = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; j++) {
+                    double arj;
+                    if (K0)
+                        arj = k0_entry(T, row, o.d, r, j);
+                    else
+                        arj = TA ? o.av[j * 6 + r] : o.av[r * 6 + j];
+                    s = fma(arj, o.bc[j], s);
+                }
+                acc[r] += s;
+            }
+        };
+        // two contributions' loads in flight, added in list order
+        for (; i + 2 <= end; i += 2) {
+            Ops o0, o1;
+            load(vals[i], o0);
+            load(vals[i + 1], o1);
+            add(o0);
+            add(o1);
+        }
+        if (i < end) {
+            Ops o0;
+            load(vals[i], o0);
+            add(o0);
+        }
+#pragma unroll
+        for (int r = 0; r < 6; r++) out[36 * q + 6 * r + c] = acc[r];
+    }
 }
 
 // P' as its own block rows: block t = transpose of P's block tent[t]
@@ -442,27 +530,35 @@ __global__ void k_rvec(int64_t n, const int32_t* __restrict__ up, const double* 
 }
 
 // ---- dense top ---------------------------------------------------------------------
-__global__ void k_dense_from_bsr(int top_i, const int32_t* __restrict__ top, const int64_t* __restrict__ pstart,
-                                 const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
-                                 const double* __restrict__ val, double* __restrict__ A) {
-    int p = top[top_i];
-    int64_t k0 = pstart[p], k1 = pstart[p + 1];
-    int64_t n = 6 * (k1 - k0);
-    for (int64_t k = k0 + blockIdx.x; k < k1; k += gridDim.x)
+// The dense top of each listed piece, block (., i) for top i: its blocks scattered into
+// the piece's n x n row-major matrix at A + off[i] (zeroed beforehand).
+template <bool K0>
+__global__ void k_dense_from_bsr_all(const int32_t* __restrict__ top, const int64_t* __restrict__ pstart,
+                                     const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                     const double* __restrict__ val, K0View k0, const int64_t* __restrict__ off,
+                                     double* __restrict__ A_all) {
+    int p = top[blockIdx.y];
+    int64_t k0p = pstart[p], k1 = pstart[p + 1];
+    int64_t n = 6 * (k1 - k0p);
+    double* A = A_all + off[blockIdx.y];
+    for (int64_t k = k0p + blockIdx.x; k < k1; k += gridDim.x) {
+        K0Row row{};
+        if (K0) row = k0_row(k0, k);
         for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
             int64_t j = col[e];
             for (int t = threadIdx.x; t < 36; t += blockDim.x) {
                 int r = t / 6, c = t % 6;
-                A[(6 * (k - k0) + r) * n + 6 * (j - k0) + c] = val[36 * e + t];
+                A[(6 * (k - k0p) + r) * n + 6 * (j - k0p) + c] =
+                    K0 ? k0_entry(k0.tpl_s, row, k0.desc[e], r, c) : val[36 * e + t];
             }
         }
+    }
 }
 
-// Left-looking Cholesky in the reference's order (bodies.rs:307-313), then
-// X = L^-1 by columns and Kinv = X' X. One block per piece.
-__global__ void __launch_bounds__(1024) k_cholesky_inverse(int n, double* __restrict__ A, double* __restrict__ X,
-                                                           double* __restrict__ Kinv, int32_t* __restrict__ status,
-                                                           int piece) {
+// Left-looking Cholesky in the reference's order (bodies.rs:307-313), then X = L^-1 by
+// columns and Kinv = X' X written over A (A is not read once X is complete). One block.
+__device__ void cholesky_inverse_block(int n, double* A, double* __restrict__ X, int32_t* __restrict__ status,
+                                       int piece) {
     __shared__ double red[1024];
     __shared__ double dsh;
     __shared__ int bad;
@@ -508,8 +604,21 @@ __global__ void __launch_bounds__(1024) k_cholesky_inverse(int n, double* __rest
         int k0 = i > j ? i : j;
         double t = 0.0;
         for (int k = k0; k < n; k++) t = fma(X[(int64_t)k * n + i], X[(int64_t)k * n + j], t);
-        Kinv[e] = t;
+        A[e] = t;
     }
+}
+
+// Every listed piece's top at once, one block per piece: A_all[off[i]..] holds the dense
+// matrix on entry and its inverse on exit; X_all is scratch of the same layout.
+__global__ void __launch_bounds__(1024) k_cholesky_inverse_all(const int32_t* __restrict__ top,
+                                                               const int64_t* __restrict__ pstart,
+                                                               const int64_t* __restrict__ off, double* A_all,
+                                                               double* __restrict__ X_all,
+                                                               int32_t* __restrict__ status) {
+    int p = top[blockIdx.x];
+    int n = (int)(6 * (pstart[p + 1] - pstart[p]));
+    if (n == 0) return;
+    cholesky_inverse_block(n, A_all + off[blockIdx.x], X_all + off[blockIdx.x], status, p);
 }
 
 __global__ void k_fill_i32(int64_t n, int32_t* __restrict__ a, int32_t v) {
@@ -550,40 +659,43 @@ void exclusive_scan(Context& ctx, const int64_t* in, int64_t* out, int64_t n) {
     cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, in, out, n, ctx.stream);
 }
 
-// Sorted, unique (row << 32 | col) keys -> CSR pattern.
+// Keys (row << cb | col), cb = bits_for(ncols), sorted and made unique -> CSR pattern.
+// The sort ping-pongs between `keys` and a second buffer (no copy of them in scratch).
 void keys_to_csr(Context& ctx, DBuf<uint64_t>& keys, int64_t nkeys, int64_t nrows, int64_t ncols, DBuf<int64_t>& rowptr,
                  DBuf<int32_t>& col, int64_t& nnz) {
     cudaStream_t st = ctx.stream;
     MemStats* ms = &ctx.mem;
-    DBuf<uint64_t> sorted;
-    sorted.alloc(std::max<int64_t>(nkeys, 1), st, ms);
-    int end_bit = 32 + bits_for(nrows);
+    const int cb = bits_for(ncols);
+    DBuf<uint64_t> other;
+    other.alloc(std::max<int64_t>(nkeys, 1), st, ms);
+    int end_bit = cb + bits_for(nrows);
     size_t tb = 0;
     if (nkeys > 0) {
-        cub::DeviceRadixSort::SortKeys(nullptr, tb, keys.get(), sorted.get(), nkeys, 0, end_bit, st);
-        cub::DeviceRadixSort::SortKeys(ctx.cub_scratch(tb), tb, keys.get(), sorted.get(), nkeys, 0, end_bit, st);
+        cub::DoubleBuffer<uint64_t> dk(keys.get(), other.get());
+        cub::DeviceRadixSort::SortKeys(nullptr, tb, dk, nkeys, 0, end_bit, st);
+        cub::DeviceRadixSort::SortKeys(ctx.cub_scratch(tb), tb, dk, nkeys, 0, end_bit, st);
+        if (dk.Current() != keys.get()) std::swap(keys, other);  // `keys` holds the sorted keys
     }
-    keys.release();
+    other.release();
     DBuf<uint64_t> uniq;
     uniq.alloc(std::max<int64_t>(nkeys, 1), st, ms);
     DBuf<int64_t> nsel;
     nsel.alloc(1, st, ms);
     nsel.zero();
     if (nkeys > 0) {
-        cub::DeviceSelect::Unique(nullptr, tb, sorted.get(), uniq.get(), nsel.get(), nkeys, st);
-        cub::DeviceSelect::Unique(ctx.cub_scratch(tb), tb, sorted.get(), uniq.get(), nsel.get(), nkeys, st);
+        cub::DeviceSelect::Unique(nullptr, tb, keys.get(), uniq.get(), nsel.get(), nkeys, st);
+        cub::DeviceSelect::Unique(ctx.cub_scratch(tb), tb, keys.get(), uniq.get(), nsel.get(), nkeys, st);
     }
     nnz = d2h_i64(ctx, nsel.get());
-    sorted.release();
+    keys.release();
     col.alloc(std::max<int64_t>(nnz, 1), st, ms);
     DBuf<int32_t> rows;
     rows.alloc(std::max<int64_t>(nnz, 1), st, ms);
-    k_unpack_pattern<<<grid_for(nnz, 256), 256, 0, st>>>(nnz, uniq.get(), col.get(), rows.get());
+    k_unpack_pattern<<<grid_for(nnz, 256), 256, 0, st>>>(nnz, uniq.get(), col.get(), rows.get(), cb);
     SC_LAUNCH_CK();
     rowptr.alloc(nrows + 1, st, ms);
     k_offsets_from_sorted<<<grid_for(nnz + 1, 256), 256, 0, st>>>(nnz, rows.get(), nrows, rowptr.get());
     SC_LAUNCH_CK();
-    (void)ncols;
 }
 
 __global__ void k_seg_flags(int64_t m, const uint64_t* __restrict__ keys, int64_t* __restrict__ flag) {
@@ -593,14 +705,14 @@ __global__ void k_seg_flags(int64_t m, const uint64_t* __restrict__ keys, int64_
 }
 __global__ void k_seg_starts(int64_t m, const uint64_t* __restrict__ keys, const int64_t* __restrict__ flag,
                              const int64_t* __restrict__ idx, int64_t* __restrict__ seg, int32_t* __restrict__ col,
-                             int32_t* __restrict__ row) {
+                             int32_t* __restrict__ row, int cb) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= m) return;
     if (flag[i]) {
         int64_t u = idx[i];
         seg[u] = i;
-        col[u] = (int32_t)(keys[i] & 0xffffffffu);
-        row[u] = (int32_t)(keys[i] >> 32);
+        col[u] = (int32_t)(keys[i] & ((uint64_t(1) << cb) - 1));
+        row[u] = (int32_t)(keys[i] >> cb);
     }
 }
 
@@ -608,20 +720,24 @@ __global__ void k_seg_starts(int64_t m, const uint64_t* __restrict__ keys, const
 // and for every stored block the range seg[q] .. seg[q+1] of its contributions in
 // `vals` (sorted by output block, candidate order kept within one).
 void keys_to_csr_with(Context& ctx, DBuf<uint64_t>& keys, DBuf<uint64_t>& vin, int64_t nkeys, int64_t nrows,
-                      DBuf<int64_t>& rowptr, DBuf<int32_t>& col, int64_t& nnz, DBuf<int64_t>& seg,
+                      int64_t ncols, DBuf<int64_t>& rowptr, DBuf<int32_t>& col, int64_t& nnz, DBuf<int64_t>& seg,
                       DBuf<uint64_t>& vals) {
     cudaStream_t st = ctx.stream;
     MemStats* ms = &ctx.mem;
+    const int cb = bits_for(ncols);
     DBuf<uint64_t> sorted;
     sorted.alloc(std::max<int64_t>(nkeys, 1), st, ms);
     vals.alloc(std::max<int64_t>(nkeys, 1), st, ms);
-    int end_bit = 32 + bits_for(nrows);
+    int end_bit = cb + bits_for(nrows);
     size_t tb = 0;
     if (nkeys > 0) {
-        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), sorted.get(), vin.get(), vals.get(), nkeys, 0, end_bit,
-                                        st);
-        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, keys.get(), sorted.get(), vin.get(), vals.get(), nkeys,
-                                        0, end_bit, st);
+        // ping-pong between the inputs and the outputs (no copies in scratch); the sort
+        // is stable, so each block's contributions keep their generation order
+        cub::DoubleBuffer<uint64_t> dk(keys.get(), sorted.get()), dv(vin.get(), vals.get());
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, nkeys, 0, end_bit, st);
+        cub::DeviceRadixSort::SortPairs(ctx.cub_scratch(tb), tb, dk, dv, nkeys, 0, end_bit, st);
+        if (dk.Current() != sorted.get()) std::swap(keys, sorted);
+        if (dv.Current() != vals.get()) std::swap(vin, vals);
     }
     keys.release();
     vin.release();
@@ -641,7 +757,7 @@ void keys_to_csr_with(Context& ctx, DBuf<uint64_t>& keys, DBuf<uint64_t>& vin, i
     rows.alloc(std::max<int64_t>(nnz, 1), st, ms);
     if (nkeys > 0) {
         k_seg_starts<<<grid_for(nkeys, 256), 256, 0, st>>>(nkeys, sorted.get(), flag.get(), idx.get(), seg.get(),
-                                                          col.get(), rows.get());
+                                                          col.get(), rows.get(), cb);
         SC_LAUNCH_CK();
     }
     SC_CK(cudaMemcpyAsync(seg.get() + nnz, &nkeys, sizeof(int64_t), cudaMemcpyHostToDevice, st));
@@ -673,6 +789,23 @@ void setup_chunks(Context& ctx, Level& L, int32_t np) {
     L.chunk_piece.upload(cp.data(), cp.size());
     L.piece_chunk.alloc(np + 1, ctx.stream, &ctx.mem);
     L.piece_chunk.upload(pc.data(), np + 1);
+}
+
+// The template view of a matrix-free level 0 during setup (all null otherwise).
+static K0View k0_view(const Batch& b, const Level& L) {
+    K0View v{};
+    if (L.matrix_free && L.desc.size()) {
+        const Grid0& g = b.grid;
+        v = K0View{L.desc.get(), g.axis.get(), g.cella.get(), g.cellb.get(), g.cell.get(), g.tpl_s.get()};
+    }
+    return v;
+}
+
+static void invert_blocks_k0(Context& ctx, const Batch& b, Level& L, int32_t* status) {
+    L.inv.alloc(36 * L.n, ctx.stream, &ctx.mem);
+    k_diag_invert_k0<<<grid_for(L.n, 128), 128, 0, ctx.stream>>>(L.n, k0_view(b, L), L.inv.get(), L.piece.get(),
+                                                                 status);
+    SC_LAUNCH_CK();
 }
 
 void invert_blocks(Context& ctx, Level& L, int32_t* status) {
@@ -724,6 +857,7 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     int np = b.npieces;
     Level& F = b.levels[l];
     int64_t n = F.n;
+    PhaseTimer pt(ctx);
     // which pieces go on: more than FEW parts (bodies.rs:447)
     std::vector<int32_t> active(np, 0);
     for (int p = 0; p < np; p++) active[p] = (F.pstart[p + 1] - F.pstart[p]) > opt.few ? 1 : 0;
@@ -784,6 +918,7 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     label.release();
     root.release();
     id.release();
+    pt.mark("  bodies");
 
     Level C;
     C.n = nc;
@@ -830,6 +965,7 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     k_rvec<<<grid_for(n, 256), 256, 0, st>>>(n, F.up.get(), F.centre.get(), C.centre.get(), rvec.get());
     SC_LAUNCH_CK();
     bool keep_mf = l == 0 && F.matrix_free;
+    pt.mark("  members, centroids");
 
     // --- P pattern and values
     DBuf<int64_t> cnt, off;
@@ -843,15 +979,25 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     {
         DBuf<uint64_t> keys;
         keys.alloc(std::max<int64_t>(tot, 1), st, ms);
-        k_fill_P<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.up.get(), off.get(), keys.get());
+        k_fill_P<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.up.get(), off.get(), keys.get(),
+                                                   bits_for(nc));
         SC_LAUNCH_CK();
         keys_to_csr(ctx, keys, tot, n, nc, F.prow, F.pcol, F.pnnz);
     }
+    cnt.release();
+    off.release();
     F.pval.alloc(36 * std::max<int64_t>(F.pnnz, 1), st, ms);
     F.pval.zero();
-    k_num_P<<<grid_for(n * 32, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.val.get(), F.up.get(),
-                                                   rvec.get(), F.inv.get(), F.step.get(), F.piece.get(), F.prow.get(),
-                                                   F.pcol.get(), F.pval.get());
+    const K0View k0 = k0_view(b, F);
+    const bool virt = k0.desc != nullptr;  // level-0 blocks made from the cell template
+    if (virt)
+        k_num_P<true><<<grid_for(n * 32, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), nullptr, k0, F.up.get(),
+                                                             rvec.get(), F.inv.get(), F.step.get(), F.piece.get(),
+                                                             F.prow.get(), F.pcol.get(), F.pval.get());
+    else
+        k_num_P<false><<<grid_for(n * 32, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.val.get(), k0,
+                                                              F.up.get(), rvec.get(), F.inv.get(), F.step.get(),
+                                                              F.piece.get(), F.prow.get(), F.pcol.get(), F.pval.get());
     SC_LAUNCH_CK();
     if (keep_mf) {
         F.mf_r = std::move(rvec);
@@ -863,11 +1009,11 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         mem_part.release();
     }
     // P transposed: entries sorted by column, stable (fine-row order within a column)
+    DBuf<int32_t> prow_of;  // the row of each P entry
+    prow_of.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
+    k_row_of_entry<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), prow_of.get());
+    SC_LAUNCH_CK();
     {
-        DBuf<int32_t> prow_of;
-        prow_of.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
-        k_row_of_entry<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), prow_of.get());
-        SC_LAUNCH_CK();
         DBuf<int64_t> ent;
         ent.alloc(std::max<int64_t>(F.pnnz, 1), st, ms);
         k_iota64<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, ent.get());
@@ -894,31 +1040,56 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
                                                                        F.ptval.get());
         SC_LAUNCH_CK();
     }
+    pt.mark("  prolongator");
     // --- K P
     DBuf<int64_t> kprow;
     DBuf<int32_t> kpcol;
-    int64_t kpnnz = 0;
-    k_count_KP<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.prow.get(), F.up.get(), cnt.get());
-    SC_LAUNCH_CK();
-    exclusive_scan(ctx, cnt.get(), off.get(), n + 1);
-    tot = d2h_i64(ctx, off.get() + n);
+    int64_t kpnnz = 0, kp_cands = 0, c_cands = 0;
     DBuf<double> kpval;
     {
+        // one thread per block of K (its row from krow), offsets by a scan over K's entries
+        const int64_t knz = F.nnzb;
+        DBuf<int32_t> krow;
+        DBuf<int64_t> kcnt, koff;
+        krow.alloc(std::max<int64_t>(knz, 1), st, ms);
+        kcnt.alloc(knz + 1, st, ms);
+        koff.alloc(knz + 1, st, ms);
+        k_row_of_entry<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), krow.get());
+        SC_LAUNCH_CK();
+        SC_CK(cudaMemsetAsync(kcnt.get() + knz, 0, sizeof(int64_t), st));
+        if (knz > 0) {
+            k_count_KP<<<grid_for(knz, 256), 256, 0, st>>>(knz, krow.get(), F.col.get(), F.prow.get(), F.up.get(),
+                                                          kcnt.get());
+            SC_LAUNCH_CK();
+        }
+        exclusive_scan(ctx, kcnt.get(), koff.get(), knz + 1);
+        tot = d2h_i64(ctx, koff.get() + knz);
+        kp_cands = tot;
+        kcnt.release();
         DBuf<uint64_t> keys, vin, vals;
         DBuf<int64_t> seg;
         keys.alloc(std::max<int64_t>(tot, 1), st, ms);
         vin.alloc(std::max<int64_t>(tot, 1), st, ms);
-        k_fill_KP<<<grid_for(n, 256), 256, 0, st>>>(n, F.rowptr.get(), F.col.get(), F.prow.get(), F.pcol.get(),
-                                                    F.up.get(), off.get(), keys.get(), vin.get());
-        SC_LAUNCH_CK();
-        keys_to_csr_with(ctx, keys, vin, tot, n, kprow, kpcol, kpnnz, seg, vals);
+        if (knz > 0) {
+            k_fill_KP<<<grid_for(knz, 256), 256, 0, st>>>(knz, krow.get(), F.col.get(), F.prow.get(), F.pcol.get(),
+                                                         F.up.get(), koff.get(), keys.get(), vin.get(), bits_for(nc));
+            SC_LAUNCH_CK();
+        }
+        koff.release();
+        keys_to_csr_with(ctx, keys, vin, tot, n, nc, kprow, kpcol, kpnnz, seg, vals);
         kpval.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
         if (kpnnz > 0) {
-            k_sum_products<false><<<(unsigned)((kpnnz + SUM_GROUPS - 1) / SUM_GROUPS), 36 * SUM_GROUPS, 0, st>>>(
-                kpnnz, seg.get(), vals.get(), F.val.get(), F.pval.get(), kpval.get());
+            unsigned nb = (unsigned)((kpnnz + SUM_GROUPS - 1) / SUM_GROUPS);
+            if (virt)
+                k_sum_products<false, true><<<std::min(nb, 148u * 8u), SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(), nullptr,
+                                                                            F.pval.get(), kpval.get(), k0, krow.get());
+            else
+                k_sum_products<false, false><<<nb, SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(), F.val.get(),
+                                                                             F.pval.get(), kpval.get(), k0, nullptr);
             SC_LAUNCH_CK();
         }
     }
+    pt.mark("  K P");
     // --- P' K P, upper triangle (d >= c)
     DBuf<int64_t> urow;
     DBuf<int32_t> ucol;
@@ -929,28 +1100,40 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         ecnt.alloc(F.pnnz + 1, st, ms);
         eoff.alloc(F.pnnz + 1, st, ms);
         SC_CK(cudaMemsetAsync(ecnt.get() + F.pnnz, 0, sizeof(int64_t), st));
-        k_count_C<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), F.pcol.get(), kprow.get(), kpcol.get(), ecnt.get());
-        SC_LAUNCH_CK();
+        if (F.pnnz > 0) {
+            k_count_C<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, prow_of.get(), F.pcol.get(), kprow.get(),
+                                                             kpcol.get(), ecnt.get());
+            SC_LAUNCH_CK();
+        }
         exclusive_scan(ctx, ecnt.get(), eoff.get(), F.pnnz + 1);
         tot = d2h_i64(ctx, eoff.get() + F.pnnz);
+        c_cands = tot;
         DBuf<uint64_t> keys, vin, vals;
         DBuf<int64_t> seg;
         keys.alloc(std::max<int64_t>(tot, 1), st, ms);
         vin.alloc(std::max<int64_t>(tot, 1), st, ms);
-        k_fill_C<<<grid_for(n, 256), 256, 0, st>>>(n, F.prow.get(), F.pcol.get(), kprow.get(), kpcol.get(), eoff.get(),
-                                                   keys.get(), vin.get());
-        SC_LAUNCH_CK();
-        keys_to_csr_with(ctx, keys, vin, tot, nc, urow, ucol, unnz, seg, vals);
+        if (F.pnnz > 0) {
+            k_fill_C<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, prow_of.get(), F.pcol.get(), kprow.get(),
+                                                            kpcol.get(), eoff.get(), keys.get(), vin.get(),
+                                                            bits_for(nc));
+            SC_LAUNCH_CK();
+        }
+        keys_to_csr_with(ctx, keys, vin, tot, nc, nc, urow, ucol, unnz, seg, vals);
         uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
         if (unnz > 0) {
-            k_sum_products<true><<<(unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS), 36 * SUM_GROUPS, 0, st>>>(
-                unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get());
+            k_sum_products<true, false><<<(unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS), SUM_THREADS, 0, st>>>(
+                unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get(), K0View{}, nullptr);
             SC_LAUNCH_CK();
         }
     }
     kpval.release();
     kprow.release();
     kpcol.release();
+    prow_of.release();
+    pt.mark("  P' K P");
+    pt.note("  sizes: rows %lld blocks %lld P %lld KP cands %lld KP %lld C cands %lld C upper %lld", (long long)n,
+            (long long)F.nnzb, (long long)F.pnnz, (long long)kp_cands, (long long)kpnnz, (long long)c_cands,
+            (long long)unnz);
     // --- full symmetric storage
     {
         DBuf<int32_t> urows;
@@ -984,7 +1167,7 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         C.col.alloc(fn, st, ms);
         DBuf<int32_t> rows;
         rows.alloc(fn, st, ms);
-        k_unpack_pattern<<<grid_for(fn, 256), 256, 0, st>>>(fn, keys_s.get(), C.col.get(), rows.get());
+        k_unpack_pattern<<<grid_for(fn, 256), 256, 0, st>>>(fn, keys_s.get(), C.col.get(), rows.get(), 32);
         SC_LAUNCH_CK();
         C.rowptr.alloc(nc + 1, st, ms);
         k_offsets_from_sorted<<<grid_for(fn + 1, 256), 256, 0, st>>>(fn, rows.get(), nc, C.rowptr.get());
@@ -993,6 +1176,7 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         k_mirror_vals<<<grid_for(36 * fn, 256), 256, 0, st>>>(fn, src_s.get(), uval.get(), C.val.get());
         SC_LAUNCH_CK();
     }
+    pt.mark("  mirror");
     b.levels.push_back(std::move(C));
     return true;
 }
@@ -1014,22 +1198,27 @@ static void build_top(Context& ctx, Batch& b, int l, const std::vector<int32_t>&
     L.kinv_off.alloc(off.size(), st, &ctx.mem);
     L.kinv_off.upload(off.data(), off.size());
     L.kinv.alloc(std::max<int64_t>(off.back(), 1), st, &ctx.mem);
-    int64_t maxnn = 1;
-    for (size_t i = 0; i < pieces.size(); i++) maxnn = std::max(maxnn, off[i + 1] - off[i]);
-    DBuf<double> A, X;
-    A.alloc(maxnn, st, &ctx.mem);
-    X.alloc(maxnn, st, &ctx.mem);
-    for (size_t i = 0; i < pieces.size(); i++) {
-        int64_t nn = off[i + 1] - off[i];
-        int n = (int)(6 * (L.pstart[pieces[i] + 1] - L.pstart[pieces[i]]));
-        if (n == 0) continue;
-        SC_CK(cudaMemsetAsync(A.get(), 0, nn * sizeof(double), st));
-        k_dense_from_bsr<<<64, 64, 0, st>>>((int)i, L.top.get(), L.pstart_d.get(), L.rowptr.get(), L.col.get(),
-                                             L.val.get(), A.get());
-        SC_LAUNCH_CK();
-        k_cholesky_inverse<<<1, 1024, 0, st>>>(n, A.get(), X.get(), L.kinv.get() + off[i], b.status_d.get(), pieces[i]);
+    // all tops factored together, one block per piece, the inverse written in place
+    SC_CK(cudaMemsetAsync(L.kinv.get(), 0, std::max<int64_t>(off.back(), 1) * sizeof(double), st));
+    DBuf<double> X;
+    X.alloc(std::max<int64_t>(off.back(), 1), st, &ctx.mem);
+    unsigned nt = (unsigned)pieces.size();
+    for (unsigned first = 0; first < nt; first += 65535u) {  // gridDim.y <= 65535
+        unsigned m = std::min(nt - first, 65535u);
+        const K0View k0 = k0_view(b, L);
+        if (k0.desc)
+            k_dense_from_bsr_all<true><<<dim3(64, m), 64, 0, st>>>(L.top.get() + first, L.pstart_d.get(),
+                                                                   L.rowptr.get(), L.col.get(), nullptr, k0,
+                                                                   L.kinv_off.get() + first, L.kinv.get());
+        else
+            k_dense_from_bsr_all<false><<<dim3(64, m), 64, 0, st>>>(L.top.get() + first, L.pstart_d.get(),
+                                                                    L.rowptr.get(), L.col.get(), L.val.get(), k0,
+                                                                    L.kinv_off.get() + first, L.kinv.get());
         SC_LAUNCH_CK();
     }
+    k_cholesky_inverse_all<<<nt, 1024, 0, st>>>(L.top.get(), L.pstart_d.get(), L.kinv_off.get(), L.kinv.get(),
+                                                 X.get(), b.status_d.get());
+    SC_LAUNCH_CK();
 }
 
 template <class T>
@@ -1055,6 +1244,7 @@ void to_float(Context& ctx, const DBuf<double>& a, DBuf<float>& b) {
 // than its parts, coarsen it (bodies.rs:444-461); then factor each piece's top.
 void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
     auto t0 = std::chrono::steady_clock::now();
+    PhaseTimer pt(ctx);
     int np = b.npieces;
     b.levels.reserve(SC_MAX_LEVELS + 1);
     b.status_d.alloc(np, ctx.stream, &ctx.mem);
@@ -1063,10 +1253,16 @@ void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
     for (int l = 0;; l++) {
         Level& L = b.levels[l];
         setup_chunks(ctx, L, np);
-        invert_blocks(ctx, L, b.status_d.get());
+        if (L.matrix_free && L.desc.size())
+            invert_blocks_k0(ctx, b, L, b.status_d.get());
+        else
+            invert_blocks(ctx, L, b.status_d.get());
+        pt.mark("chunks + inverses");
         smoother_step(ctx, b, l);
+        pt.mark("smoother step");
         octree += 1;
         bool more = l + 1 < SC_MAX_LEVELS && coarsen(ctx, b, l, octree, opt);
+        pt.mark("coarsen");
         Level& F = b.levels[l];  // reference may have moved
         // pieces whose top is this level
         std::vector<int32_t> tops;
@@ -1080,6 +1276,7 @@ void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
             }
         }
         build_top(ctx, b, l, tops);
+        pt.mark("tops");
         if (!more) break;
     }
     // a matrix-free level 0 keeps only what the solve reads: the assembled blocks, their
@@ -1087,6 +1284,8 @@ void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
     if (b.levels[0].matrix_free && b.levels.size() > 1) {
         Level& L0 = b.levels[0];
         L0.val.release();
+        L0.desc.release();
+        b.grid.tpl_s.release();
         L0.col.release();
         L0.rowptr.release();
         L0.inv.release();
@@ -1097,6 +1296,7 @@ void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
         L0.tent.release();
         L0.trow.release();
     }
+    pt.mark("release level 0");
     b.piece_levels.assign(np, 0);
     for (size_t l = 0; l < b.levels.size(); l++)
         for (int p = 0; p < np; p++)

@@ -10,6 +10,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <memory>
 #include <vector>
 
@@ -26,7 +27,7 @@ struct Grid0 {
     DBuf<int4> cell;            // 2 int4 per free cell: part ids of slots 0..5 (-1 held), k bits, 0
     DBuf<int32_t> perm;         // parts in order, grouped by axis inside tiles of 1024 parts
     DBuf<int4> slots;           // per perm slot: part, lesser cell, greater cell, axis
-    bool pencil = true;         // the plane-pencil stencil (tile 0) or the per-slot one
+    bool pencil = false;        // the plane-pencil stencil (tile 1) or the per-slot one
     DBuf<int32_t> gridmap;      // per grid cell: its free-cell index or -1
     DBuf<uint8_t> tiles;        // pencil tiles (piece, x0, y0, z0)
     DBuf<uint8_t> geo;          // per piece: dims and first flat cell
@@ -35,6 +36,7 @@ struct Grid0 {
     DBuf<int32_t> cella, cellb; // per part: its lesser cell (node is that cell's + face) and greater cell; -1 if not free
     DBuf<int8_t> axis;          // per part
     DBuf<int64_t> cell_flat;    // per free cell: its flat index in the batch's concatenated grids
+    DBuf<double> tpl_s;         // the cell template at spacing s, 36 x 36 (setup only)
     std::vector<int64_t> grid_off;  // per piece: first flat cell index; npieces + 1
 };
 
@@ -50,8 +52,10 @@ struct Level {
     bool matrix_free = false;        // level 0 of voxel pieces: apply through Grid0
     DBuf<int64_t> rowptr;
     DBuf<int32_t> col;
-    DBuf<double> val;
+    DBuf<double> val;                // 36 per stored block; empty on a matrix-free level 0
     DBuf<float> val32;
+    DBuf<uint8_t> desc;              // matrix-free level 0, setup only: each stored block's
+                                     // origin in the cell template (level0_blocks.cuh)
     DBuf<double> inv;                // inverse of each part's own block
     DBuf<float> inv32;
     DBuf<double> step;               // per piece: 4/3 / lambda_max(D^-1 K)
@@ -150,6 +154,7 @@ struct SolveStats {
 };
 void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st);
 void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st);
+void pcg_fp32_cycle(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st);
 template <class T>
 void level_apply(Context& ctx, const Batch& b, int l, const T* x, T* y);
 void seg_dot(Context& ctx, const Level& L, const double* a, const double* bb, double* out_per_piece);
@@ -198,6 +203,20 @@ struct Context {
     std::unique_ptr<Batch> last;     // the last solve's hierarchy (parity queries)
     void* cub_scratch(size_t bytes);
     ~Context();
+};
+
+// Wall-clock phases of a setup: with SC_TIMING=1 in the environment, mark() waits for
+// the stream and prints the milliseconds since the previous mark to stderr; otherwise
+// it does nothing.
+struct PhaseTimer {
+    Context& ctx;
+    bool on;
+    std::chrono::steady_clock::time_point t;
+    double alloc_ms0 = 0;
+    int64_t allocs0 = 0;
+    explicit PhaseTimer(Context& c);
+    void mark(const char* phase);
+    void note(const char* fmt, ...);  // a line of its own (when on)
 };
 
 }  // namespace sc

@@ -27,7 +27,7 @@ LIB_PATH = os.path.join(HERE, "libstatics_cuda.so")
 OK, MAXITER, BREAKDOWN, NOT_SPD, BAD_INPUT, TIMEOUT, CUDA, NO_DEVICE = range(8)
 CELL_EMPTY, CELL_FREE, CELL_HELD = 0, 1, 2
 K_UNIFORM, K_LOGNORMAL = 0, 1
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_FP32_KRYLOV = 0, 1, 2
 MAX_LEVELS = 24
 (FAM_STENCIL64, FAM_STENCIL32, FAM_SPMV64, FAM_SPMV32, FAM_TRANSFER64, FAM_TRANSFER32, FAM_SMOOTH64,
  FAM_SMOOTH32, FAM_TOP) = range(9)

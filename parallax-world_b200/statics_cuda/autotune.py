@@ -1,12 +1,17 @@
 """Autotuner for batched solves of voxel pieces.
 
 Pieces are put in size classes (their grid cells rounded up to a power of two). For
-each class it times one representative piece's full solve (setup + PCG to the
-requested tolerance) under every candidate setting -- block-Jacobi sweeps before and
+each class it times the full solves (setup + PCG to the requested tolerance) of up to
+SAMPLES of its pieces under every candidate setting -- block-Jacobi sweeps before and
 after each coarse correction (the reference does one, statics/src/bodies.rs:386,
 396-401) and the stencil tile (the window of parts grouped by axis) -- and keeps the
-fastest. Choices are cached in a JSON file keyed by class, precision and tolerance, so
-a later batch of the same classes is not tuned again.
+fastest setting that solved every sample. Two sweeps per level make a stronger
+preconditioner, but the damped-Jacobi step 4/(3 lambda_max) is the reference's choice
+for one sweep; on some pieces two sweeps lose definiteness and CG stalls, so a setting
+counts only if all its samples converge within TRIAL_MAX_ITER iterations. Choices are
+cached in a JSON file keyed by class, precision and tolerance, so a later batch of the
+same classes is not tuned again. A piece that still fails in the batched solve is
+solved again alone with the reference's one sweep (its info then says retried).
 """
 from __future__ import annotations
 
@@ -16,8 +21,12 @@ import time
 
 from . import FP64, MIXED, Solver, options
 
-SWEEPS = (1, 2, 3)
+SWEEPS = (1, 2)
 TILES = (256, 1024, 4096)
+SAMPLES = 3
+TRIAL_MAX_ITER = 2000
+MAX_ITER = 20000
+FALLBACK = {"sweeps": 1, "tile": 0}
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_cache.json")
 
 
@@ -48,38 +57,49 @@ def save(cache: dict, path: str = DEFAULT_CACHE) -> None:
     os.replace(tmp, path)
 
 
-def tune_class(solver: Solver, piece, precision: int = MIXED, tol: float = 1e-8, repeats: int = 2) -> dict:
-    """Times every (sweeps, tile) on one piece; returns the fastest with its timings."""
-    state, k = piece
+def tune_class(solver: Solver, samples, precision: int = MIXED, tol: float = 1e-8, repeats: int = 2) -> dict:
+    """Times every (sweeps, tile) on the sample pieces; returns the fastest setting that
+    solved all of them, with the timings (the reference's setting if none did)."""
     trials = []
     for sweeps in SWEEPS:
         for tile in TILES:
-            opt = options(tol=tol, precision=precision, sweeps=sweeps, tile=tile, max_iter=20000)
-            best = None
-            for _ in range(repeats):
-                t = time.perf_counter()
-                _, info = solver.solve_grid(state, k, opt)
-                dt = time.perf_counter() - t
-                if info["status"] != 0:
-                    dt = float("inf")
-                best = dt if best is None else min(best, dt)
-            trials.append({"sweeps": sweeps, "tile": tile, "seconds": best, "iterations": info["iterations"]})
-    win = min(trials, key=lambda t: t["seconds"])
+            opt = options(tol=tol, precision=precision, sweeps=sweeps, tile=tile, max_iter=TRIAL_MAX_ITER)
+            total, iters = 0.0, []
+            for state, k in samples:
+                best = None
+                for _ in range(repeats):
+                    t = time.perf_counter()
+                    _, info = solver.solve_grid(state, k, opt)
+                    dt = time.perf_counter() - t
+                    if info["status"] != 0 or not info["residual"] <= tol * 1.0001:
+                        dt = float("inf")
+                    best = dt if best is None else min(best, dt)
+                    if dt == float("inf"):
+                        break
+                total += best
+                iters.append(info["iterations"])
+                if total == float("inf"):
+                    break
+            trials.append({"sweeps": sweeps, "tile": tile, "seconds": total, "iterations": iters})
+    ok = [t for t in trials if t["seconds"] < float("inf")]
+    if not ok:
+        return dict(FALLBACK, seconds=None, trials=trials)
+    win = min(ok, key=lambda t: t["seconds"])
     return {"sweeps": win["sweeps"], "tile": win["tile"], "seconds": win["seconds"], "trials": trials}
 
 
 def choose(solver: Solver, pieces, precision: int = MIXED, tol: float = 1e-8, path: str = DEFAULT_CACHE) -> dict:
     """The setting for each size class present in `pieces` (tuning the classes the cache
-    lacks). Returns {class: {"sweeps": s, "tile": t, ...}}."""
+    lacks on up to SAMPLES of their pieces). Returns {class: {"sweeps": s, "tile": t, ...}}."""
     cache = load(path)
-    out, changed = {}, False
+    classes: dict[int, list] = {}
     for piece in pieces:
-        cls = size_class(piece[0])
-        if cls in out:
-            continue
+        classes.setdefault(size_class(piece[0]), []).append(piece)
+    out, changed = {}, False
+    for cls, members in classes.items():
         key = _key(cls, precision, tol)
         if key not in cache:
-            cache[key] = tune_class(solver, piece, precision, tol)
+            cache[key] = tune_class(solver, members[:SAMPLES], precision, tol)
             changed = True
         out[cls] = cache[key]
     if changed:
@@ -90,16 +110,23 @@ def choose(solver: Solver, pieces, precision: int = MIXED, tol: float = 1e-8, pa
 def solve_batch(solver: Solver, pieces, precision: int = MIXED, tol: float = 1e-8, path: str = DEFAULT_CACHE,
                 settings: dict | None = None):
     """Solves `pieces` grouped by size class, each group one batched solve with its
-    tuned setting. Returns (motions, infos) in the order of `pieces`."""
+    tuned setting; a piece that did not converge is solved again alone with the
+    reference's setting. Returns (motions, infos) in the order of `pieces`."""
     settings = settings or choose(solver, pieces, precision, tol, path)
     groups: dict[int, list[int]] = {}
     for i, p in enumerate(pieces):
         groups.setdefault(size_class(p[0]), []).append(i)
     motions, infos = [None] * len(pieces), [None] * len(pieces)
     for cls, idx in groups.items():
-        s = settings[cls]
-        opt = options(tol=tol, precision=precision, sweeps=s["sweeps"], tile=s["tile"], max_iter=20000)
+        s = settings.get(cls, FALLBACK)
+        opt = options(tol=tol, precision=precision, sweeps=s["sweeps"], tile=s["tile"], max_iter=MAX_ITER)
         outs, inf = solver.solve_grid_batch([pieces[i] for i in idx], opt)
         for j, i in enumerate(idx):
             motions[i], infos[i] = outs[j], inf[j]
+    fallback = options(tol=tol, precision=precision, sweeps=FALLBACK["sweeps"], tile=FALLBACK["tile"],
+                       max_iter=MAX_ITER)
+    for i, info in enumerate(infos):
+        if info["status"] != 0 or not info["residual"] <= tol * 1.0001:
+            motions[i], infos[i] = solver.solve_grid(*pieces[i], fallback)
+            infos[i]["retried"] = True
     return motions, infos

@@ -98,17 +98,40 @@ def test_motions_special_pieces(solver, name, st, k):
 
 
 def test_mixed_precision_against_fp64(solver):
+    """SC_MIXED (FP64 CG, FP32 V-cycle) and SC_MIXED_FP32_KRYLOV (FP32 CG with FP64
+    residual replacement) both reach the tolerance on the FP64 true residual and the
+    oracle's FP64 motions; the FP32 V-cycle leaves the iteration count near FP64's."""
     st, k = piece(32, 1)
     lat = oracle_lattice(st, k)
     loads, ex = z_loads(lat)
     u_ref, _ = lat.motions(loads, tol=1e-12)
     u64, i64 = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8))
+    assert rel(u64, u_ref) < DISP_TOL
     u32, i32 = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8, precision=sc.MIXED))
     assert i32["status"] == sc.OK
     assert i32["residual"] <= 1e-8 * 1.0001
-    assert i32["refinements"] >= 1
-    assert rel(u64, u_ref) < DISP_TOL
+    assert i32["iterations"] <= 1.5 * i64["iterations"] + 2
     assert rel(u32, u_ref) < DISP_TOL
+    uk, ik = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8, precision=sc.MIXED_FP32_KRYLOV))
+    assert ik["status"] == sc.OK
+    assert ik["residual"] <= 1e-8 * 1.0001
+    assert ik["refinements"] >= 1
+    assert rel(uk, u_ref) < DISP_TOL
+
+
+def test_mixed_precision_hard_piece(solver):
+    """A 16 x 16 x 24 piece on which the all-FP32 Krylov recurrence breaks down: the
+    FP32 V-cycle inside FP64 CG converges like FP64."""
+    st, k = sc.generate_piece(16, 16, 24, 10_017, sc.K_UNIFORM)
+    _, i64 = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8))
+    u, info = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8, precision=sc.MIXED))
+    assert info["status"] == sc.OK
+    assert info["residual"] <= 1e-8 * 1.0001
+    assert info["iterations"] <= i64["iterations"] + 5
+    lat = oracle_lattice(st, k)
+    loads, _ = z_loads(lat)
+    u_ref, _ = lat.motions(loads, tol=1e-12)
+    assert rel(u, u_ref) < DISP_TOL
 
 
 def test_golden_large(solver):
@@ -152,6 +175,58 @@ def test_batch_mixed(solver):
         loads, _ = z_loads(lat)
         u_ref, _ = lat.motions(loads, tol=1e-12)
         assert info["residual"] <= 1e-8 * 1.0001
+        assert rel(u, u_ref) < DISP_TOL
+
+
+@pytest.mark.parametrize("tile", [1, 32, 4096])
+@pytest.mark.parametrize("precision", [sc.FP64, sc.MIXED], ids=["fp64", "mixed"])
+def test_stencil_variants(solver, tile, precision):
+    """The level-0 stencils sc_options.tile selects (1: the plane-pencil stencil; a power
+    of two: the per-part stencil's axis-grouping window) apply the same operator: the
+    same hierarchy and iterations as the default, motions within the displacement bar of
+    the oracle's. The shape is ragged against the pencil's 16 x 8 x 32 blocks."""
+    st, k = piece(0, 41, shape=(37, 21, 45))
+    lat = oracle_lattice(st, k)
+    loads, _ = z_loads(lat)
+    u_ref, _ = lat.motions(loads, tol=1e-12)
+    u0, i0 = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8, precision=precision))
+    u, info = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8, precision=precision, tile=tile))
+    assert info["status"] == sc.OK
+    assert info["parts"] == i0["parts"]
+    assert abs(info["iterations"] - i0["iterations"]) <= 1
+    assert rel(u, u_ref) < DISP_TOL
+    if precision == sc.FP64:
+        x = np.random.default_rng(2).standard_normal((sc.grid_count(st)[1], 6))
+        assert rel(solver.grid_apply(st, k, x), lat.level0_apply(x)) < OP_TOL64
+
+
+@pytest.mark.parametrize("sweeps", [2, 3])
+def test_more_sweeps(solver, sweeps):
+    """Several block-Jacobi sweeps before and after each coarse correction (the
+    reference does one): a different preconditioner, the same solution."""
+    st, k = piece(32, 2)
+    lat = oracle_lattice(st, k)
+    loads, _ = z_loads(lat)
+    u_ref, _ = lat.motions(loads, tol=1e-12)
+    u, info = solver.solve_grid(st, k, sc.options(max_iter=5000, tol=1e-8, sweeps=sweeps))
+    if info["status"] == sc.OK:
+        assert rel(u, u_ref) < DISP_TOL
+    else:  # more sweeps of the reference's damping can lose definiteness; it must say so
+        assert info["status"] in (sc.MAXITER, sc.BREAKDOWN)
+
+
+def test_autotuned_batch(solver, tmp_path):
+    """The autotuner's batched solve: every piece converges (a failed group member is
+    solved again with the reference's setting) and matches the oracle."""
+    from statics_cuda import autotune
+    pieces = [piece(0, 300 + i, shape=(16 + 8 * (i % 2), 16, 24 - 8 * (i % 3 == 0))) for i in range(6)]
+    outs, infos = autotune.solve_batch(solver, pieces, sc.MIXED, 1e-8, path=str(tmp_path / "cache.json"))
+    for (st, k), u, info in zip(pieces, outs, infos):
+        assert info["status"] == sc.OK
+        assert info["residual"] <= 1e-8 * 1.0001
+        lat = oracle_lattice(st, k)
+        loads, _ = z_loads(lat)
+        u_ref, _ = lat.motions(loads, tol=1e-12)
         assert rel(u, u_ref) < DISP_TOL
 
 
