@@ -459,14 +459,15 @@ def batch_section(solver, sc, rank, world, args):
     single = world * len(sample) / (ms_1 / 1000.0)
     bad = sum(1 for i in infos if i["status"] != 0 or i["residual"] > TOL * 1.0001)
     retried = sum(1 for i in infos if i.get("retried"))
-    groups = len({autotune.size_class(p[0]) for p in pieces})
+    groups = len({(settings[autotune.size_class(p[0])]["sweeps"], settings[autotune.size_class(p[0])]["tile"])
+                  for p in pieces})
     return {"workload": f"{len(pieces)} pieces per rank, edges from {list(EDGES)} per axis, seeds 10000+; "
                         f"value noise period 8 thr 0.5, k U[0.5,2], tol {TOL:g}",
             "pieces": len(pieces), "dof": dof, "mixed_batched_solves_per_s": batched,
             "fp64_single_solves_per_s": single, "fp64_single_sample": len(sample),
             "speedup_batched_mixed_vs_fp64_single": batched / single,
             "mixed_batched_ms": ms_b, "iterations_mean": float(np.mean([i["iterations"] for i in infos])),
-            "pieces_not_converged": bad, "pieces_retried": retried, "size_classes": groups, "autotune": {str(k): {"sweeps": v["sweeps"], "tile": v["tile"]}
+            "pieces_not_converged": bad, "pieces_retried": retried, "batched_solves": groups, "autotune": {str(k): {"sweeps": v["sweeps"], "tile": v["tile"]}
                                                        for k, v in settings.items()},
             "autotune_seconds": tune_s}
 

@@ -124,6 +124,11 @@ void* Context::cub_scratch(size_t bytes) {
     return cub_tmp;
 }
 
+int32_t* Context::pinned_i32() {
+    if (!pinned) SC_CK(cudaMallocHost((void**)&pinned, 16));
+    return pinned;
+}
+
 Context::~Context() {
     last.reset();
     partial.release();
@@ -134,6 +139,7 @@ Context::~Context() {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
     }
+    if (pinned) cudaFreeHost(pinned);
 }
 
 namespace {
@@ -252,6 +258,7 @@ void read_steps(Context& ctx, const Batch& b, int piece, sc_solve_info* info) {
 sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st, double& solve_ms) {
     b.sweeps = opt.sweeps;
     build_hierarchy(ctx, b, opt);
+    PhaseTimer pt(ctx);
     auto t0 = std::chrono::steady_clock::now();
     if (opt.precision == SC_MIXED)
         pcg_fp32_cycle(ctx, b, opt, x, st);
@@ -261,6 +268,7 @@ sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double
         pcg_fp64(ctx, b, opt, x, st);
     SC_CK(cudaStreamSynchronize(ctx.stream));
     solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    pt.mark("conjugate gradients");
     b.piece_status = b.status_d.to_host();
     int worst = 0;
     for (int s : b.piece_status) worst = std::max(worst, s);
@@ -319,6 +327,10 @@ sc_status sc_create(int32_t device, sc_context** out) {
         SC_CK(cudaDeviceGetDefaultMemPool(&pool, device));
         uint64_t thr = UINT64_MAX;
         SC_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+        size_t free_b = 0, total_b = 0;
+        SC_CK(cudaSetDevice(device));
+        SC_CK(cudaMemGetInfo(&free_b, &total_b));
+        ctx->c.mem.cap = total_b / 2;
     });
     if (s != SC_OK) {
         delete ctx;

@@ -47,15 +47,17 @@ inline void require(bool ok, sc_status s, const std::string& msg) {
 // as cudaFreeAsync / cudaMallocAsync would, but without calling the driver, whose
 // allocation calls were measured at milliseconds each: repeated solves of similar sizes
 // then allocate nothing. Requests are rounded up to size classes (1/8 steps of their
-// power of two, at least 512 bytes) so that similar sizes share blocks, and the cache
-// keeps at most twice the largest amount ever held at once; beyond that a released block
-// goes back to the pool.
+// power of two, at least 512 bytes) so that similar sizes share blocks. Like a caching
+// allocator, the cache keeps what it is given up to `cap` bytes (half the device's memory
+// by default); when the pool runs out, an allocation gives the cached blocks back and
+// tries again.
 struct MemStats {
     int64_t now = 0, peak = 0, top = 0;
     double alloc_ms = 0;
     int64_t allocs = 0;
     std::multimap<size_t, void*> cache;  // block bytes -> block
     size_t cached = 0;
+    size_t cap = size_t(64) << 30;
     void add(int64_t b) {
         now += b;
         if (now > peak) peak = now;
@@ -77,7 +79,7 @@ struct MemStats {
         return p;
     }
     bool give(void* p, size_t bytes) {
-        if (cached + bytes > 2 * (size_t)top) return false;
+        if (cached + bytes > cap) return false;
         cache.emplace(bytes, p);
         cached += bytes;
         return true;

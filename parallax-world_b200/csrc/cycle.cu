@@ -4,6 +4,7 @@
 // FP64 iterative refinement.
 #include <chrono>
 
+#include <cstdlib>
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -278,6 +279,16 @@ __global__ void k_cg_beta_flex(int np, CgScalars s, const double* __restrict__ z
     s.iters[p] += 1;
 }
 
+// The condition of the device-side iteration loop: go on while a piece is not done and
+// fewer than `chunk` iterations ran since the launch (count is zeroed before each launch;
+// any value it holds ends the loop within chunk + 1 iterations).
+__global__ void k_loop_more(cudaGraphConditionalHandle h, const int32_t* __restrict__ ndone, int np,
+                            uint32_t* __restrict__ count, uint32_t chunk) {
+    uint32_t c = *count + 1u;
+    *count = c;
+    cudaGraphSetConditional(h, (*ndone < np && c < chunk) ? 1u : 0u);
+}
+
 // b = a in another precision for the pieces not done, one block per chunk
 template <class A, class B>
 __global__ void __launch_bounds__(256) k_cast_chunks(const int64_t* __restrict__ chunk_lo,
@@ -383,6 +394,7 @@ struct CgState {
     DBuf<int32_t> flags;
     DBuf<int64_t> iters;
     DBuf<int32_t> ndone;
+    DBuf<uint32_t> loop_count;  // iterations since the device-side loop's launch
     CgScalars s{};
     double* beta = nullptr;
     double* zap = nullptr;  // (z, Ap) for the Polak-Ribiere beta
@@ -396,6 +408,7 @@ struct CgState {
         iters.alloc(np, ctx.stream, &ctx.mem);
         iters.zero();
         ndone.alloc(1, ctx.stream, &ctx.mem);
+        loop_count.alloc(1, ctx.stream, &ctx.mem);
         double* q = scal.get();
         s.bb = q;
         s.goal = q + np;
@@ -441,11 +454,60 @@ static void dot2(Context& ctx, const Level& L, const int32_t* done, const T* a, 
     SC_LAUNCH_CK();
 }
 
+// CUDA graphs replay the CG iterations unless the environment sets SC_NO_GRAPHS=1 (for
+// kernel profilers, which then see every launch on its own) or kernels are being timed.
+static bool graphs_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("SC_NO_GRAPHS");
+        return !(e && e[0] == '1');
+    }();
+    return on;
+}
+
+// A graph of one conditional WHILE node whose body is what `fill` launches on `st`
+// (captured), instantiated; null where the driver offers no conditional nodes (the
+// caller then replays a plain graph from the host). The body must end by setting the
+// condition through ctx.loop_handle, which this creates.
+template <class F>
+static cudaGraphExec_t capture_loop(cudaStream_t st, F&& fill, Context& ctx) {
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNodeParams prm = {};
+    prm.type = cudaGraphNodeTypeConditional;
+    prm.conditional.type = cudaGraphCondTypeWhile;
+    prm.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphConditionalHandleCreate(&ctx.loop_handle, g, 1, cudaGraphCondAssignDefault) == cudaSuccess &&
+        (prm.conditional.handle = ctx.loop_handle, cudaGraphAddNode(&node, g, nullptr, 0, &prm) == cudaSuccess) &&
+        cudaStreamBeginCaptureToGraph(st, prm.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        cudaGraph_t body = nullptr;
+        try {
+            fill();
+        } catch (...) {
+            cudaStreamEndCapture(st, &body);
+            cudaGraphDestroy(g);
+            throw;
+        }
+        if (cudaStreamEndCapture(st, &body) == cudaSuccess && cudaGraphInstantiate(&exec, g, 0) != cudaSuccess)
+            exec = nullptr;
+    }
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return exec;
+}
+
 // PCG with per-piece scalars on level 0. V is the vector type of p, r, z, Ap; S the
 // type of x; P the precision of the V-cycle preconditioner (with rp, zp its vectors when
-// it differs from V). On return x holds the solution of K x = rhs for each piece.
+// it differs from V). On return x holds the solution of K x = rhs for each piece. Returns
+// the kernels one iteration of the device-side loop launches (0 when the loop ran from
+// the host), for the launch count.
 template <class V, class S, class P = V>
-static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V* ap, double tol, int64_t max_iter,
+static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V* ap, double tol, int64_t max_iter,
                 CgState& cg, int64_t timeout_ms, std::chrono::steady_clock::time_point t_start,
                 const int32_t* start_done = nullptr, P* rp = nullptr, P* zp = nullptr) {
     Level& L = b.levels[0];
@@ -514,29 +576,46 @@ static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V*
         k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
         SC_LAUNCH_CK();
     };
-    int32_t* ndone_h = nullptr;
-    SC_CK(cudaMallocHost((void**)&ndone_h, sizeof(int32_t)));
-    cudaGraphExec_t exec = nullptr;
+    int32_t* ndone_h = ctx.pinned_i32();
+    cudaGraphExec_t exec = nullptr, loop = nullptr;
+    int64_t per_iteration = 0, graph_kernels = 0;
+    // iterations one launch of the device-side loop runs at most between looks at the
+    // done count (and at the time limit)
+    const uint32_t chunk = 32;
     try {
         // Replaying a captured iteration saves ~50 launches an iteration; timing
         // individual kernels (profiling) launches them one by one instead.
-        bool use_graph = ctx.prof.mask == 0;
+        bool use_graph = ctx.prof.mask == 0 && graphs_enabled();
         if (use_graph) {
             ensure_partial(ctx, L);
             for (auto& lv : b.levels) prepare_top(lv);
-            cudaGraph_t graph = nullptr;
-            SC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            try {
+            // first choice: the iterations loop on the device, a graph whose conditional
+            // WHILE node replays the iteration until every piece is done (or `chunk` ran)
+            const int64_t l0 = g_launches.load();
+            loop = capture_loop(st, [&] {
                 body();
-            } catch (...) {
-                cudaStreamEndCapture(st, &graph);
-                if (graph) cudaGraphDestroy(graph);
-                throw;
+                k_loop_more<<<1, 1, 0, st>>>(ctx.loop_handle, cg.ndone.get(), np, cg.loop_count.get(), chunk);
+                SC_LAUNCH_CK();
+            }, ctx);
+            per_iteration = g_launches.load() - l0;
+            g_launches.fetch_sub(per_iteration);  // counted per iteration run, below
+            if (!loop) {
+                per_iteration = 0;
+                cudaGraph_t graph = nullptr;
+                SC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                try {
+                    body();
+                } catch (...) {
+                    cudaStreamEndCapture(st, &graph);
+                    if (graph) cudaGraphDestroy(graph);
+                    throw;
+                }
+                SC_CK(cudaStreamEndCapture(st, &graph));
+                cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+                cudaGraphDestroy(graph);
+                SC_CK(e);
+                graph_kernels = g_launches.load() - l0;
             }
-            SC_CK(cudaStreamEndCapture(st, &graph));
-            cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-            cudaGraphDestroy(graph);
-            SC_CK(e);
         }
         SC_CK(cudaMemsetAsync(cg.ndone.get(), 0, sizeof(int32_t), st));
         k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
@@ -551,20 +630,37 @@ static void pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p, V*
                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count() >
                     timeout_ms)
                 throw Error(SC_TIMEOUT, "solve ran past its time limit");
+            if (loop) {
+                SC_CK(cudaMemsetAsync(cg.loop_count.get(), 0, sizeof(uint32_t), st));
+                SC_CK(cudaGraphLaunch(loop, st));
+                continue;
+            }
             for (int g = 0; g < per_look; g++) {
-                if (exec)
+                if (exec) {
                     SC_CK(cudaGraphLaunch(exec, st));
-                else
+                    g_launches.fetch_add(graph_kernels);
+                } else {
                     body();
+                }
             }
         }
     } catch (...) {
         if (exec) cudaGraphExecDestroy(exec);
-        cudaFreeHost(ndone_h);
+        if (loop) cudaGraphExecDestroy(loop);
         throw;
     }
     if (exec) cudaGraphExecDestroy(exec);
-    cudaFreeHost(ndone_h);
+    if (loop) cudaGraphExecDestroy(loop);
+    return per_iteration;
+}
+
+// the device-side loop ran one iteration per iteration of its slowest piece (and one
+// more whose kernels returned at once after the last piece finished)
+static void count_loop_launches(int64_t per_iteration, const std::vector<int64_t>& iters) {
+    if (per_iteration <= 0) return;
+    int64_t most = 0;
+    for (int64_t i : iters) most = std::max(most, i);
+    g_launches.fetch_add(per_iteration * (most + 1));
 }
 
 // |b - K x| / |b| per piece, in FP64
@@ -599,11 +695,12 @@ void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, So
     ap.alloc(n6, ctx.stream, &ctx.mem);
     CgState cg;
     cg.init(ctx, b.npieces, b.status_d.get());
-    pcg<double, double>(ctx, b, b.loads.get(), x.get(), r.get(), z.get(), p.get(), ap.get(), opt.tol, opt.max_iter, cg,
-                        opt.timeout_ms, t0);
+    int64_t per_it = pcg<double, double>(ctx, b, b.loads.get(), x.get(), r.get(), z.get(), p.get(), ap.get(), opt.tol,
+                                         opt.max_iter, cg, opt.timeout_ms, t0);
     std::vector<int64_t> it(b.npieces);
     cg.iters.download(it.data(), b.npieces);
     SC_CK(cudaStreamSynchronize(ctx.stream));
+    count_loop_launches(per_it, it);
     stats.iterations = it;
     stats.refinements.assign(b.npieces, 0);
     true_residual(ctx, b, x.get(), stats.residual);
@@ -722,11 +819,13 @@ void pcg_fp32_cycle(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>&
     z32.alloc(n6, ctx.stream, &ctx.mem);
     CgState cg;
     cg.init(ctx, b.npieces, b.status_d.get());
-    pcg<double, double, float>(ctx, b, b.loads.get(), x.get(), r.get(), z.get(), p.get(), ap.get(), opt.tol,
-                               opt.max_iter, cg, opt.timeout_ms, t0, nullptr, r32.get(), z32.get());
+    int64_t per_it = pcg<double, double, float>(ctx, b, b.loads.get(), x.get(), r.get(), z.get(), p.get(), ap.get(),
+                                                opt.tol, opt.max_iter, cg, opt.timeout_ms, t0, nullptr, r32.get(),
+                                                z32.get());
     std::vector<int64_t> it(b.npieces);
     cg.iters.download(it.data(), b.npieces);
     SC_CK(cudaStreamSynchronize(ctx.stream));
+    count_loop_launches(per_it, it);
     stats.iterations = it;
     stats.refinements.assign(b.npieces, 0);
     true_residual(ctx, b, x.get(), stats.residual);
@@ -816,10 +915,11 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
         k_mixed_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cand.get(), counts.get());
         SC_LAUNCH_CK();
     };
-    int32_t* counts_h = nullptr;
-    SC_CK(cudaMallocHost((void**)&counts_h, 2 * sizeof(int32_t)));
+    int32_t* counts_h = ctx.pinned_i32();
     cudaGraphExec_t plain = nullptr, upd = nullptr;
-    auto capture = [&](auto fn) {
+    int64_t plain_kernels = 0, upd_kernels = 0;
+    auto capture = [&](auto fn, int64_t& kernels) {
+        const int64_t l0 = g_launches.load();
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         SC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -834,16 +934,18 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
         cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         SC_CK(e);
+        kernels = g_launches.load() - l0;
+        g_launches.fetch_sub(kernels);  // counted per replay
         return exec;
     };
     try {
-        bool use_graph = ctx.prof.mask == 0;
+        bool use_graph = ctx.prof.mask == 0 && graphs_enabled();
         auto it_plain = [&]() { first(); second(); };
         auto it_upd = [&]() { first(); update(); second(); };
         if (use_graph) {
             ensure_partial(ctx, L);
-            plain = capture(it_plain);
-            upd = capture(it_upd);
+            plain = capture(it_plain, plain_kernels);
+            upd = capture(it_upd, upd_kernels);
         }
         // the starting verdict: b = 0 finishes at once
         SC_CK(cudaMemsetAsync(counts.get(), 0, 2 * sizeof(int32_t), st));
@@ -861,15 +963,18 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
                     second();
                 } else if (upd) {
                     SC_CK(cudaGraphLaunch(upd, st));
+                    g_launches.fetch_add(upd_kernels);
                 } else {
                     it_upd();
                 }
                 since = 0;
             } else {
-                if (plain)
+                if (plain) {
                     SC_CK(cudaGraphLaunch(plain, st));
-                else
+                    g_launches.fetch_add(plain_kernels);
+                } else {
                     it_plain();
+                }
                 since++;
             }
             SC_CK(cudaMemcpyAsync(counts_h, counts.get(), 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -882,12 +987,10 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
     } catch (...) {
         if (plain) cudaGraphExecDestroy(plain);
         if (upd) cudaGraphExecDestroy(upd);
-        cudaFreeHost(counts_h);
         throw;
     }
     if (plain) cudaGraphExecDestroy(plain);
     if (upd) cudaGraphExecDestroy(upd);
-    cudaFreeHost(counts_h);
     std::vector<int64_t> it(np), up(np);
     cg.iters.download(it.data(), np);
     updates.download(up.data(), np);

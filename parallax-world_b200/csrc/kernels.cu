@@ -27,7 +27,22 @@ __global__ void __launch_bounds__(256) k_spmv(int64_t nrows, const int64_t* __re
     T acc = T(0);
     int64_t e0 = rowptr[row], e1 = rowptr[row + 1];
     if (rr < 6) {
-        for (int64_t e = e0 + g; e < e1; e += 4) {
+        // two of the slot's blocks (e, e + 4) loaded before either is used: 8 blocks in
+        // flight per warp; the lane still adds its blocks in the order e0 + g, + 4, + 8, ...
+        int64_t e = e0 + g;
+        for (; e + 4 < e1; e += 8) {
+            int32_t j0 = col[e], j1 = col[e + 4];
+            T a0[6], x0[6], a1[6], x1[6];
+            ld6<T>(val + 36 * e + 6 * rr, a0);
+            ld6<T>(val + 36 * (e + 4) + 6 * rr, a1);
+            ld6<T>(x + 6 * (int64_t)j0, x0);
+            ld6<T>(x + 6 * (int64_t)j1, x1);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a0[c], x0[c], acc);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a1[c], x1[c], acc);
+        }
+        if (e < e1) {
             int32_t j = col[e];
             T a[6], xv[6];
             ld6<T>(val + 36 * e + 6 * rr, a);

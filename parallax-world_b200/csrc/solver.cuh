@@ -201,7 +201,10 @@ struct Context {
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
     std::unique_ptr<Batch> last;     // the last solve's hierarchy (parity queries)
+    int32_t* pinned = nullptr;       // 16 bytes of pinned host memory for small reads
+    cudaGraphConditionalHandle loop_handle = 0;  // the device-side CG loop's condition
     void* cub_scratch(size_t bytes);
+    int32_t* pinned_i32();
     ~Context();
 };
 

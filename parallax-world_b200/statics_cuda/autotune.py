@@ -109,17 +109,18 @@ def choose(solver: Solver, pieces, precision: int = MIXED, tol: float = 1e-8, pa
 
 def solve_batch(solver: Solver, pieces, precision: int = MIXED, tol: float = 1e-8, path: str = DEFAULT_CACHE,
                 settings: dict | None = None):
-    """Solves `pieces` grouped by size class, each group one batched solve with its
-    tuned setting; a piece that did not converge is solved again alone with the
-    reference's setting. Returns (motions, infos) in the order of `pieces`."""
+    """Solves `pieces` with their size classes' tuned settings: the pieces that share a
+    setting form one batched solve (fewer, larger batches than one per class); a piece
+    that did not converge is solved again alone with the reference's setting. Returns
+    (motions, infos) in the order of `pieces`."""
     settings = settings or choose(solver, pieces, precision, tol, path)
-    groups: dict[int, list[int]] = {}
+    groups: dict[tuple, list[int]] = {}
     for i, p in enumerate(pieces):
-        groups.setdefault(size_class(p[0]), []).append(i)
+        s = settings.get(size_class(p[0]), FALLBACK)
+        groups.setdefault((s["sweeps"], s["tile"]), []).append(i)
     motions, infos = [None] * len(pieces), [None] * len(pieces)
-    for cls, idx in groups.items():
-        s = settings.get(cls, FALLBACK)
-        opt = options(tol=tol, precision=precision, sweeps=s["sweeps"], tile=s["tile"], max_iter=MAX_ITER)
+    for (sweeps, tile), idx in groups.items():
+        opt = options(tol=tol, precision=precision, sweeps=sweeps, tile=tile, max_iter=MAX_ITER)
         outs, inf = solver.solve_grid_batch([pieces[i] for i in idx], opt)
         for j, i in enumerate(idx):
             motions[i], infos[i] = outs[j], inf[j]
