@@ -332,9 +332,12 @@ def run_probe(args):
         # validated against the CPU oracle up to 128^3 by the parity tests)
         import numpy as np
         n = args.large_n
+        solver = sc.Solver(0)
+        ws, wk = sc.generate_piece(48, 48, 48, 1, sc.K_LOGNORMAL)
+        for prec in (sc.MIXED, sc.FP64):  # warm-up: the library's kernels loaded once
+            solver.compliance_grad(ws, wk, sc.options(tol=TOL, precision=prec))
         st, k = sc.generate_piece(n, n, n, args.seed, sc.K_LOGNORMAL)
         nodes, parts = sc.grid_count(st)
-        solver = sc.Solver(0)
         out = {"probe": "large", "grid": [n, n, n], "free_cells": int((st == sc.CELL_FREE).sum()),
                "dof": 6 * parts, "tol": TOL}
         res = {}

@@ -209,9 +209,8 @@ sc_status sc_context_stream(sc_context* ctx, void** stream);
  * Compliance without device allocation. No counterpart in the reference.
  *
  * For callers that must not have the library allocate device memory: an engine that
- * owns the GPU's memory through its own arena, code running while its caller captures
- * a CUDA graph, or a per-frame loop that cannot afford cudaMalloc's implicit device
- * synchronisation. It computes C = f . u (n_values doubles each, device pointers; e.g.
+ * owns the GPU's memory through its own arena, or a per-frame loop that cannot afford
+ * cudaMalloc's implicit device synchronisation. It computes C = f . u (n_values doubles each, device pointers; e.g.
  * the loads and the motions of sc_solve_grid, node order) into *compliance (a device
  * pointer), on `stream` (a cudaStream_t; NULL = the legacy default stream), with the
  * solver's deterministic chunked sum, and allocates nothing: its partial sums live in

@@ -1,14 +1,16 @@
 """Autotuner for batched solves of voxel pieces.
 
 Pieces are put in size classes (their grid cells rounded up to a power of two). For
-each class it times the full solves (setup + PCG to the requested tolerance) of up to
-SAMPLES of its pieces under every candidate setting -- block-Jacobi sweeps before and
-after each coarse correction (the reference does one, statics/src/bodies.rs:386,
-396-401) and the stencil tile (the window of parts grouped by axis) -- and keeps the
-fastest setting that solved every sample. Two sweeps per level make a stronger
-preconditioner, but the damped-Jacobi step 4/(3 lambda_max) is the reference's choice
-for one sweep; on some pieces two sweeps lose definiteness and CG stalls, so a setting
-counts only if all its samples converge within TRIAL_MAX_ITER iterations. Choices are
+each class it times a batched solve (setup + PCG to the requested tolerance, as the
+batch will run) of up to SAMPLES of its pieces under every candidate setting --
+block-Jacobi sweeps before and after each coarse correction (the reference does one,
+statics/src/bodies.rs:386, 396-401) and the stencil tile (the window of parts grouped
+by axis) -- and keeps the fastest setting that solved every sample. A batch iterates
+until its slowest piece converges, so timing single pieces misjudges a setting: two
+sweeps per level cut the mean iteration count but can leave a straggler (the damped-
+Jacobi step 4/(3 lambda_max) is the reference's choice for one sweep; on some pieces
+two sweeps lose definiteness and CG stalls), so a setting counts only if all its
+samples converge within TRIAL_MAX_ITER iterations. Choices are
 cached in a JSON file keyed by class, precision and tolerance, so a later batch of the
 same classes is not tuned again. A piece that still fails in the batched solve is
 solved again alone with the reference's one sweep (its info then says retried).
@@ -23,7 +25,7 @@ from . import FP64, MIXED, Solver, options
 
 SWEEPS = (1, 2)
 TILES = (256, 1024, 4096)
-SAMPLES = 3
+SAMPLES = 8
 TRIAL_MAX_ITER = 2000
 MAX_ITER = 20000
 FALLBACK = {"sweeps": 1, "tile": 0}
@@ -39,7 +41,7 @@ def size_class(state) -> int:
 
 
 def _key(cls: int, precision: int, tol: float) -> str:
-    return f"{cls}:{'mixed' if precision == MIXED else 'fp64'}:{tol:g}"
+    return f"batch:{cls}:{precision}:{tol:g}"
 
 
 def load(path: str = DEFAULT_CACHE) -> dict:
@@ -58,29 +60,25 @@ def save(cache: dict, path: str = DEFAULT_CACHE) -> None:
 
 
 def tune_class(solver: Solver, samples, precision: int = MIXED, tol: float = 1e-8, repeats: int = 2) -> dict:
-    """Times every (sweeps, tile) on the sample pieces; returns the fastest setting that
-    solved all of them, with the timings (the reference's setting if none did)."""
+    """Times a batched solve of the sample pieces under every (sweeps, tile); returns the
+    fastest setting that solved all of them, with the timings (the reference's setting if
+    none did)."""
     trials = []
     for sweeps in SWEEPS:
         for tile in TILES:
             opt = options(tol=tol, precision=precision, sweeps=sweeps, tile=tile, max_iter=TRIAL_MAX_ITER)
-            total, iters = 0.0, []
-            for state, k in samples:
-                best = None
-                for _ in range(repeats):
-                    t = time.perf_counter()
-                    _, info = solver.solve_grid(state, k, opt)
-                    dt = time.perf_counter() - t
-                    if info["status"] != 0 or not info["residual"] <= tol * 1.0001:
-                        dt = float("inf")
-                    best = dt if best is None else min(best, dt)
-                    if dt == float("inf"):
-                        break
-                total += best
-                iters.append(info["iterations"])
-                if total == float("inf"):
+            best, iters = float("inf"), []
+            for _ in range(repeats):
+                t = time.perf_counter()
+                _, infos = solver.solve_grid_batch(samples, opt)
+                dt = time.perf_counter() - t
+                iters = [i["iterations"] for i in infos]
+                if any(i["status"] != 0 or not i["residual"] <= tol * 1.0001 for i in infos):
+                    dt = float("inf")
+                    best = dt
                     break
-            trials.append({"sweeps": sweeps, "tile": tile, "seconds": total, "iterations": iters})
+                best = min(best, dt)
+            trials.append({"sweeps": sweeps, "tile": tile, "seconds": best, "iterations": iters})
     ok = [t for t in trials if t["seconds"] < float("inf")]
     if not ok:
         return dict(FALLBACK, seconds=None, trials=trials)

@@ -1,6 +1,6 @@
 """sc_compliance_noalloc — compliance of motions already on the device, for callers that
 cannot let the library allocate device memory (an engine that owns the GPU's memory,
-code inside a graph capture, a frame loop that cannot stall on cudaMalloc). Its result
+a frame loop that cannot stall on cudaMalloc). Its result
 must match the compliance sc_compliance_grad reports for the same solve, call after
 call, although it keeps its partial sums in one array shared by every call.
 
