@@ -207,7 +207,7 @@ def run_ours(args):
     def timed(precision, steps, warmup):
         """K solves on the solver's stream, CUDA events around them, profiling off (the
         CG iterations run as CUDA graphs)."""
-        opt = sc.options(tol=TOL, precision=precision)
+        opt = sc.options(tol=TOL, precision=precision, tile=args.tile)
         for _ in range(warmup):
             solver.solve_grid_device(grid, opt, out_d.data_ptr(), out_d.numel())
         barrier(world)
@@ -225,7 +225,7 @@ def run_ours(args):
     def profiled(precision, mask):
         """One more solve of the same workload with per-launch CUDA events on the
         solver's stream for the kernel families in `mask` (kernels launched one by one)."""
-        opt = sc.options(tol=TOL, precision=precision)
+        opt = sc.options(tol=TOL, precision=precision, tile=args.tile)
         barrier(world)
         torch.cuda.synchronize()
         solver.profile(mask)
@@ -394,12 +394,15 @@ def run_probe(args):
         print(json.dumps({"probe": "fp64 single", "pieces": 32, "seconds": time.perf_counter() - t}), flush=True)
         solver.close()
         return
-    state, k = sc.generate_piece(N, N, N, args.seed, sc.K_UNIFORM)
+    pn = args.probe_n
+    state, k = sc.generate_piece(pn, pn, pn, args.seed, sc.K_UNIFORM)
     if args.probe == "solve":
         solver = sc.Solver(0)
-        for prec in (sc.FP64, sc.MIXED, sc.MIXED_FP32_KRYLOV, sc.FP64, sc.MIXED, sc.MIXED_FP32_KRYLOV):
-            _, info = solver.solve_grid(state, k, sc.options(tol=TOL, precision=prec))
-            print(json.dumps({"probe": "solve", "precision": prec, "iterations": info["iterations"],
+        order = {"all": (sc.FP64, sc.MIXED, sc.MIXED_FP32_KRYLOV) * 2, "mixed": (sc.MIXED,) * 2,
+                 "fp64": (sc.FP64,) * 2}[args.precision]
+        for prec in order:
+            _, info = solver.solve_grid(state, k, sc.options(tol=TOL, precision=prec, tile=args.tile))
+            print(json.dumps({"probe": "solve", "precision": prec, "tile": args.tile, "iterations": info["iterations"],
                               "setup_ms": info["setup_ms"], "solve_ms": info["solve_ms"]}))
         solver.close()
         return
@@ -487,6 +490,10 @@ def main():
     ap.add_argument("--batch", type=int, default=512, help="pieces in the batched section")
     ap.add_argument("--batch-sample", type=int, default=64, help="pieces the one-at-a-time FP64 leg solves")
     ap.add_argument("--large-n", type=int, default=256, help="edge of the --probe large piece")
+    ap.add_argument("--tile", type=int, default=0, help="sc_options.tile of the solves (0: the default stencil)")
+    ap.add_argument("--probe-n", type=int, default=N, help="edge of the --probe solve / stencil piece")
+    ap.add_argument("--precision", choices=["all", "mixed", "fp64"], default="all",
+                    help="the --probe solve precisions: all three twice, or two solves of one")
     ap.add_argument("--probe", choices=["stencil", "solve", "batch", "large"], help="run one kernel or one solve alone (profiling)")
     args = ap.parse_args()
     if args.probe:

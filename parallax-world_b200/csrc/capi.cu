@@ -198,8 +198,8 @@ void check_options(const sc_options& o) {
     require(o.precision == SC_FP64 || o.precision == SC_MIXED || o.precision == SC_MIXED_FP32_KRYLOV, SC_BAD_INPUT,
             "unknown precision");
     require(o.sweeps >= 1 && o.sweeps <= 8, SC_BAD_INPUT, "sweeps must be 1 to 8");
-    require(o.tile == 0 || o.tile == 1 || (o.tile >= 32 && o.tile <= (1 << 20) && (o.tile & (o.tile - 1)) == 0), SC_BAD_INPUT,
-            "tile must be 0, 1 or a power of two from 32");
+    require(o.tile == 0 || o.tile == 1 || o.tile == 2 || (o.tile >= 32 && o.tile <= (1 << 20) && (o.tile & (o.tile - 1)) == 0), SC_BAD_INPUT,
+            "tile must be 0, 1, 2 or a power of two from 32");
 }
 
 // The reference's Work for a solve of one piece: parts + pairs per level apply

@@ -747,6 +747,99 @@ __global__ void __launch_bounds__(PENCIL_THREADS, 2) k_stencil_pencil(
     }
 }
 
+// ---- the two-pass (cell, then part) stencil --------------------------------------
+// Pass 1 gives each free cell's six face rows of k_c s D Kt D x (36 values, slot by
+// slot) to a per-cell buffer: a cell gathers its six faces once, where the per-part
+// stencil gathers each face about six times (once per part of the two cells), and
+// consecutive cells write consecutive records. Pass 2 walks the parts in slot order and
+// adds the two records' rows of its faces, Kx = Y_lesser[2a+1] + Y_greater[2a], before
+// the part's epilogue. It moves the 36 values a cell twice more than the per-part
+// stencil's algorithmic bytes but reads them coalesced.
+template <class T>
+__global__ void __launch_bounds__(256) k_cell_rows(int64_t ncells, const int4* __restrict__ cell,
+                                                   const T* __restrict__ x, T s, T* __restrict__ ycell,
+                                                   const int32_t* __restrict__ cell_piece,
+                                                   const int32_t* __restrict__ done) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    if (done && done[cell_piece[c]]) return;
+    const int4 a = __ldg(cell + 2 * c), b = __ldg(cell + 2 * c + 1);
+    const T kc = (T)__int_as_float(b.z);
+    T xs[6][6];
+    gather_cell<T>(a, b, x, s, xs);
+    T* out = ycell + 36 * c;
+    T y6[6];
+    slot_out<0, T>(xs, kc, s, y6);
+    store6<T>(out, 0, y6);
+    slot_out<1, T>(xs, kc, s, y6);
+    store6<T>(out, 1, y6);
+    slot_out<2, T>(xs, kc, s, y6);
+    store6<T>(out, 2, y6);
+    slot_out<3, T>(xs, kc, s, y6);
+    store6<T>(out, 3, y6);
+    slot_out<4, T>(xs, kc, s, y6);
+    store6<T>(out, 4, y6);
+    slot_out<5, T>(xs, kc, s, y6);
+    store6<T>(out, 5, y6);
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) k_part_rows(int64_t n_perm, const int4* __restrict__ slots,
+                                                   const int4* __restrict__ cell, const T* __restrict__ ycell,
+                                                   const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
+                                                   T* __restrict__ y2, T s, const int32_t* __restrict__ piece,
+                                                   const double* __restrict__ step,
+                                                   const int32_t* __restrict__ skip_row,
+                                                   const int32_t* __restrict__ done) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n_perm) return;
+    const int4 sl = __ldg(slots + i);  // part, lesser cell, greater cell, axis
+    const int32_t k = sl.x, A = sl.y, B = sl.z;
+    if (skip_row && skip_row[k]) return;
+    const int p = (done || step) ? piece[k] : 0;
+    if (done && done[p]) return;
+    const T w = step ? (T)step[p] : T(0);
+    T kx[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    if (A >= 0) {
+        T v[6];
+        load6<T>(ycell + 36 * (int64_t)A, 2 * sl.w + 1, v);
+#pragma unroll
+        for (int j = 0; j < 6; j++) kx[j] += v[j];
+    }
+    if (B >= 0) {
+        T v[6];
+        load6<T>(ycell + 36 * (int64_t)B, 2 * sl.w, v);
+#pragma unroll
+        for (int j = 0; j < 6; j++) kx[j] += v[j];
+    }
+    T kA = T(0), kB = T(0);
+    if constexpr (MODE == ST_RES_JAC || MODE == ST_PROLONG || MODE == ST_SMOOTH) {
+        if (A >= 0) kA = (T)__int_as_float(__ldg(&cell[2 * A + 1].z));
+        if (B >= 0) kB = (T)__int_as_float(__ldg(&cell[2 * B + 1].z));
+    }
+    if (sl.w == 0)
+        pencil_finish<0, T, MODE>(k, kx, kA, kB, s, w, x, r, y, y2);
+    else if (sl.w == 1)
+        pencil_finish<1, T, MODE>(k, kx, kA, kB, s, w, x, r, y, y2);
+    else
+        pencil_finish<2, T, MODE>(k, kx, kA, kB, s, w, x, r, y, y2);
+}
+
+// a free cell's piece (from its flat index and the pieces' first flat cells)
+__global__ void k_cell_piece(int64_t ncells, const int64_t* __restrict__ cell_flat, const int64_t* __restrict__ goff,
+                             int np, int32_t* __restrict__ cell_piece) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int64_t f = cell_flat[c];
+    int lo = 0, hi = np;  // last piece whose first cell is <= f
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (goff[mid] <= f) lo = mid;
+        else hi = mid;
+    }
+    cell_piece[c] = lo;
+}
+
 // x = w D^-1 r with D^-1 matrix-free (pre-smoothing, bodies.rs:386)
 template <class T>
 __global__ void __launch_bounds__(256) k_jacobi_mf(int64_t n, const int8_t* __restrict__ axis,
@@ -881,7 +974,19 @@ static void launch_stencil(Context& ctx, const Batch& b, const T* x, const T* r,
         SC_LAUNCH_CK();
         return;
     }
-    k_stencil<T, MODE><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.slots.get(), g.cell.get(), x, r, y, y2, (T)g.s, L.piece.get(), step, skip_row, done);
+    if (g.two_pass) {
+        T* yc = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)g.ycell64.get() : (void*)g.ycell32.get());
+        k_cell_rows<T><<<grid_for(g.ncells, 256), 256, 0, ctx.stream>>>(g.ncells, g.cell.get(), x, (T)g.s, yc,
+                                                                        g.cell_piece.get(), done);
+        SC_LAUNCH_CK();
+        k_part_rows<T, MODE><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.slots.get(), g.cell.get(), yc, x, r, y,
+                                                                       y2, (T)g.s, L.piece.get(), step, skip_row,
+                                                                       done);
+        SC_LAUNCH_CK();
+        return;
+    }
+    k_stencil<T, MODE><<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, g.slots.get(), g.cell.get(), x, r, y, y2, (T)g.s,
+                                                                 L.piece.get(), step, skip_row, done);
     SC_LAUNCH_CK();
 }
 
@@ -984,7 +1089,7 @@ void grid_cell_energy(Context& ctx, const Batch& b, const double* x, double* ene
 // Builds level 0 of a batch of voxel pieces. The grids' state/k are uploaded (or
 // copied device to device) into one concatenated array.
 void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool keep_blocks, int32_t tile) {
-    const int64_t TILE = tile > 1 ? tile : STENCIL_TILE;
+    const int64_t TILE = tile >= 32 ? tile : STENCIL_TILE;
     PhaseTimer pt(ctx);
     cudaStream_t st = ctx.stream;
     MemStats* ms = &ctx.mem;
@@ -1155,6 +1260,17 @@ void grid_level0(Context& ctx, Batch& b, const std::vector<sc_grid>& grids, bool
         SC_CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
     }
     g.pencil = tile == 1;
+    g.two_pass = tile == 2;
+    if (g.two_pass) {
+        g.cell_piece.alloc(std::max<int64_t>(nfree, 1), st, ms);
+        if (nfree > 0) {
+            k_cell_piece<<<grid_for(nfree, 256), 256, 0, st>>>(nfree, g.cell_flat.get(), goff_d.get(), np,
+                                                              g.cell_piece.get());
+            SC_LAUNCH_CK();
+        }
+        g.ycell64.alloc(36 * std::max<int64_t>(nfree, 1), st, ms);
+        g.ycell32.alloc(36 * std::max<int64_t>(nfree, 1), st, ms);
+    }
     SC_LAUNCH_CK();
     // parts in order, grouped by axis only within tiles of STENCIL_TILE parts: the
     // stencil sweeps the piece once in part order (x neighbours stay in L2) while a

@@ -28,6 +28,10 @@ struct Grid0 {
     DBuf<int32_t> perm;         // parts in order, grouped by axis inside tiles of 1024 parts
     DBuf<int4> slots;           // per perm slot: part, lesser cell, greater cell, axis
     bool pencil = false;        // the plane-pencil stencil (tile 1) or the per-slot one
+    bool two_pass = false;      // the two-pass stencil (tile 2): per-cell rows, then per part
+    DBuf<int32_t> cell_piece;   // two-pass: per free cell its piece
+    DBuf<double> ycell64;       // two-pass: 36 values per free cell
+    DBuf<float> ycell32;
     DBuf<int32_t> gridmap;      // per grid cell: its free-cell index or -1
     DBuf<uint8_t> tiles;        // pencil tiles (piece, x0, y0, z0)
     DBuf<uint8_t> geo;          // per piece: dims and first flat cell

@@ -178,11 +178,12 @@ def test_batch_mixed(solver):
         assert rel(u, u_ref) < DISP_TOL
 
 
-@pytest.mark.parametrize("tile", [1, 32, 4096])
+@pytest.mark.parametrize("tile", [1, 2, 32, 4096])
 @pytest.mark.parametrize("precision", [sc.FP64, sc.MIXED], ids=["fp64", "mixed"])
 def test_stencil_variants(solver, tile, precision):
-    """The level-0 stencils sc_options.tile selects (1: the plane-pencil stencil; a power
-    of two: the per-part stencil's axis-grouping window) apply the same operator: the
+    """The level-0 stencils sc_options.tile selects (1: the plane-pencil stencil; 2: the
+    two-pass cell-then-part stencil; a power of two: the per-part stencil's axis-grouping
+    window) apply the same operator: the
     same hierarchy and iterations as the default, motions within the displacement bar of
     the oracle's. The shape is ragged against the pencil's 16 x 8 x 32 blocks."""
     st, k = piece(0, 41, shape=(37, 21, 45))
