@@ -486,9 +486,11 @@ __device__ __forceinline__ void stencil_row(int32_t k, int32_t A, int32_t B, int
     }
 }
 
-// Level 0 applied matrix-free over the parts grouped by axis (perm).
+// Level 0 applied matrix-free over the parts grouped by axis (perm). The register cap
+// (four blocks of 256 in FP32, three in FP64) trades a few FP64 spills for occupancy:
+// the gathers are latency-bound, and the capped kernel measured 2-4 % faster.
 template <class T, int MODE>
-__global__ void __launch_bounds__(256, 2) k_stencil(int64_t n_perm, const int4* __restrict__ slots,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_stencil(int64_t n_perm, const int4* __restrict__ slots,
                                                  const int4* __restrict__ cell,
                                                  const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
                                                  T* __restrict__ y2, T s, const int32_t* __restrict__ piece,
