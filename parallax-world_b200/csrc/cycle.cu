@@ -363,19 +363,29 @@ __global__ void __launch_bounds__(256) k_chunk_dot2(const int64_t* __restrict__ 
     }
 }
 
+// per piece: the sums of its chunks' two partials, one warp per piece (each lane a
+// strided run of chunks, then a shuffle tree: a fixed order, so the same value every run)
 __global__ void k_piece_sum2(int np, const int64_t* __restrict__ piece_chunk, const double* __restrict__ pa,
                              const double* __restrict__ pb, const int32_t* __restrict__ done, double* __restrict__ oa,
                              double* __restrict__ ob) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (p >= np) return;
     if (done && done[p]) return;
     double s1 = 0.0, s2 = 0.0;
-    for (int64_t c = piece_chunk[p]; c < piece_chunk[p + 1]; c++) {
+    for (int64_t c = piece_chunk[p] + lane; c < piece_chunk[p + 1]; c += 32) {
         s1 += pa[c];
-        s2 += pb[c];
+        if (ob) s2 += pb[c];
     }
-    oa[p] = s1;
-    if (ob) ob[p] = s2;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+    }
+    if (lane == 0) {
+        oa[p] = s1;
+        if (ob) ob[p] = s2;
+    }
 }
 
 template <class T>
@@ -450,7 +460,8 @@ static void dot2(Context& ctx, const Level& L, const int32_t* done, const T* a, 
                                                                     pa, pb);
         SC_LAUNCH_CK();
     }
-    k_piece_sum2<<<grid_for(np, 128), 128, 0, ctx.stream>>>(np, L.piece_chunk.get(), pa, pb, done, oab, oaa);
+    k_piece_sum2<<<grid_for((int64_t)np * 32, 128), 128, 0, ctx.stream>>>(np, L.piece_chunk.get(), pa, pb, done, oab,
+                                                                         oaa);
     SC_LAUNCH_CK();
 }
 

@@ -188,13 +188,18 @@ __global__ void __launch_bounds__(256) k_chunk_dot(const int64_t* __restrict__ c
     if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
 }
 
+// per piece: the sum of its chunks' partials, one warp per piece (strided lanes, then a
+// shuffle tree: a fixed order)
 __global__ void k_piece_sum(int np, const int64_t* __restrict__ piece_chunk, const double* __restrict__ partial,
                             double* __restrict__ out) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (p >= np) return;
     double s = 0.0;
-    for (int64_t c = piece_chunk[p]; c < piece_chunk[p + 1]; c++) s += partial[c];
-    out[p] = s;
+    for (int64_t c = piece_chunk[p] + lane; c < piece_chunk[p + 1]; c += 32) s += partial[c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) out[p] = s;
 }
 
 }  // namespace
@@ -267,7 +272,8 @@ void seg_dot_t(Context& ctx, const Level& L, const T* a, const T* b, double* out
         k_chunk_dot<T><<<(unsigned)L.nchunks, 256, 0, ctx.stream>>>(L.chunk_lo.get(), a, b, ctx.partial.get());
         SC_LAUNCH_CK();
     }
-    k_piece_sum<<<grid_for(np, 128), 128, 0, ctx.stream>>>(np, L.piece_chunk.get(), ctx.partial.get(), out);
+    k_piece_sum<<<grid_for((int64_t)np * 32, 128), 128, 0, ctx.stream>>>(np, L.piece_chunk.get(), ctx.partial.get(),
+                                                                        out);
     SC_LAUNCH_CK();
 }
 
