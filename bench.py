@@ -297,6 +297,12 @@ def run_ours(args):
         "roofline": roof(prof, dominant),
         "stencil_roofline": roof(prof, stencil),
         "kernel_ms": {f: round(prof[f]["ms"], 3) for f in prof if prof[f]["launches"]},
+        # the whole CG phase against HBM: the algorithmic bytes of every timed kernel family
+        # of the profiled solve over the timed solves' CG time (dots and axpys not counted)
+        "solve_roofline": {"bytes_per_solve": sum(prof[f]["bytes"] for f in prof),
+                           "achieved": sum(prof[f]["bytes"] for f in prof) / (solve_ms_m / 1000.0) / 1e9,
+                           "peak": hbm, "unit": "GB/s",
+                           "frac": sum(prof[f]["bytes"] for f in prof) / (solve_ms_m / 1000.0) / 1e9 / hbm},
         "roofline_method": "per-launch CUDA events on the solver's stream during one profiled solve of the same "
                            "workload after the timed region (the timed region runs CUDA graphs, no events)",
         "e2e": {"value": world * K / (ms_e2e / 1000.0), "unit": "solves/s",

@@ -206,6 +206,42 @@ int64_t sc_launches(void);
 sc_status sc_context_stream(sc_context* ctx, void** stream);
 
 /* ---------------------------------------------------------------------------
+ * The callers of motions: the structure standing, and settling.
+ * ------------------------------------------------------------------------- */
+/* Per node its mass (Node::m) and per bond its material's strengths (Mat::ft, fc, fs),
+ * statics/src/model.rs:43-51, 92-111: what the loads and the bonds' use need beyond
+ * sc_lattice. Host arrays. */
+typedef struct sc_strength {
+    const double* m;   /* n_nodes */
+    const double* ft;  /* n_bonds: tensile */
+    const double* fc;  /* n_bonds: compressive */
+    const double* fs;  /* n_bonds: shear */
+} sc_strength;
+
+/* Replaces statics::bodies::used_standing (statics/src/bodies.rs:550-554): every bond
+ * alive, the nodes not joined to a held node through bonds gone, each node's weight
+ * (m * 9.81 down y, bodies.rs:408) as its load; writes each bond's used fraction of its
+ * strength (Bond::used, model.rs:123-129; 0 for a bond with a gone end) into used
+ * (n_bonds, host). */
+sc_status sc_used_standing(sc_context* ctx, const sc_lattice* lattice, const sc_strength* strength,
+                           const sc_options* opt, double* used, sc_solve_info* info);
+
+typedef struct sc_settle_info {
+    double fell;     /* the fallen fraction of the free mass (Outcome::fallen) */
+    int64_t rounds;  /* solves run */
+    double work;     /* the reference's Work counter over all rounds */
+    int32_t status;  /* the worst sc_status of the rounds' solves */
+    int32_t pad;
+} sc_settle_info;
+
+/* Replaces statics::bodies::settle (statics/src/bodies.rs:511-541): rounds of motions under
+ * the weights, each breaking every beam (4 consecutive bonds) with an alive bond used
+ * beyond 1 whose ends stand, and dropping the nodes no longer joined to a held node,
+ * until a round breaks nothing. gone: n_nodes bytes (host), 1 for a fallen node. */
+sc_status sc_settle(sc_context* ctx, const sc_lattice* lattice, const sc_strength* strength, const sc_options* opt,
+                    uint8_t* gone, sc_settle_info* out);
+
+/* ---------------------------------------------------------------------------
  * Compliance without device allocation. No counterpart in the reference.
  *
  * For callers that must not have the library allocate device memory: an engine that

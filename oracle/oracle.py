@@ -50,6 +50,7 @@ def lib():
         L.or_cell_energy.argtypes = [P, pd, I64, pd]
         L.or_used_standing.argtypes = [P, pd]
         L.or_settle.argtypes = [P, pd, pi64, pu8]
+        L.or_strengths.argtypes = [P, pd, pd, pd]
         L.or_as_generated.argtypes = [P, P]
         L.or_level0_apply.argtypes = [P, I64, pd, pd]
         L.or_invert.argtypes = [pd, pd]
@@ -161,6 +162,13 @@ class Lattice:
         x = np.ascontiguousarray(x, dtype=np.float64)
         lib().or_cell_energy(self.h, _p(x, C.c_double), n_cells, _p(e, C.c_double))
         return e
+
+    def strengths(self) -> dict:
+        """Each bond's tensile, compressive and shear strength (its material's)."""
+        b = self.n_bonds
+        out = dict(ft=np.zeros(b), fc=np.zeros(b), fs=np.zeros(b))
+        lib().or_strengths(self.h, _p(out["ft"], C.c_double), _p(out["fc"], C.c_double), _p(out["fs"], C.c_double))
+        return out
 
     def used_standing(self) -> np.ndarray:
         u = np.zeros(self.n_bonds)

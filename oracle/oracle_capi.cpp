@@ -86,6 +86,17 @@ void or_export(void* p, double* x, double* m, uint8_t* held, int64_t* around, in
     }
 }
 
+// Each bond's strengths (Mat::ft, fc, fs of its material, statics/src/model.rs:43-51).
+void or_strengths(void* p, double* ft, double* fc, double* fs) {
+    auto* h = static_cast<Handle*>(p);
+    const Lattice& L = h->lat;
+    for (size_t b = 0; b < L.bonds.size(); b++) {
+        ft[b] = L.bonds[b].mat.ft;
+        fc[b] = L.bonds[b].mat.fc;
+        fs[b] = L.bonds[b].mat.fs;
+    }
+}
+
 // motions (bodies.rs:429-468) with explicit loads (6 per node). Hierarchy outputs
 // (any may be null): counts/pairs/steps per level (capacity max_levels), n_levels,
 // and the concatenated `up` arrays of every coarsening (capacity up_cap).

@@ -278,6 +278,47 @@ sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double
 }  // namespace
 }  // namespace sc
 
+namespace sc {
+
+void check_lattice(const sc_lattice& lat) {
+    require(lat.n_nodes > 0 && lat.n_bonds >= 0, SC_BAD_INPUT, "empty lattice");
+    require(lat.x && lat.held && lat.around, SC_BAD_INPUT, "node arrays are required");
+    require(lat.n_bonds == 0 || (lat.bond_i && lat.bond_j && lat.bond_p && lat.bond_n && lat.bond_a && lat.bond_d &&
+                                 lat.bond_e && lat.bond_g),
+            SC_BAD_INPUT, "bond arrays are required");
+    for (int64_t b = 0; b < lat.n_bonds; b++)
+        require(lat.bond_i[b] >= 0 && lat.bond_i[b] < lat.n_nodes && lat.bond_j[b] >= 0 &&
+                    lat.bond_j[b] < lat.n_nodes,
+                SC_BAD_INPUT, "bond end out of range");
+}
+
+// motions (bodies.rs:429-468) of a lattice into out (6 per node, device), zeros for held
+// and gone nodes; returns the solve's status (the hierarchy stays as ctx.last)
+sc_status lattice_motions(Context& c, const sc_lattice& lat, const uint8_t* alive, const uint8_t* gone,
+                          const double* loads, const sc_options& opt, double* out, sc_solve_info* info) {
+    auto b = std::make_unique<Batch>();
+    c.last.reset();  // the previous solve's hierarchy is not kept through this one
+    SC_CK(cudaStreamSynchronize(c.stream));
+    c.mem.peak = c.mem.now;
+    lattice_level0(c, *b, lat, alive, gone, loads);
+    DBuf<double> x;
+    SolveStats st;
+    double solve_ms = 0;
+    sc_status solve_status = solve_batch(c, *b, opt, x, st, solve_ms);
+    SC_CK(cudaMemsetAsync(out, 0, 6 * lat.n_nodes * sizeof(double), c.stream));
+    const Level& L = b->levels[0];
+    k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(), b->part_node.get(),
+                                                         x.get(), out);
+    SC_LAUNCH_CK();
+    SC_CK(cudaStreamSynchronize(c.stream));
+    fill_info(*b, 0, st, info, solve_ms, c.mem.peak);
+    read_steps(c, *b, 0, info);
+    c.last = std::move(b);
+    return solve_status;
+}
+
+}  // namespace sc
+
 using namespace sc;
 
 extern "C" {
@@ -577,6 +618,7 @@ sc_status sc_last_up(sc_context* ctx, int32_t level, int32_t* up, int64_t capaci
     });
 }
 
+
 sc_status sc_motions(sc_context* ctx, const sc_lattice* lat, const uint8_t* alive, const uint8_t* gone,
                      const double* loads, const sc_options* opt, double* motions, sc_solve_info* info) {
     if (!lat || !loads || !opt || !motions) return SC_BAD_INPUT;
@@ -584,37 +626,40 @@ sc_status sc_motions(sc_context* ctx, const sc_lattice* lat, const uint8_t* aliv
     sc_status s = guarded(ctx, [&] {
         Context& c = ctx->c;
         check_options(*opt);
-        require(lat->n_nodes > 0 && lat->n_bonds >= 0, SC_BAD_INPUT, "empty lattice");
-        require(lat->x && lat->held && lat->around, SC_BAD_INPUT, "node arrays are required");
-        require(lat->n_bonds == 0 || (lat->bond_i && lat->bond_j && lat->bond_p && lat->bond_n && lat->bond_a &&
-                                      lat->bond_d && lat->bond_e && lat->bond_g),
-                SC_BAD_INPUT, "bond arrays are required");
-        for (int64_t b = 0; b < lat->n_bonds; b++)
-            require(lat->bond_i[b] >= 0 && lat->bond_i[b] < lat->n_nodes && lat->bond_j[b] >= 0 &&
-                        lat->bond_j[b] < lat->n_nodes,
-                    SC_BAD_INPUT, "bond end out of range");
-        auto b = std::make_unique<Batch>();
-        c.last.reset();  // the previous solve's hierarchy is not kept through this one
-        SC_CK(cudaStreamSynchronize(c.stream));
-        c.mem.peak = c.mem.now;
-        lattice_level0(c, *b, *lat, alive, gone, loads);
-        DBuf<double> x;
-        SolveStats st;
-        double solve_ms = 0;
-        solve_status = solve_batch(c, *b, *opt, x, st, solve_ms);
-        int64_t nodes = lat->n_nodes;
+        check_lattice(*lat);
         DBuf<double> out;
-        out.alloc(6 * nodes, c.stream, &c.mem);
-        out.zero();
-        const Level& L = b->levels[0];
-        k_scatter<<<grid_for(L.n, 256), 256, 0, c.stream>>>(L.n, L.piece.get(), b->node_start.get(),
-                                                             b->part_node.get(), x.get(), out.get());
-        SC_LAUNCH_CK();
-        out.download(motions, 6 * nodes);
+        out.alloc(6 * lat->n_nodes, c.stream, &c.mem);
+        solve_status = lattice_motions(c, *lat, alive, gone, loads, *opt, out.get(), info);
+        out.download(motions, 6 * lat->n_nodes);
         SC_CK(cudaStreamSynchronize(c.stream));
-        fill_info(*b, 0, st, info, solve_ms, c.mem.peak);
-        read_steps(c, *b, 0, info);
-        c.last = std::move(b);
+    });
+    return s != SC_OK ? s : solve_status;
+}
+
+sc_status sc_used_standing(sc_context* ctx, const sc_lattice* lat, const sc_strength* str, const sc_options* opt,
+                           double* used, sc_solve_info* info) {
+    if (!lat || !str || !opt || !used) return SC_BAD_INPUT;
+    sc_status solve_status = SC_OK;
+    sc_status s = guarded(ctx, [&] {
+        check_options(*opt);
+        check_lattice(*lat);
+        require(str->m && (lat->n_bonds == 0 || (str->ft && str->fc && str->fs)), SC_BAD_INPUT,
+                "masses and strengths are required");
+        solve_status = used_standing(ctx->c, *lat, *str, *opt, used, info);
+    });
+    return s != SC_OK ? s : solve_status;
+}
+
+sc_status sc_settle(sc_context* ctx, const sc_lattice* lat, const sc_strength* str, const sc_options* opt,
+                    uint8_t* gone, sc_settle_info* out) {
+    if (!lat || !str || !opt || !gone) return SC_BAD_INPUT;
+    sc_status solve_status = SC_OK;
+    sc_status s = guarded(ctx, [&] {
+        check_options(*opt);
+        check_lattice(*lat);
+        require(str->m && (lat->n_bonds == 0 || (str->ft && str->fc && str->fs)), SC_BAD_INPUT,
+                "masses and strengths are required");
+        solve_status = settle(ctx->c, *lat, *str, *opt, gone, out);
     });
     return s != SC_OK ? s : solve_status;
 }

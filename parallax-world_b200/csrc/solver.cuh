@@ -143,6 +143,15 @@ void level0_smooth(Context& ctx, const Batch& b, const T* r, const T* x, T* z, c
 void lattice_level0(Context& ctx, Batch& b, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,
                     const double* loads);
 
+// --- capi.cu / settle.cu -----------------------------------------------------------------
+// motions of a lattice into out_dev (6 per node, device); the solve's status
+sc_status lattice_motions(Context& ctx, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,
+                          const double* loads, const sc_options& opt, double* out_dev, sc_solve_info* info);
+sc_status used_standing(Context& ctx, const sc_lattice& L, const sc_strength& S, const sc_options& opt,
+                        double* used, sc_solve_info* info);
+sc_status settle(Context& ctx, const sc_lattice& L, const sc_strength& S, const sc_options& opt, uint8_t* gone,
+                 sc_settle_info* out);
+
 // --- hierarchy.cu ---------------------------------------------------------------------
 void setup_chunks(Context& ctx, Level& L, int32_t npieces);
 void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt);

@@ -78,6 +78,15 @@ class LatticeC(C.Structure):
                 ("bond_e", C.c_void_p), ("bond_g", C.c_void_p)]
 
 
+class Strength(C.Structure):
+    _fields_ = [("m", C.c_void_p), ("ft", C.c_void_p), ("fc", C.c_void_p), ("fs", C.c_void_p)]
+
+
+class SettleInfo(C.Structure):
+    _fields_ = [("fell", C.c_double), ("rounds", C.c_int64), ("work", C.c_double), ("status", C.c_int32),
+                ("pad", C.c_int32)]
+
+
 _lib = None
 
 
@@ -113,12 +122,17 @@ def lib():
         L.sc_launches.restype = C.c_int64
         L.sc_launches.argtypes = []
         L.sc_context_stream.argtypes = [P, C.POINTER(P)]
+        L.sc_used_standing.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
+                                       C.POINTER(SolveInfo)]
+        L.sc_settle.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
+                                C.POINTER(SettleInfo)]
         L.sc_compliance_noalloc.argtypes = [P, P, C.c_int64, P, P]
         L.sc_compliance_noalloc.restype = C.c_int
         for name in ("sc_profile", "sc_profile_read", "sc_context_stream"):
             getattr(L, name).restype = C.c_int
         for name in ("sc_create", "sc_generate_piece", "sc_grid_count", "sc_solve_grid", "sc_solve_grid_batch",
-                     "sc_compliance_grad", "sc_grid_apply", "sc_last_up", "sc_motions"):
+                     "sc_compliance_grad", "sc_grid_apply", "sc_last_up", "sc_motions", "sc_used_standing",
+                     "sc_settle"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -326,20 +340,10 @@ class Solver:
         arrays: x (n,3), held (n,), around (n,2,3), bi, bj (b,), p, n (b,3), a, d, e, g (b,),
         level. `loads` is (n, 6) or a callable of the node index, as in the reference."""
         nn = int(lattice["x"].shape[0])
-        nb = int(lattice["bi"].shape[0])
         if callable(loads):
             loads = np.array([loads(v) for v in range(nn)], dtype=np.float64)
         loads = np.ascontiguousarray(loads, np.float64).reshape(nn, 6)
-        arr = {}
-        for key, dt in (("x", np.float64), ("held", np.uint8), ("around", np.int64), ("bi", np.int64),
-                        ("bj", np.int64), ("p", np.float64), ("n", np.float64), ("a", np.float64),
-                        ("d", np.float64), ("e", np.float64), ("g", np.float64)):
-            arr[key] = np.ascontiguousarray(lattice[key], dt)
-        L = LatticeC()
-        L.level, L.n_nodes, L.n_bonds = int(lattice.get("level", 0)), nn, nb
-        L.x, L.held, L.around = _ptr(arr["x"]), _ptr(arr["held"]), _ptr(arr["around"])
-        L.bond_i, L.bond_j, L.bond_p, L.bond_n = _ptr(arr["bi"]), _ptr(arr["bj"]), _ptr(arr["p"]), _ptr(arr["n"])
-        L.bond_a, L.bond_d, L.bond_e, L.bond_g = _ptr(arr["a"]), _ptr(arr["d"]), _ptr(arr["e"]), _ptr(arr["g"])
+        L, arr = _lattice_c(lattice)
         al = None if alive is None else np.ascontiguousarray(alive, np.uint8)
         gn = None if gone is None else np.ascontiguousarray(gone, np.uint8)
         out = np.zeros((nn, 6))
@@ -352,6 +356,55 @@ class Solver:
             work.status = s
             work.info = info.as_dict()
         return out
+
+
+    def used_standing(self, lattice: dict, opt: Options | None = None):
+        """statics::bodies::used_standing (bodies.rs:550-554): each bond's used fraction
+        of its strength with everything standing under the nodes' weights. The lattice
+        dict also carries m (n,) and ft, fc, fs (b,). Returns (used, info)."""
+        L, arr = _lattice_c(lattice)
+        S, keep = _strength_c(lattice)
+        used = np.zeros(max(L.n_bonds, 1))
+        info = SolveInfo()
+        s = lib().sc_used_standing(self.h, C.byref(L), C.byref(S), C.byref(opt or options()), _ptr(used),
+                                   C.byref(info))
+        self._check(s, "sc_used_standing", soft=(OK, MAXITER))
+        return used[:L.n_bonds], info.as_dict()
+
+    def settle(self, lattice: dict, opt: Options | None = None):
+        """statics::bodies::settle (bodies.rs:511-541): (fallen fraction of the free mass,
+        rounds, gone flags per node, info)."""
+        L, arr = _lattice_c(lattice)
+        S, keep = _strength_c(lattice)
+        gone = np.zeros(L.n_nodes, np.uint8)
+        out = SettleInfo()
+        s = lib().sc_settle(self.h, C.byref(L), C.byref(S), C.byref(opt or options()), _ptr(gone), C.byref(out))
+        self._check(s, "sc_settle", soft=(OK, MAXITER))
+        return out.fell, out.rounds, gone, dict(work=out.work, status=out.status)
+
+
+def _lattice_c(lattice: dict):
+    """The sc_lattice view of a lattice dict (and the arrays it points into)."""
+    nn = int(lattice["x"].shape[0])
+    nb = int(lattice["bi"].shape[0])
+    arr = {}
+    for key, dt in (("x", np.float64), ("held", np.uint8), ("around", np.int64), ("bi", np.int64),
+                    ("bj", np.int64), ("p", np.float64), ("n", np.float64), ("a", np.float64),
+                    ("d", np.float64), ("e", np.float64), ("g", np.float64)):
+        arr[key] = np.ascontiguousarray(lattice[key], dt)
+    L = LatticeC()
+    L.level, L.n_nodes, L.n_bonds = int(lattice.get("level", 0)), nn, nb
+    L.x, L.held, L.around = _ptr(arr["x"]), _ptr(arr["held"]), _ptr(arr["around"])
+    L.bond_i, L.bond_j, L.bond_p, L.bond_n = _ptr(arr["bi"]), _ptr(arr["bj"]), _ptr(arr["p"]), _ptr(arr["n"])
+    L.bond_a, L.bond_d, L.bond_e, L.bond_g = _ptr(arr["a"]), _ptr(arr["d"]), _ptr(arr["e"]), _ptr(arr["g"])
+    return L, arr
+
+
+def _strength_c(lattice: dict):
+    keep = {k: np.ascontiguousarray(lattice[k], np.float64) for k in ("m", "ft", "fc", "fs")}
+    S = Strength()
+    S.m, S.ft, S.fc, S.fs = (_ptr(keep[k]) for k in ("m", "ft", "fc", "fs"))
+    return S, keep
 
 
 _default: Solver | None = None
