@@ -469,7 +469,7 @@ def batch_section(solver, sc, rank, world, args):
     ms_1 = max_over_ranks(e0.elapsed_time(e1), world)
     batched = world * len(pieces) / (ms_b / 1000.0)
     single = world * len(sample) / (ms_1 / 1000.0)
-    bad = sum(1 for i in infos if i["status"] != 0 or i["residual"] > TOL * 1.0001)
+    bad = sum(1 for i in infos if not autotune.converged(i, TOL))
     retried = sum(1 for i in infos if i.get("retried"))
     groups = len({(settings[autotune.size_class(p[0])]["sweeps"], settings[autotune.size_class(p[0])]["tile"])
                   for p in pieces})
@@ -479,8 +479,9 @@ def batch_section(solver, sc, rank, world, args):
             "fp64_single_solves_per_s": single, "fp64_single_sample": len(sample),
             "speedup_batched_mixed_vs_fp64_single": batched / single,
             "mixed_batched_ms": ms_b, "iterations_mean": float(np.mean([i["iterations"] for i in infos])),
-            "pieces_not_converged": bad, "pieces_retried": retried, "batched_solves": groups, "autotune": {str(k): {"sweeps": v["sweeps"], "tile": v["tile"]}
-                                                       for k, v in settings.items()},
+            "pieces_not_converged": bad, "max_true_residual": max(i["residual"] for i in infos),
+            "pieces_retried": retried, "batched_solves": groups,
+            "autotune": {str(k): {"sweeps": v["sweeps"], "tile": v["tile"]} for k, v in settings.items()},
             "autotune_seconds": tune_s}
 
 

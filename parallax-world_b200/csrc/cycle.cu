@@ -305,7 +305,7 @@ template <class V, class S>
 __global__ void __launch_bounds__(256) k_axpy2(const int64_t* __restrict__ chunk_lo, const int32_t* __restrict__ cpiece,
                                                const int32_t* __restrict__ done, const double* __restrict__ alpha,
                                                S* __restrict__ x, const V* __restrict__ p, V* __restrict__ r,
-                                               const V* __restrict__ ap) {
+                                               const V* __restrict__ ap, float* __restrict__ r32) {
     int c = blockIdx.x;
     int pc = cpiece[c];
     if (done[pc]) return;
@@ -313,15 +313,17 @@ __global__ void __launch_bounds__(256) k_axpy2(const int64_t* __restrict__ chunk
     int64_t lo = 6 * chunk_lo[c], hi = 6 * chunk_lo[c + 1];
     for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         x[i] += (S)(a * (double)p[i]);
-        r[i] = (V)((double)r[i] - a * (double)ap[i]);
+        const V rn = (V)((double)r[i] - a * (double)ap[i]);
+        r[i] = rn;
+        if (r32) r32[i] = (float)rn;  // the FP32 V-cycle's input, written in the same pass
     }
 }
 
 // p = z + beta p (bodies.rs:365-369)
-template <class V>
+template <class V, class Z = V>
 __global__ void __launch_bounds__(256) k_pupdate(const int64_t* __restrict__ chunk_lo, const int32_t* __restrict__ cpiece,
                                                  const int32_t* __restrict__ done, const double* __restrict__ beta,
-                                                 V* __restrict__ p, const V* __restrict__ z) {
+                                                 V* __restrict__ p, const Z* __restrict__ z) {
     int c = blockIdx.x;
     int pc = cpiece[c];
     if (done[pc]) return;
@@ -331,10 +333,10 @@ __global__ void __launch_bounds__(256) k_pupdate(const int64_t* __restrict__ chu
 }
 
 // two dots in one pass: out_a = a.b, out_c = a.a
-template <class T>
+template <class T, class U = T>
 __global__ void __launch_bounds__(256) k_chunk_dot2(const int64_t* __restrict__ chunk_lo, const int32_t* __restrict__ cpiece,
                                                     const int32_t* __restrict__ done, const T* __restrict__ a,
-                                                    const T* __restrict__ b, double* __restrict__ pa,
+                                                    const U* __restrict__ b, double* __restrict__ pa,
                                                     double* __restrict__ pb) {
     int c = blockIdx.x;
     __shared__ double r1[256], r2[256];
@@ -448,16 +450,16 @@ static void ensure_partial(Context& ctx, const Level& L) {
 static void prepare_top(const Level&) {}
 
 // two chunked dots (a.b and a.a) per piece
-template <class T>
-static void dot2(Context& ctx, const Level& L, const int32_t* done, const T* a, const T* b, double* oab, double* oaa) {
+template <class T, class U = T>
+static void dot2(Context& ctx, const Level& L, const int32_t* done, const T* a, const U* b, double* oab, double* oaa) {
     int np = (int)L.pstart.size() - 1;
     if ((int64_t)ctx.partial.size() < 2 * std::max<int64_t>(L.nchunks, 1))
         ctx.partial.alloc(2 * (L.nchunks + 1024), ctx.stream, &ctx.mem);
     double* pa = ctx.partial.get();
     double* pb = pa + std::max<int64_t>(L.nchunks, 1);
     if (L.nchunks > 0) {
-        k_chunk_dot2<T><<<(unsigned)L.nchunks, 256, 0, ctx.stream>>>(L.chunk_lo.get(), L.chunk_piece.get(), done, a, b,
-                                                                    pa, pb);
+        k_chunk_dot2<T, U><<<(unsigned)L.nchunks, 256, 0, ctx.stream>>>(L.chunk_lo.get(), L.chunk_piece.get(), done, a,
+                                                                       b, pa, pb);
         SC_LAUNCH_CK();
     }
     k_piece_sum2<<<grid_for((int64_t)np * 32, 128), 128, 0, ctx.stream>>>(np, L.piece_chunk.get(), pa, pb, done, oab,
@@ -526,32 +528,38 @@ static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p,
     int np = b.npieces;
     int64_t n6 = 6 * L.n;
     constexpr bool same = std::is_same<V, P>::value;
-    // z = M r
+    static_assert(same || std::is_same<P, float>::value, "the preconditioner runs in V or in FP32");
+    // The preconditioned residual: z itself, or (FP32 cycle) zp, which the dots and the
+    // direction update read directly (no FP64 copy of z is made); rp, the cycle's input,
+    // is written by the residual update itself.
+    const P* zs = same ? reinterpret_cast<const P*>(z) : zp;
     auto precondition = [&]() {
-        if constexpr (same) {
+        if constexpr (same)
             cycle<V>(ctx, b, 0, r, z, cg.s.done);
-        } else {
-            if (L.nchunks > 0) {
-                k_cast_chunks<V, P><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(),
-                                                                          cg.s.done, r, rp);
-                SC_LAUNCH_CK();
-            }
+        else
             cycle<P>(ctx, b, 0, rp, zp, cg.s.done);
-            if (L.nchunks > 0) {
-                k_cast_chunks<P, V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(),
-                                                                          cg.s.done, zp, z);
-                SC_LAUNCH_CK();
-            }
-        }
     };
     SC_CK(cudaMemsetAsync(x, 0, n6 * sizeof(S), st));
     SC_CK(cudaMemcpyAsync(r, rhs, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
     dot2<V>(ctx, L, nullptr, rhs, rhs, cg.s.bb, nullptr);
     k_cg_init<<<grid_for(np, 128), 128, 0, st>>>(np, tol, cg.s, start_done);
     SC_LAUNCH_CK();
+    if constexpr (!same) {
+        if (L.nchunks > 0) {
+            k_cast_chunks<V, P><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(),
+                                                                      cg.s.done, r, rp);
+            SC_LAUNCH_CK();
+        }
+    }
     precondition();
-    SC_CK(cudaMemcpyAsync(p, z, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
-    dot2<V>(ctx, L, cg.s.done, r, z, cg.s.rz, cg.s.rr);
+    if constexpr (same) {
+        SC_CK(cudaMemcpyAsync(p, z, n6 * sizeof(V), cudaMemcpyDeviceToDevice, st));
+    } else if (L.nchunks > 0) {
+        k_cast_chunks<P, V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
+                                                                  zp, p);
+        SC_LAUNCH_CK();
+    }
+    dot2<V, P>(ctx, L, cg.s.done, r, zs, cg.s.rz, cg.s.rr);
     // one iteration (bodies.rs:351-371), ending with the next iteration's check
     auto body = [&]() {
         if (L.matrix_free) {
@@ -566,21 +574,22 @@ static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p,
         SC_LAUNCH_CK();
         if (L.nchunks > 0) {
             k_axpy2<V, S><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
-                                                              cg.s.alpha, x, p, r, ap);
+                                                              cg.s.alpha, x, p, r, ap,
+                                                              same ? nullptr : reinterpret_cast<float*>(rp));
             SC_LAUNCH_CK();
         }
         precondition();
-        dot2<V>(ctx, L, cg.s.done, r, z, cg.s.next, cg.s.rr);
+        dot2<V, P>(ctx, L, cg.s.done, r, zs, cg.s.next, cg.s.rr);
         if constexpr (same) {
             k_cg_beta<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.beta);
         } else {
-            dot2<V>(ctx, L, cg.s.done, ap, z, cg.zap, nullptr);
+            dot2<V, P>(ctx, L, cg.s.done, ap, zs, cg.zap, nullptr);
             k_cg_beta_flex<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, cg.zap, cg.beta);
         }
         SC_LAUNCH_CK();
         if (L.nchunks > 0) {
-            k_pupdate<V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
-                                                             cg.beta, p, z);
+            k_pupdate<V, P><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
+                                                                cg.beta, p, zs);
             SC_LAUNCH_CK();
         }
         SC_CK(cudaMemsetAsync(cg.ndone.get(), 0, sizeof(int32_t), st));
@@ -823,14 +832,14 @@ void pcg_fp32_cycle(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>&
     Level& L = b.levels[0];
     int64_t n6 = 6 * L.n;
     x.alloc(n6, ctx.stream, &ctx.mem);
-    DBuf<double> r, z, p, ap;
-    for (auto* v : {&r, &z, &p, &ap}) v->alloc(n6, ctx.stream, &ctx.mem);
+    DBuf<double> r, p, ap;  // the preconditioned residual stays FP32 (z32)
+    for (auto* v : {&r, &p, &ap}) v->alloc(n6, ctx.stream, &ctx.mem);
     DBuf<float> r32, z32;
     r32.alloc(n6, ctx.stream, &ctx.mem);
     z32.alloc(n6, ctx.stream, &ctx.mem);
     CgState cg;
     cg.init(ctx, b.npieces, b.status_d.get());
-    int64_t per_it = pcg<double, double, float>(ctx, b, b.loads.get(), x.get(), r.get(), z.get(), p.get(), ap.get(),
+    int64_t per_it = pcg<double, double, float>(ctx, b, b.loads.get(), x.get(), r.get(), nullptr, p.get(), ap.get(),
                                                 opt.tol, opt.max_iter, cg, opt.timeout_ms, t0, nullptr, r32.get(),
                                                 z32.get());
     std::vector<int64_t> it(b.npieces);
@@ -896,7 +905,7 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
         k_cg_alpha<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s);
         SC_LAUNCH_CK();
         chunks(k_axpy2<float, float>, (const int32_t*)cg.s.done, (const double*)cg.s.alpha, x32.get(),
-               (const float*)p.get(), r.get(), (const float*)ap.get());
+               (const float*)p.get(), r.get(), (const float*)ap.get(), (float*)nullptr);
     };
     // the FP64 update: fold x32 into x, r = b - K x in FP64, its verdict
     auto update = [&]() {
