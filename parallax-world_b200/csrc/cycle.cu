@@ -79,7 +79,7 @@ void level_apply(Context& ctx, const Batch& b, int l, const T* x, T* y) {
         stencil_apply<T>(ctx, b, x, y, nullptr, nullptr);
     else
         spmv<T>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, nullptr, y, nullptr, nullptr,
-                L.piece.get(), nullptr, nullptr);
+                L.piece.get(), nullptr, nullptr, L.nnzb);
 }
 template void level_apply<double>(Context&, const Batch&, int, const double*, double*);
 template void level_apply<float>(Context&, const Batch&, int, const float*, float*);
@@ -151,7 +151,7 @@ static void cycle(Context& ctx, Batch& b, int l, const T* r, T* z, const int32_t
             } else {
                 ProfScope ps(ctx, fam_of<T>(SC_FAM_SPMV64), spmv_bytes<T>(L, 3) + vb + 36.0 * sizeof(T) * L.n);
                 spmv<T>(ctx, SPMV_RES_SMOOTH, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, r, left, INV<T>(L),
-                        L.step.get(), L.piece.get(), skip, done);
+                        L.step.get(), L.piece.get(), skip, done, L.nnzb);
             }
             SC_CK(cudaMemcpyAsync(x, left, 6 * L.n * sizeof(T), cudaMemcpyDeviceToDevice, ctx.stream));
         }
@@ -161,21 +161,21 @@ static void cycle(Context& ctx, Batch& b, int l, const T* r, T* z, const int32_t
         } else {
             ProfScope ps(ctx, fam_of<T>(SC_FAM_SPMV64), spmv_bytes<T>(L, 3));
             spmv<T>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, r, left, nullptr, nullptr,
-                    L.piece.get(), skip, done);
+                    L.piece.get(), skip, done, L.nnzb);
         }
         Level& C = b.levels[l + 1];
         // coarse = P' left (bodies.rs:388-390)
         {
             ProfScope ps(ctx, fam_of<T>(SC_FAM_TRANSFER64), transfer_bytes<T>(L, C));
             spmv<T>(ctx, SPMV_Y, C.n, L.tptr.get(), L.trow.get(), PTVAL<T>(L), left, nullptr, VR<T>(C).get(),
-                    nullptr, nullptr, C.piece.get(), nullptr, done);
+                    nullptr, nullptr, C.piece.get(), nullptr, done, L.pnnz);
         }
         cycle<T>(ctx, b, l + 1, VR<T>(C).get(), VZ<T>(C).get(), done);
         // x += P y (bodies.rs:392-395)
         {
             ProfScope ps(ctx, fam_of<T>(SC_FAM_TRANSFER64), transfer_bytes<T>(L, C) + vb);
             spmv<T>(ctx, SPMV_ADD, L.n, L.prow.get(), L.pcol.get(), PVAL<T>(L), VZ<T>(C).get(), nullptr, x, nullptr,
-                    nullptr, L.piece.get(), skip, done);
+                    nullptr, L.piece.get(), skip, done, L.pnnz);
         }
         // z = x + step D^-1 (r - K x) (bodies.rs:396-401), after any further sweeps
         for (int sweep = 1; sweep < b.sweeps; sweep++) {
@@ -184,7 +184,7 @@ static void cycle(Context& ctx, Batch& b, int l, const T* r, T* z, const int32_t
             } else {
                 ProfScope ps(ctx, fam_of<T>(SC_FAM_SPMV64), spmv_bytes<T>(L, 3) + vb + 36.0 * sizeof(T) * L.n);
                 spmv<T>(ctx, SPMV_RES_SMOOTH, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, r, left, INV<T>(L),
-                        L.step.get(), L.piece.get(), skip, done);
+                        L.step.get(), L.piece.get(), skip, done, L.nnzb);
             }
             SC_CK(cudaMemcpyAsync(x, left, 6 * L.n * sizeof(T), cudaMemcpyDeviceToDevice, ctx.stream));
         }
@@ -195,7 +195,7 @@ static void cycle(Context& ctx, Batch& b, int l, const T* r, T* z, const int32_t
         } else {
             ProfScope ps(ctx, fam_of<T>(SC_FAM_SPMV64), spmv_bytes<T>(L, 3) + vb + 36.0 * sizeof(T) * L.n);
             spmv<T>(ctx, SPMV_RES_SMOOTH, L.n, L.rowptr.get(), L.col.get(), VAL<T>(L), x, r, z, INV<T>(L),
-                    L.step.get(), L.piece.get(), skip, done);
+                    L.step.get(), L.piece.get(), skip, done, L.nnzb);
         }
     }
     if (!L.top_h.empty()) {
@@ -567,7 +567,7 @@ static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p,
         } else {
             ProfScope ps(ctx, fam_of<V>(SC_FAM_SPMV64), spmv_bytes<V>(L, 2));
             spmv<V>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), VAL<V>(L), p, nullptr, ap, nullptr, nullptr,
-                    L.piece.get(), nullptr, cg.s.done);
+                    L.piece.get(), nullptr, cg.s.done, L.nnzb);
         }
         dot2<V>(ctx, L, cg.s.done, p, ap, cg.s.pap, nullptr);
         k_cg_alpha<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s);
@@ -694,7 +694,7 @@ static void true_residual(Context& ctx, Batch& b, const double* x, std::vector<d
         stencil_residual<double>(ctx, b, x, b.loads.get(), res.get(), nullptr, nullptr);
     else
         spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), x, b.loads.get(), res.get(),
-                     nullptr, nullptr, L.piece.get(), nullptr, nullptr);
+                     nullptr, nullptr, L.piece.get(), nullptr, nullptr, L.nnzb);
     dot2<double>(ctx, L, nullptr, res.get(), res.get(), nr.get(), nullptr);
     dot2<double>(ctx, L, nullptr, b.loads.get(), b.loads.get(), nr.get() + np, nullptr);
     std::vector<double> h = nr.to_host();
@@ -900,7 +900,7 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
             stencil_apply<float>(ctx, b, p.get(), ap.get(), nullptr, cg.s.done);
         else
             spmv<float>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), L.val32.get(), p.get(), nullptr, ap.get(),
-                        nullptr, nullptr, L.piece.get(), nullptr, cg.s.done);
+                        nullptr, nullptr, L.piece.get(), nullptr, cg.s.done, L.nnzb);
         dot2<float>(ctx, L, cg.s.done, p.get(), ap.get(), cg.s.pap, nullptr);
         k_cg_alpha<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s);
         SC_LAUNCH_CK();
@@ -916,7 +916,7 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
             stencil_residual<double>(ctx, b, x.get(), b.loads.get(), r64.get(), nullptr, skip.get());
         else
             spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), x.get(), b.loads.get(),
-                         r64.get(), nullptr, nullptr, L.piece.get(), nullptr, skip.get());
+                         r64.get(), nullptr, nullptr, L.piece.get(), nullptr, skip.get(), L.nnzb);
         dot2<double>(ctx, L, skip.get(), r64.get(), r64.get(), rr64.get(), nullptr);
         chunks(k_to32, (const int32_t*)skip.get(), (const double*)r64.get(), r.get());
         SC_CK(cudaMemsetAsync(counts.get(), 0, 2 * sizeof(int32_t), st));

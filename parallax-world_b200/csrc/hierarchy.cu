@@ -15,9 +15,11 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 
 #include "kernels.cuh"
 #include "level0_blocks.cuh"
+#include "rowprod.cuh"
 
 namespace sc {
 
@@ -396,92 +398,131 @@ __global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restr
 // Every output block of a product as the ordered sum of its contributions: after the
 // symbolic sort, output block q's contributions are vals[seg[q] .. seg[q+1]), each the
 // pair (a << 32 | b) of a left block and a right block, in the order the candidates were
-// generated (a stable sort), so the sum is deterministic. 36 threads per output block,
-// one per entry; the left operand transposed when TA.
+// generated (a stable sort), so the sum is deterministic. Every entry (r, c) is summed
+// over the contributions in list order, each contribution's six products first, as a
+// one-thread-per-entry sum would.
 constexpr int SUM_GROUPS = 32;  // output blocks per thread block, 6 threads each
 constexpr int SUM_THREADS = 6 * SUM_GROUPS;
 // out[q] = sum over q's contributions (a << 32 | b) of op(A_a) B_b, op = transpose when TA.
 // Six threads per output block, thread c owning its column c: each reads the whole left
 // block (the same addresses across the six, one transaction) and its column of the
 // right one, so a contribution costs 42 loads a thread instead of 12 for each of 36
-// threads. Every entry is summed over the contributions in list order, each
-// contribution's six products first, as a one-thread-per-entry sum would.
-// K0 (K P on a matrix-free level 0): A_a is block a of the level-0 pattern, made from the
-// cell template (krow gives its row); A is unused, and blocks stay resident, striding
-// over the outputs (the template is staged once per block).
-template <bool TA, bool K0>
+// threads.
+template <bool TA>
 __global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, const int64_t* __restrict__ seg,
                                                              const uint64_t* __restrict__ vals,
                                                              const double* __restrict__ A,
-                                                             const double* __restrict__ B, double* __restrict__ out,
-                                                             K0View k0, const int32_t* __restrict__ krow) {
-    __shared__ double T[K0 ? 36 * 36 : 1];
-    if (K0) {
-        for (int t = threadIdx.x; t < 36 * 36; t += blockDim.x) T[t] = k0.tpl_s[t];
-        __syncthreads();
-    }
+                                                             const double* __restrict__ B, double* __restrict__ out) {
     const int g = threadIdx.x / 6, c = threadIdx.x % 6;
-    for (int64_t q = (int64_t)blockIdx.x * SUM_GROUPS + g; q < nout; q += K0 ? (int64_t)gridDim.x * SUM_GROUPS : nout) {
-        int64_t i = seg[q];
-        const int64_t end = seg[q + 1];
+    const int64_t q = (int64_t)blockIdx.x * SUM_GROUPS + g;
+    if (q >= nout) return;
+    int64_t i = seg[q];
+    const int64_t end = seg[q + 1];
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    // one contribution's operands: column c of its right block and its left block
+    struct Ops {
+        double bc[6];
+        double av[36];
+    };
+    auto load = [&](uint64_t v, Ops& o) {
+        const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
+#pragma unroll
+        for (int j = 0; j < 6; j++) o.bc[j] = bb[j * 6 + c];
+        const double2* a2 = reinterpret_cast<const double2*>(A + 36 * (int64_t)(v >> 32));
+#pragma unroll
+        for (int t = 0; t < 18; t++) {
+            double2 w = a2[t];
+            o.av[2 * t] = w.x;
+            o.av[2 * t + 1] = w.y;
+        }
+    };
+    // acc(r) += sum_j op(A)(r, j) B(j, c)
+    auto add = [&](const Ops& o) {
+#pragma unroll
+        for (int r = 0; r < 6; r++) {
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; j++) s = fma(TA ? o.av[j * 6 + r] : o.av[r * 6 + j], o.bc[j], s);
+            acc[r] += s;
+        }
+    };
+    // two contributions' loads in flight, added in list order
+    for (; i + 2 <= end; i += 2) {
+        Ops o0, o1;
+        load(vals[i], o0);
+        load(vals[i + 1], o1);
+        add(o0);
+        add(o1);
+    }
+    if (i < end) {
+        Ops o0;
+        load(vals[i], o0);
+        add(o0);
+    }
+#pragma unroll
+    for (int r = 0; r < 6; r++) out[36 * q + 6 * r + c] = acc[r];
+}
+
+// The same for K P on a matrix-free level 0: the left block of contribution (e << 32 | f)
+// is block e of the level-0 pattern, made from the cell template (krow gives its row),
+// the right one block f of P. Thread c of a group owns column c of the output block as
+// above, but makes only row c of each template block and takes the other rows from its
+// group's lanes by shuffles, so the groups sit inside warps: five to a warp, two lanes
+// idle. Blocks stay resident, striding over the outputs (the template is staged once
+// per block).
+constexpr int K0SUM_WARPS = 6;
+constexpr int K0SUM_GROUPS = 5 * K0SUM_WARPS;
+__global__ void __launch_bounds__(32 * K0SUM_WARPS) k_sum_products_k0(int64_t nout, const int64_t* __restrict__ seg,
+                                                                     const uint64_t* __restrict__ vals,
+                                                                     const double* __restrict__ B,
+                                                                     double* __restrict__ out, K0View k0,
+                                                                     const int32_t* __restrict__ krow) {
+    __shared__ double T[36 * 36];
+    for (int t = threadIdx.x; t < 36 * 36; t += blockDim.x) T[t] = k0.tpl_s[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gl = min(lane / 6, 4), c = lane - 6 * gl;  // lanes 30, 31 shadow group 4's lanes 0, 1
+    const bool idle = lane >= 30;
+    const int base = 6 * gl;
+    const int g = 5 * warp + gl;
+    // the whole warp runs the same trip count, so the shuffles always find every lane
+    const int64_t first_q = (int64_t)blockIdx.x * K0SUM_GROUPS;
+    for (int64_t q0 = first_q; q0 < nout; q0 += (int64_t)gridDim.x * K0SUM_GROUPS) {
+        const int64_t q = q0 + g;
+        const bool live = !idle && q < nout;
+        int64_t i = live ? seg[q] : 0;
+        const int64_t end = live ? seg[q + 1] : 0;
         K0Row row{};
-        if (K0 && i < end) row = k0_row(k0, krow[vals[i] >> 32]);
+        if (i < end) row = k0_row(k0, krow[vals[i] >> 32]);
+        // the most contributions of any group of the warp
+        int64_t n = end - i, most = n;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) most = max(most, __shfl_xor_sync(0xffffffffu, most, o));
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        // one contribution's operands: column c of its right block, and its left block
-        // (or, K0, the block's template descriptor)
-        struct Ops {
-            double bc[6];
-            double av[K0 ? 1 : 36];
-            uint8_t d;
-        };
-        auto load = [&](uint64_t v, Ops& o) {
-            const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
+        for (int64_t t = 0; t < most; t++) {
+            const bool has = t < n;
+            double bc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, ar[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (has) {
+                const uint64_t v = vals[i + t];
+                const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
 #pragma unroll
-            for (int j = 0; j < 6; j++) o.bc[j] = bb[j * 6 + c];
-            if (K0) {
-                o.d = k0.desc[v >> 32];
-            } else {
-                const double2* a2 = reinterpret_cast<const double2*>(A + 36 * (int64_t)(v >> 32));
+                for (int j = 0; j < 6; j++) bc[j] = bb[j * 6 + c];
+                const uint8_t d = k0.desc[v >> 32];
 #pragma unroll
-                for (int t = 0; t < 18; t++) {
-                    double2 w = a2[t];
-                    o.av[2 * t] = w.x;
-                    o.av[2 * t + 1] = w.y;
-                }
+                for (int j = 0; j < 6; j++) ar[j] = k0_entry(T, row, d, c, j);  // row c of A
             }
-        };
-        // acc(r) += sum_j op(A)(r, j) B(j, c)
-        auto add = [&](const Ops& o) {
+            // acc(r) += sum_j A(r, j) B(j, c), row r of A from lane base + r
 #pragma unroll
             for (int r = 0; r < 6; r++) {
                 double s = 0.0;
 #pragma unroll
-                for (int j = 0; j < 6; j++) {
-                    double arj;
-                    if (K0)
-                        arj = k0_entry(T, row, o.d, r, j);
-                    else
-                        arj = TA ? o.av[j * 6 + r] : o.av[r * 6 + j];
-                    s = fma(arj, o.bc[j], s);
-                }
-                acc[r] += s;
+                for (int j = 0; j < 6; j++) s = fma(__shfl_sync(0xffffffffu, ar[j], base + r), bc[j], s);
+                if (has) acc[r] += s;
             }
-        };
-        // two contributions' loads in flight, added in list order
-        for (; i + 2 <= end; i += 2) {
-            Ops o0, o1;
-            load(vals[i], o0);
-            load(vals[i + 1], o1);
-            add(o0);
-            add(o1);
         }
-        if (i < end) {
-            Ops o0;
-            load(vals[i], o0);
-            add(o0);
-        }
+        if (live)
 #pragma unroll
-        for (int r = 0; r < 6; r++) out[36 * q + 6 * r + c] = acc[r];
+            for (int r = 0; r < 6; r++) out[36 * q + 6 * r + c] = acc[r];
     }
 }
 
@@ -1049,12 +1090,40 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         SC_LAUNCH_CK();
     }
     pt.mark("  prolongator");
+    // A product goes row by row (rowprod.cuh) when every piece's coarse level fits the
+    // bitmap window and B's rows are long enough to keep a block's 32 groups busy (eight
+    // blocks a row or more: levels 1 and up of voxel pieces), else through sorted
+    // candidate lists. Both give the same bits; SC_GALERKIN=sort or =rows forces one
+    // (rows only where the window fits).
+    int64_t widest = 0;
+    for (int p = 0; p < np; p++) widest = std::max<int64_t>(widest, C.pstart[p + 1] - C.pstart[p]);
+    const char* gal_env = std::getenv("SC_GALERKIN");
+    const std::string gal = gal_env ? gal_env : "";
+    const bool fits = widest <= ROWS_MAX_WIDTH && gal != "sort";
+    const bool by_rows = fits && (gal == "rows" || F.pnnz >= 8 * n);
     // --- K P
     DBuf<int64_t> kprow;
     DBuf<int32_t> kpcol;
     int64_t kpnnz = 0, kp_cands = 0, c_cands = 0;
     DBuf<double> kpval;
-    {
+    if (by_rows) {
+        DBuf<int32_t> lo, hi;
+        lo.alloc(n, st, ms);
+        hi.alloc(n, st, ms);
+        kp_windows(ctx, n, F.up.get(), F.prow.get(), F.pcol.get(), F.piece.get(), C.pstart_d.get(), lo.get(), hi.get());
+        RowArgs a{};
+        a.arow = F.rowptr.get();
+        a.acol = F.col.get();
+        a.aval = virt ? nullptr : F.val.get();
+        a.k0 = k0;
+        a.annz = F.nnzb;
+        a.brow = F.prow.get();
+        a.bcol = F.pcol.get();
+        a.bval = F.pval.get();
+        a.lo = lo.get();
+        a.hi = hi.get();
+        row_products(ctx, virt ? ROWS_K0 : ROWS_PLAIN, a, n, widest, kprow, kpcol, kpval, kpnnz, kp_cands);
+    } else {
         // one thread per block of K (its row from krow), offsets by a scan over K's entries
         const int64_t knz = F.nnzb;
         DBuf<int32_t> krow;
@@ -1089,11 +1158,12 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         if (kpnnz > 0) {
             unsigned nb = (unsigned)((kpnnz + SUM_GROUPS - 1) / SUM_GROUPS);
             if (virt)
-                k_sum_products<false, true><<<std::min(nb, 148u * 8u), SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(), nullptr,
-                                                                            F.pval.get(), kpval.get(), k0, krow.get());
+                k_sum_products_k0<<<std::min((unsigned)((kpnnz + K0SUM_GROUPS - 1) / K0SUM_GROUPS), 148u * 8u),
+                                    32 * K0SUM_WARPS, 0, st>>>(kpnnz, seg.get(), vals.get(), F.pval.get(),
+                                                               kpval.get(), k0, krow.get());
             else
-                k_sum_products<false, false><<<nb, SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(), F.val.get(),
-                                                                             F.pval.get(), kpval.get(), k0, nullptr);
+                k_sum_products<false><<<nb, SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(), F.val.get(),
+                                                                  F.pval.get(), kpval.get());
             SC_LAUNCH_CK();
         }
     }
@@ -1103,7 +1173,25 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     DBuf<int32_t> ucol;
     DBuf<double> uval;
     int64_t unnz = 0;
-    {
+    // the upper product's rows see about half of each K P row
+    if (fits && (gal == "rows" || kpnnz >= 12 * n)) {
+        DBuf<int32_t> lo, hi;
+        lo.alloc(nc, st, ms);
+        hi.alloc(nc, st, ms);
+        upper_windows(ctx, nc, C.piece.get(), C.pstart_d.get(), lo.get(), hi.get());
+        RowArgs a{};
+        a.arow = F.tptr.get();
+        a.acol = F.trow.get();
+        a.aent = F.tent.get();
+        a.aval = F.pval.get();
+        a.annz = F.pnnz;
+        a.brow = kprow.get();
+        a.bcol = kpcol.get();
+        a.bval = kpval.get();
+        a.lo = lo.get();
+        a.hi = hi.get();
+        row_products(ctx, ROWS_TRANSPOSED, a, nc, widest, urow, ucol, uval, unnz, c_cands);
+    } else {
         DBuf<int64_t> ecnt, eoff;
         ecnt.alloc(F.pnnz + 1, st, ms);
         eoff.alloc(F.pnnz + 1, st, ms);
@@ -1129,8 +1217,8 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         keys_to_csr_with(ctx, keys, vin, tot, nc, nc, urow, ucol, unnz, seg, vals);
         uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
         if (unnz > 0) {
-            k_sum_products<true, false><<<(unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS), SUM_THREADS, 0, st>>>(
-                unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get(), K0View{}, nullptr);
+            k_sum_products<true><<<(unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS), SUM_THREADS, 0, st>>>(
+                unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get());
             SC_LAUNCH_CK();
         }
     }

@@ -75,6 +75,81 @@ __global__ void __launch_bounds__(256) k_spmv(int64_t nrows, const int64_t* __re
     }
 }
 
+// The same with each row split over WPR warps, for levels of few, long rows (coarse
+// levels and their transfers), where one warp a row leaves the device idle. Warp w of a
+// row takes its blocks e0 + 4 w + g, then every 4 WPR, two in flight; the warps' partial
+// sums meet in shared memory and are added in warp order (a fixed order).
+template <class T, int MODE, int WPR>
+__global__ void __launch_bounds__(32 * (WPR > 8 ? WPR : 8)) k_spmv_split(
+    int64_t nrows, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col, const T* __restrict__ val,
+    const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y, const T* __restrict__ inv,
+    const double* __restrict__ step, const int32_t* __restrict__ piece, const int32_t* __restrict__ skip_row,
+    const int32_t* __restrict__ done) {
+    constexpr int RPC = WPR >= 8 ? 1 : 8 / WPR;  // rows per thread block
+    constexpr int STRIDE = 4 * WPR;
+    __shared__ T part[RPC * WPR][6];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wr = warp % WPR;
+    const int64_t row = (int64_t)blockIdx.x * RPC + warp / WPR;
+    bool active = row < nrows && !(skip_row && skip_row[row]);
+    const int p = active && piece ? piece[row] : 0;
+    if (active && done && done[p]) active = false;
+    const int g = lane >> 3, rr = lane & 7;
+    T acc = T(0);
+    if (active && rr < 6) {
+        const int64_t e1 = rowptr[row + 1];
+        int64_t e = rowptr[row] + 4 * wr + g;
+        for (; e + STRIDE < e1; e += 2 * STRIDE) {
+            int32_t j0 = col[e], j1 = col[e + STRIDE];
+            T a0[6], x0[6], a1[6], x1[6];
+            ld6<T>(val + 36 * e + 6 * rr, a0);
+            ld6<T>(val + 36 * (e + STRIDE) + 6 * rr, a1);
+            ld6<T>(x + 6 * (int64_t)j0, x0);
+            ld6<T>(x + 6 * (int64_t)j1, x1);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a0[c], x0[c], acc);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a1[c], x1[c], acc);
+        }
+        if (e < e1) {
+            int32_t j = col[e];
+            T a[6], xv[6];
+            ld6<T>(val + 36 * e + 6 * rr, a);
+            ld6<T>(x + 6 * (int64_t)j, xv);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a[c], xv[c], acc);
+        }
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+    if (lane < 6) part[warp][lane] = acc;
+    __syncthreads();
+    if (!active || wr != 0) return;  // whole warps
+    acc = T(0);
+    if (lane < 6)
+#pragma unroll
+        for (int w = 0; w < WPR; w++) acc += part[warp + w][lane];
+    if (MODE == SPMV_Y) {
+        if (lane < 6) y[6 * row + lane] = acc;
+    } else if (MODE == SPMV_ADD) {
+        if (lane < 6) y[6 * row + lane] += acc;
+    } else if (MODE == SPMV_RES) {
+        if (lane < 6) y[6 * row + lane] = r[6 * row + lane] - acc;
+    } else {
+        T left = (lane < 6) ? r[6 * row + lane] - acc : T(0);
+        T l6[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) l6[c] = __shfl_sync(0xffffffffu, left, c);
+        if (lane < 6) {
+            const T* d = inv + 36 * row + 6 * lane;
+            T s = T(0);
+#pragma unroll
+            for (int c = 0; c < 6; c++) s = fma(d[c], l6[c], s);
+            y[6 * row + lane] = x[6 * row + lane] + (T)step[p] * s;
+        }
+    }
+}
+
 template <class T>
 __global__ void k_jacobi(int64_t n, const T* __restrict__ inv, const T* __restrict__ r, T* __restrict__ x,
                          const double* __restrict__ step, const int32_t* __restrict__ piece,
@@ -204,11 +279,63 @@ __global__ void k_piece_sum(int np, const int64_t* __restrict__ piece_chunk, con
 
 }  // namespace
 
+template <class T, int WPR>
+void launch_split(Context& ctx, int mode, int64_t nrows, const int64_t* rowptr, const int32_t* col, const T* val,
+                  const T* x, const T* r, T* y, const T* inv, const double* step, const int32_t* piece,
+                  const int32_t* skip_row, const int32_t* done) {
+    constexpr int RPC = WPR >= 8 ? 1 : 8 / WPR;
+    constexpr int threads = 32 * (WPR > 8 ? WPR : 8);
+    const unsigned g = grid_for(nrows, RPC);
+    switch (mode) {
+        case SPMV_Y:
+            k_spmv_split<T, SPMV_Y, WPR><<<g, threads, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv, step,
+                                                                         piece, skip_row, done);
+            break;
+        case SPMV_ADD:
+            k_spmv_split<T, SPMV_ADD, WPR><<<g, threads, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv, step,
+                                                                           piece, skip_row, done);
+            break;
+        case SPMV_RES:
+            k_spmv_split<T, SPMV_RES, WPR><<<g, threads, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv, step,
+                                                                           piece, skip_row, done);
+            break;
+        default:
+            k_spmv_split<T, SPMV_RES_SMOOTH, WPR><<<g, threads, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv,
+                                                                                  step, piece, skip_row, done);
+    }
+    SC_LAUNCH_CK();
+}
+
+// Warps a row: one, unless the rows are too few to fill the device twice over and each
+// warp would still stream 16 or more blocks (doubling up to 32).
+static int warps_per_row(int64_t nrows, int64_t nnz) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        SC_CK(cudaGetDevice(&dev));
+        SC_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int64_t target = (int64_t)sms * 64;  // two waves of 32 warps an SM
+    const int64_t avg = nnz / std::max<int64_t>(nrows, 1);
+    int w = 1;
+    while (w < 32 && nrows * w < target && avg >= 32 * w) w *= 2;
+    return w;
+}
+
 template <class T>
 void spmv(Context& ctx, int mode, int64_t nrows, const int64_t* rowptr, const int32_t* col, const T* val, const T* x,
           const T* r, T* y, const T* inv, const double* step, const int32_t* piece, const int32_t* skip_row,
-          const int32_t* done) {
+          const int32_t* done, int64_t nnz) {
     if (nrows <= 0) return;
+    const int wpr = nnz > 0 ? warps_per_row(nrows, nnz) : 1;
+    switch (wpr) {
+        case 2: return launch_split<T, 2>(ctx, mode, nrows, rowptr, col, val, x, r, y, inv, step, piece, skip_row, done);
+        case 4: return launch_split<T, 4>(ctx, mode, nrows, rowptr, col, val, x, r, y, inv, step, piece, skip_row, done);
+        case 8: return launch_split<T, 8>(ctx, mode, nrows, rowptr, col, val, x, r, y, inv, step, piece, skip_row, done);
+        case 16: return launch_split<T, 16>(ctx, mode, nrows, rowptr, col, val, x, r, y, inv, step, piece, skip_row, done);
+        case 32: return launch_split<T, 32>(ctx, mode, nrows, rowptr, col, val, x, r, y, inv, step, piece, skip_row, done);
+        default: break;
+    }
     unsigned g = grid_for(nrows * 32, 256);
     switch (mode) {
         case SPMV_Y:
@@ -283,7 +410,7 @@ void seg_dot(Context& ctx, const Level& L, const double* a, const double* b, dou
 
 #define SC_INST(T)                                                                                                 \
     template void spmv<T>(Context&, int, int64_t, const int64_t*, const int32_t*, const T*, const T*, const T*, T*, \
-                          const T*, const double*, const int32_t*, const int32_t*, const int32_t*);                \
+                          const T*, const double*, const int32_t*, const int32_t*, const int32_t*, int64_t);       \
     template void jacobi<T>(Context&, int64_t, const T*, const T*, T*, const double*, const int32_t*,              \
                             const int32_t*, const int32_t*);                                                       \
     template void jacobi_add<T>(Context&, int64_t, const T*, const T*, const T*, T*, const double*, const int32_t*, \

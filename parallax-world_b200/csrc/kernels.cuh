@@ -46,10 +46,11 @@ __device__ __forceinline__ void st6(T* __restrict__ p, const T (&o)[6]) {
 }
 
 // Host launchers (kernels.cu).
+// nnz (the stored blocks) picks the warps a row (one when 0); see warps_per_row.
 template <class T>
 void spmv(Context& ctx, int mode, int64_t nrows, const int64_t* rowptr, const int32_t* col, const T* val, const T* x,
           const T* r, T* y, const T* inv, const double* step, const int32_t* piece, const int32_t* skip_row,
-          const int32_t* done);
+          const int32_t* done, int64_t nnz = 0);
 template <class T>
 void jacobi(Context& ctx, int64_t n, const T* inv, const T* r, T* x, const double* step, const int32_t* piece,
             const int32_t* skip_row, const int32_t* done);

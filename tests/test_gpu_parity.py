@@ -178,6 +178,36 @@ def test_batch_mixed(solver):
         assert rel(u, u_ref) < DISP_TOL
 
 
+@pytest.mark.parametrize("env", [{}, {"SC_GALERKIN": "rows"},
+                                 {"SC_GALERKIN": "rows", "SC_ROWS_SLOTS": "3", "SC_ROWS_META": "5"}],
+                         ids=["default", "rows", "rows-tiled"])
+def test_galerkin_rows_match_sorted(solver, monkeypatch, env):
+    """The row-by-row Galerkin products (pieces with at most 65536 coarse parts a level)
+    and the sorted-candidate ones add the same products in the same order: the same
+    bits, for a single piece and a batch, with the default choice per product and with
+    every product row by row (level 0's K P then reads the cell template). Tiles of 3
+    output blocks and 5 staged entries split a row over many blocks and walk it often."""
+    opts = sc.options(max_iter=5000, tol=1e-8)
+    st, k = piece(0, 11, shape=(40, 28, 36))
+    batch = [piece(0, 300 + i, shape=(16 + 8 * (i % 3), 24, 20)) for i in range(4)]
+    for name, v in env.items():
+        monkeypatch.setenv(name, v)
+    u_rows, i_rows = solver.solve_grid(st, k, opts)
+    b_rows, bi_rows = solver.solve_grid_batch(batch, opts)
+    for name in env:
+        monkeypatch.delenv(name)
+    monkeypatch.setenv("SC_GALERKIN", "sort")
+    u_sort, i_sort = solver.solve_grid(st, k, opts)
+    b_sort, bi_sort = solver.solve_grid_batch(batch, opts)
+    assert i_rows["status"] == sc.OK
+    assert i_rows["iterations"] == i_sort["iterations"]
+    assert i_rows["steps"] == i_sort["steps"]
+    assert np.array_equal(u_rows, u_sort)
+    for a, b, ia, ib in zip(b_rows, b_sort, bi_rows, bi_sort):
+        assert ia["iterations"] == ib["iterations"]
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("tile", [1, 2, 32, 4096])
 @pytest.mark.parametrize("precision", [sc.FP64, sc.MIXED], ids=["fp64", "mixed"])
 def test_stencil_variants(solver, tile, precision):
