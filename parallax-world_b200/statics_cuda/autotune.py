@@ -1,19 +1,22 @@
 """Autotuner for batched solves of voxel pieces.
 
-Pieces are put in size classes (their grid cells rounded up to a power of two). For
-each class it times a batched solve (setup + PCG to the requested tolerance, as the
-batch will run) of up to SAMPLES of its pieces under every candidate setting --
+A batch iterates until its slowest piece converges (converged pieces skip their work but
+ride along), so the setting that matters is the one for the batch as a whole, and one
+batch beats several: per-size-class settings would split the batch into one solve per
+setting, each as slow as its worst member. So the tuner times a batched solve (setup +
+PCG to the requested tolerance, as the batch will run) of a sample of the batch -- up to
+SAMPLES pieces spread evenly over its size range -- under every candidate setting:
 block-Jacobi sweeps before and after each coarse correction (the reference does one,
-statics/src/bodies.rs:386, 396-401) and the stencil tile (the window of parts grouped
-by axis) -- and keeps the fastest setting that solved every sample. A batch iterates
-until its slowest piece converges, so timing single pieces misjudges a setting: two
-sweeps per level cut the mean iteration count but can leave a straggler (the damped-
-Jacobi step 4/(3 lambda_max) is the reference's choice for one sweep; on some pieces
-two sweeps lose definiteness and CG stalls), so a setting counts only if all its
-samples converge within TRIAL_MAX_ITER iterations. Choices are
-cached in a JSON file keyed by class, precision and tolerance, so a later batch of the
-same classes is not tuned again. A piece that still fails in the batched solve is
-solved again alone with the reference's one sweep (its info then says retried).
+statics/src/bodies.rs:386, 396-401) and the stencil tile (the window of parts grouped by
+axis). It keeps the fastest setting that solved every sample: two sweeps per level cut
+the mean iteration count but can leave a straggler (the damped-Jacobi step 4/(3
+lambda_max) is the reference's choice for one sweep; on some pieces two sweeps lose
+definiteness and CG stalls), so a setting counts only if all its samples converge within
+TRIAL_MAX_ITER iterations. Choices are cached in a JSON file keyed by the batch's size
+classes, precision and tolerance, so a later batch of the same classes is not tuned
+again. A piece that fails in the batched solve under a setting other than the
+reference's is solved again alone with the reference's one sweep (its info then says
+retried).
 """
 from __future__ import annotations
 
@@ -25,7 +28,7 @@ from . import FP64, MIXED, Solver, options
 
 SWEEPS = (1, 2)
 TILES = (256, 1024, 4096)
-SAMPLES = 8
+SAMPLES = 32
 TRIAL_MAX_ITER = 2000
 MAX_ITER = 20000
 FALLBACK = {"sweeps": 1, "tile": 0}
@@ -46,8 +49,17 @@ def size_class(state) -> int:
     return c
 
 
-def _key(cls: int, precision: int, tol: float) -> str:
-    return f"batch:{cls}:{precision}:{tol:g}"
+def _key(classes, precision: int, tol: float) -> str:
+    return "batch:" + "-".join(str(c) for c in sorted(set(classes))) + f":{precision}:{tol:g}"
+
+
+def sample(pieces, count: int = SAMPLES) -> list:
+    """Up to `count` of `pieces`, spread evenly over them in order of size."""
+    order = sorted(range(len(pieces)), key=lambda i: int(pieces[i][0].size))
+    if len(order) <= count:
+        return [pieces[i] for i in order]
+    step = (len(order) - 1) / (count - 1)
+    return [pieces[order[round(j * step)]] for j in range(count)]
 
 
 def load(path: str = DEFAULT_CACHE) -> dict:
@@ -65,7 +77,7 @@ def save(cache: dict, path: str = DEFAULT_CACHE) -> None:
     os.replace(tmp, path)
 
 
-def tune_class(solver: Solver, samples, precision: int = MIXED, tol: float = 1e-8, repeats: int = 2) -> dict:
+def tune(solver: Solver, samples, precision: int = MIXED, tol: float = 1e-8, repeats: int = 2) -> dict:
     """Times a batched solve of the sample pieces under every (sweeps, tile); returns the
     fastest setting that solved all of them, with the timings (the reference's setting if
     none did)."""
@@ -79,7 +91,7 @@ def tune_class(solver: Solver, samples, precision: int = MIXED, tol: float = 1e-
                 _, infos = solver.solve_grid_batch(samples, opt)
                 dt = time.perf_counter() - t
                 iters = [i["iterations"] for i in infos]
-                if any(not converged(i, tol) for i in infos):
+                if any(i["status"] != 0 for i in infos):
                     dt = float("inf")
                     best = dt
                     break
@@ -93,45 +105,31 @@ def tune_class(solver: Solver, samples, precision: int = MIXED, tol: float = 1e-
 
 
 def choose(solver: Solver, pieces, precision: int = MIXED, tol: float = 1e-8, path: str = DEFAULT_CACHE) -> dict:
-    """The setting for each size class present in `pieces` (tuning the classes the cache
-    lacks on up to SAMPLES of their pieces). Returns {class: {"sweeps": s, "tile": t, ...}}."""
+    """The setting for a batch of `pieces` (tuned on a sample of them unless the cache has
+    one for the same size classes). Returns {"sweeps": s, "tile": t, ...}."""
     cache = load(path)
-    classes: dict[int, list] = {}
-    for piece in pieces:
-        classes.setdefault(size_class(piece[0]), []).append(piece)
-    out, changed = {}, False
-    for cls, members in classes.items():
-        key = _key(cls, precision, tol)
-        if key not in cache:
-            cache[key] = tune_class(solver, members[:SAMPLES], precision, tol)
-            changed = True
-        out[cls] = cache[key]
-    if changed:
+    key = _key([size_class(p[0]) for p in pieces], precision, tol)
+    if key not in cache:
+        cache[key] = tune(solver, sample(pieces), precision, tol)
         save(cache, path)
-    return out
+    return cache[key]
 
 
 def solve_batch(solver: Solver, pieces, precision: int = MIXED, tol: float = 1e-8, path: str = DEFAULT_CACHE,
-                settings: dict | None = None):
-    """Solves `pieces` with their size classes' tuned settings: the pieces that share a
-    setting form one batched solve (fewer, larger batches than one per class); a piece
-    that did not converge is solved again alone with the reference's setting. Returns
-    (motions, infos) in the order of `pieces`."""
-    settings = settings or choose(solver, pieces, precision, tol, path)
-    groups: dict[tuple, list[int]] = {}
-    for i, p in enumerate(pieces):
-        s = settings.get(size_class(p[0]), FALLBACK)
-        groups.setdefault((s["sweeps"], s["tile"]), []).append(i)
-    motions, infos = [None] * len(pieces), [None] * len(pieces)
-    for (sweeps, tile), idx in groups.items():
-        opt = options(tol=tol, precision=precision, sweeps=sweeps, tile=tile, max_iter=MAX_ITER)
-        outs, inf = solver.solve_grid_batch([pieces[i] for i in idx], opt)
-        for j, i in enumerate(idx):
-            motions[i], infos[i] = outs[j], inf[j]
-    fallback = options(tol=tol, precision=precision, sweeps=FALLBACK["sweeps"], tile=FALLBACK["tile"],
-                       max_iter=MAX_ITER)
-    for i, info in enumerate(infos):
-        if not converged(info, tol):
-            motions[i], infos[i] = solver.solve_grid(*pieces[i], fallback)
-            infos[i]["retried"] = True
+                setting: dict | None = None):
+    """Solves `pieces` in one batched solve with the batch's tuned setting; a piece that
+    failed (a status other than OK) under a setting other than the reference's is solved
+    again alone with the reference's setting. Returns (motions, infos) in the order of
+    `pieces`."""
+    setting = setting or choose(solver, pieces, precision, tol, path)
+    opt = options(tol=tol, precision=precision, sweeps=setting["sweeps"], tile=setting["tile"], max_iter=MAX_ITER)
+    motions, infos = solver.solve_grid_batch(pieces, opt)
+    motions, infos = list(motions), list(infos)
+    if (setting["sweeps"], setting["tile"]) != (FALLBACK["sweeps"], FALLBACK["tile"]):
+        fallback = options(tol=tol, precision=precision, sweeps=FALLBACK["sweeps"], tile=FALLBACK["tile"],
+                           max_iter=MAX_ITER)
+        for i, info in enumerate(infos):
+            if info["status"] != 0:
+                motions[i], infos[i] = solver.solve_grid(*pieces[i], fallback)
+                infos[i]["retried"] = True
     return motions, infos
