@@ -388,25 +388,35 @@ const char* sc_last_error(const sc_context* ctx) { return ctx ? ctx->c.last_erro
 sc_status sc_grid_count(const sc_grid* g, int64_t* n_nodes, int64_t* n_parts) {
     if (!g || !n_nodes || !n_parts || g->on_device) return SC_BAD_INPUT;
     if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || !g->state) return SC_BAD_INPUT;
+    // the reference's node creation (lattice.rs:124-163): a free cell's + faces are new, a
+    // - face is new unless the cell before it on that axis is free; a node is held when
+    // its other cell is held. Rows along z, the four neighbouring rows by pointer.
     const int nx = g->nx, ny = g->ny, nz = g->nz;
-    auto st = [&](int x, int y, int z) -> int {
-        if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return SC_CELL_EMPTY;
-        return g->state[((int64_t)x * ny + y) * nz + z];
-    };
+    const int64_t syz = (int64_t)ny * nz;
     int64_t nodes = 0, held = 0;
+    auto face = [&](int other, bool plus) {
+        if (plus || other != SC_CELL_FREE) {
+            nodes++;
+            held += other == SC_CELL_HELD;
+        }
+    };
     for (int x = 0; x < nx; x++)
-        for (int y = 0; y < ny; y++)
+        for (int y = 0; y < ny; y++) {
+            const uint8_t* row = g->state + ((int64_t)x * ny + y) * nz;
+            const uint8_t* xm = x > 0 ? row - syz : nullptr;
+            const uint8_t* xp = x + 1 < nx ? row + syz : nullptr;
+            const uint8_t* ym = y > 0 ? row - nz : nullptr;
+            const uint8_t* yp = y + 1 < ny ? row + nz : nullptr;
             for (int z = 0; z < nz; z++) {
-                if (st(x, y, z) != SC_CELL_FREE) continue;
-                int o[6][3] = {{x - 1, y, z}, {x + 1, y, z}, {x, y - 1, z}, {x, y + 1, z}, {x, y, z - 1}, {x, y, z + 1}};
-                for (int s = 0; s < 6; s++) {
-                    int other = st(o[s][0], o[s][1], o[s][2]);
-                    bool is_new = (s & 1) || other != SC_CELL_FREE;
-                    if (!is_new) continue;
-                    nodes++;
-                    if (other == SC_CELL_HELD) held++;
-                }
+                if (row[z] != SC_CELL_FREE) continue;
+                face(xm ? xm[z] : SC_CELL_EMPTY, false);
+                face(xp ? xp[z] : SC_CELL_EMPTY, true);
+                face(ym ? ym[z] : SC_CELL_EMPTY, false);
+                face(yp ? yp[z] : SC_CELL_EMPTY, true);
+                face(z > 0 ? row[z - 1] : SC_CELL_EMPTY, false);
+                face(z + 1 < nz ? row[z + 1] : SC_CELL_EMPTY, true);
             }
+        }
     *n_nodes = nodes;
     *n_parts = nodes - held;
     return SC_OK;
