@@ -26,8 +26,8 @@ namespace sc {
 
 namespace {
 
-constexpr int RP_THREADS = 192;
-constexpr int RP_GROUPS = RP_THREADS / 6;
+constexpr int RP_THREADS = 192;  // the count kernel's threads; the fill kernel's for long B rows
+constexpr int RP_SMALL = 64;     // the fill kernel's threads where B rows are short
 constexpr int RP_META = 256;  // A entries staged at a time (SC_ROWS_META lowers it)
 
 // The staged A entries of a segment: the first B entry inside the window, the count
@@ -39,17 +39,18 @@ struct Meta {
     int* pos;
     int64_t* ent;
 };
-using MetaScan = cub::BlockScan<int, RP_THREADS>;
+template <int TH>
+using MetaScan = cub::BlockScan<int, TH>;
 
-// Stages A entries [s0, s0 + nm) (nm <= 2 * RP_THREADS) in M -- thread t takes entries
+// Stages A entries [s0, s0 + nm) (nm <= 2 * TH) in M -- thread t takes entries
 // 2t and 2t + 1, reading their first B entry from `first`, or, SEARCH, finding it by a
 // binary search and storing it in `found` -- then sets the window bits of every B entry
 // from there on, the candidates split evenly over the threads with four loads in flight.
 // Returns the segment's candidates (block-uniform).
-template <bool SEARCH, int MODE>
+template <bool SEARCH, int MODE, int TH>
 __device__ int stage_and_mark(const RowArgs& a, int64_t s0, int nm, int32_t l, int32_t h,
                               const int64_t* __restrict__ first, int64_t* __restrict__ found, const Meta& M,
-                              uint32_t* bm, typename MetaScan::TempStorage& tmp) {
+                              uint32_t* bm, typename MetaScan<TH>::TempStorage& tmp) {
     int len[2] = {0, 0};
 #pragma unroll
     for (int u = 0; u < 2; u++) {
@@ -72,13 +73,13 @@ __device__ int stage_and_mark(const RowArgs& a, int64_t s0, int nm, int32_t l, i
         }
     }
     int pos[2], total;
-    MetaScan(tmp).ExclusiveSum(len, pos, total);
+    MetaScan<TH>(tmp).ExclusiveSum(len, pos, total);
 #pragma unroll
     for (int u = 0; u < 2; u++)
         if (2 * (int)threadIdx.x + u < nm) M.pos[2 * threadIdx.x + u] = pos[u];
     if (threadIdx.x == 0) M.pos[nm] = total;
     __syncthreads();
-    const int per = (total + RP_THREADS - 1) / RP_THREADS;
+    const int per = (total + TH - 1) / TH;
     int idx = min(total, (int)threadIdx.x * per);
     const int iend = min(total, idx + per);
     if (idx < iend) {
@@ -130,7 +131,7 @@ __global__ void __launch_bounds__(RP_THREADS) k_rows_count(int64_t nrows, RowArg
     using Reduce = cub::BlockReduce<int64_t, RP_THREADS>;
     __shared__ union {
         typename Reduce::TempStorage red;
-        typename MetaScan::TempStorage scan;
+        typename MetaScan<RP_THREADS>::TempStorage scan;
     } tmp;
     const Meta M{cmeta, reinterpret_cast<int*>(cmeta + RP_META), reinterpret_cast<int*>(cmeta + RP_META) + RP_META,
                  nullptr};
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(RP_THREADS) k_rows_count(int64_t nrows, RowArg
     if (nw > 0) {
         const int64_t e0 = a.arow[i], e1 = a.arow[i + 1];
         for (int64_t s0 = e0; s0 < e1; s0 += RP_META)
-            mine += stage_and_mark<true, ROWS_PLAIN>(a, s0, (int)min((int64_t)RP_META, e1 - s0), l, h, nullptr,
+            mine += stage_and_mark<true, ROWS_PLAIN, RP_THREADS>(a, s0, (int)min((int64_t)RP_META, e1 - s0), l, h, nullptr,
                                                      first, M, bm, tmp.scan);
     }
     int64_t n = 0;
@@ -181,13 +182,14 @@ struct BEntry {
     double b[6];
 };
 
-template <int MODE>
-__global__ void __launch_bounds__(RP_THREADS, 2) k_rows_fill(int64_t nrows, RowArgs a, const int64_t* __restrict__ first,
+template <int MODE, int TH>
+__global__ void __launch_bounds__(TH, TH == RP_THREADS ? 2 : 6) k_rows_fill(int64_t nrows, RowArgs a, const int64_t* __restrict__ first,
                                                            const int64_t* __restrict__ crow,
                                                            int32_t* __restrict__ ccol, double* __restrict__ cval,
                                                            int S, int nwmax, int meta) {
     extern __shared__ double smem[];
-    __shared__ typename MetaScan::TempStorage scan;
+    constexpr int NG = TH / 6;  // groups of six threads
+    __shared__ typename MetaScan<TH>::TempStorage scan;
     double* acc = smem;                                             // S blocks
     double* T = acc + (size_t)S * 36;                               // K0: the scaled template
     double* Ast = T + (MODE == ROWS_K0 ? 36 * 36 : 0);              // two staged A blocks
@@ -207,20 +209,20 @@ __global__ void __launch_bounds__(RP_THREADS, 2) k_rows_fill(int64_t nrows, RowA
     const int t1 = min(nslots, t0 + S);
     const int nw = (h - l + 31) >> 5;
     if constexpr (MODE == ROWS_K0)
-        for (int t = threadIdx.x; t < 36 * 36; t += RP_THREADS) T[t] = a.k0.tpl_s[t];
-    for (int w = threadIdx.x; w < nw; w += RP_THREADS) bm[w] = 0u;
-    for (int x = threadIdx.x; x < S * 36; x += RP_THREADS) acc[x] = 0.0;
+        for (int t = threadIdx.x; t < 36 * 36; t += TH) T[t] = a.k0.tpl_s[t];
+    for (int w = threadIdx.x; w < nw; w += TH) bm[w] = 0u;
+    for (int x = threadIdx.x; x < S * 36; x += TH) acc[x] = 0.0;
     __syncthreads();
     const int64_t e0 = a.arow[i], e1 = a.arow[i + 1];
     for (int64_t s0 = e0; s0 < e1; s0 += meta)
-        stage_and_mark<false, MODE>(a, s0, (int)min((int64_t)meta, e1 - s0), l, h, first, nullptr, M, bm, scan);
+        stage_and_mark<false, MODE, TH>(a, s0, (int)min((int64_t)meta, e1 - s0), l, h, first, nullptr, M, bm, scan);
     {
-        const int per = (nw + RP_THREADS - 1) / RP_THREADS;
+        const int per = (nw + TH - 1) / TH;
         const int w0 = min(nw, (int)threadIdx.x * per), w1 = min(nw, w0 + per);
         int s = 0;
         for (int w = w0; w < w1; w++) s += __popc(bm[w]);
         int ex = 0;
-        MetaScan(scan).ExclusiveSum(s, ex);
+        MetaScan<TH>(scan).ExclusiveSum(s, ex);
         for (int w = w0; w < w1; w++) {
             pre[w] = ex;
             ex += __popc(bm[w]);
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(RP_THREADS, 2) k_rows_fill(int64_t nrows, RowA
     }
     __syncthreads();
     if (blockIdx.y == 0)
-        for (int w = threadIdx.x; w < nw; w += RP_THREADS) {
+        for (int w = threadIdx.x; w < nw; w += TH) {
             uint32_t m = bm[w];
             int64_t o = c0 + pre[w];
             while (m) {
@@ -241,6 +243,7 @@ __global__ void __launch_bounds__(RP_THREADS, 2) k_rows_fill(int64_t nrows, RowA
     K0Row row{};
     if constexpr (MODE == ROWS_K0) row = k0_row(a.k0, i);
     const int g = threadIdx.x / 6, c = threadIdx.x % 6;
+    const bool grp = g < NG;  // the last threads of a 64-thread block make no group
     const int x36 = threadIdx.x;  // the A entry this thread stages, when < 36
     auto fetch = [&](int64_t f, BEntry& x) {
         x.col = a.bcol[f];
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(RP_THREADS, 2) k_rows_fill(int64_t nrows, RowA
         const int nm = (int)min((int64_t)meta, e1 - s0);
         __syncthreads();  // the last segment's users of the staged entries are done
         if (restage) {
-            for (int m = threadIdx.x; m < nm; m += RP_THREADS) {
+            for (int m = threadIdx.x; m < nm; m += TH) {
                 const int64_t e = s0 + m;
                 mf0[m] = first[e];
                 mlen[m] = (int)(a.brow[a.acol[e] + 1] - mf0[m]);
@@ -283,7 +286,7 @@ __global__ void __launch_bounds__(RP_THREADS, 2) k_rows_fill(int64_t nrows, RowA
             if (nm > 1) araw = a_fetch<MODE>(a, s0 + 1, ment[1], x36);
         }
         BEntry nx;
-        bool hn = g < mlen[0];
+        bool hn = grp && g < mlen[0];
         if (hn) fetch(mf0[0] + g, nx);
         __syncthreads();
         for (int m = 0; m < nm; m++) {
@@ -297,22 +300,22 @@ __global__ void __launch_bounds__(RP_THREADS, 2) k_rows_fill(int64_t nrows, RowA
             const int64_t fs = mf0[m] + g, fe = mf0[m] + mlen[m];
             hn = false;
             if (m + 1 < nm) {
-                hn = g < mlen[m + 1];
+                hn = grp && g < mlen[m + 1];
                 if (hn) fetch(mf0[m + 1] + g, nx);
             }
             if (hc) add(A, cur);
-            for (int64_t f = fs + RP_GROUPS; f < fe; f += 2 * RP_GROUPS) {
+            for (int64_t f = fs + NG; grp && f < fe; f += 2 * NG) {
                 BEntry x0, x1;
                 fetch(f, x0);
-                const bool h1 = f + RP_GROUPS < fe;
-                if (h1) fetch(f + RP_GROUPS, x1);
+                const bool h1 = f + NG < fe;
+                if (h1) fetch(f + NG, x1);
                 add(A, x0);
                 if (h1) add(A, x1);
             }
             __syncthreads();
         }
     }
-    for (int x = threadIdx.x; x < (t1 - t0) * 36; x += RP_THREADS) cval[36 * (c0 + t0) + x] = acc[x];
+    for (int x = threadIdx.x; x < (t1 - t0) * 36; x += TH) cval[36 * (c0 + t0) + x] = acc[x];
 }
 
 __global__ void k_kp_windows(int64_t n, const int32_t* __restrict__ up, const int64_t* __restrict__ prow,
@@ -340,15 +343,27 @@ __global__ void k_upper_windows(int64_t nc, const int32_t* __restrict__ cpiece, 
 // staged A entries: first B entry and value block (8 bytes each), count and prefix
 size_t meta_bytes(int meta) { return (size_t)meta * 2 * sizeof(int64_t) + (size_t)(2 * meta + 2) * sizeof(int); }
 
-template <int MODE>
-void launch_fill(Context& ctx, int64_t nrows, const RowArgs& a, const int64_t* first, const int64_t* crow,
-                 int32_t* ccol, double* cval, int S, int ntiles, int nwmax, int meta) {
+template <int MODE, int TH>
+void launch_fill_th(Context& ctx, int64_t nrows, const RowArgs& a, const int64_t* first, const int64_t* crow,
+                    int32_t* ccol, double* cval, int S, int ntiles, int nwmax, int meta) {
+    meta = std::min(meta, 2 * TH);
     size_t smem = (size_t)S * 36 * sizeof(double) + (MODE == ROWS_K0 ? 36 * 36 * sizeof(double) : 0) +
                   72 * sizeof(double) + meta_bytes(meta) + 2 * (size_t)nwmax * sizeof(uint32_t);
-    SC_CK(cudaFuncSetAttribute(k_rows_fill<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_rows_fill<MODE><<<dim3((unsigned)nrows, (unsigned)ntiles), RP_THREADS, smem, ctx.stream>>>(
+    SC_CK(cudaFuncSetAttribute(k_rows_fill<MODE, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_rows_fill<MODE, TH><<<dim3((unsigned)nrows, (unsigned)ntiles), TH, smem, ctx.stream>>>(
         nrows, a, first, crow, ccol, cval, S, nwmax, meta);
     SC_LAUNCH_CK();
+}
+
+// 64-thread blocks (ten groups) where a step adds fewer than 16 B blocks on average, so
+// more rows run at once and a barrier holds two warps; 192 threads otherwise.
+template <int MODE>
+void launch_fill(Context& ctx, int64_t nrows, const RowArgs& a, const int64_t* first, const int64_t* crow,
+                 int32_t* ccol, double* cval, int S, int ntiles, int nwmax, int meta, bool small) {
+    if (small)
+        launch_fill_th<MODE, RP_SMALL>(ctx, nrows, a, first, crow, ccol, cval, S, ntiles, nwmax, meta);
+    else
+        launch_fill_th<MODE, RP_THREADS>(ctx, nrows, a, first, crow, ccol, cval, S, ntiles, nwmax, meta);
 }
 
 }  // namespace
@@ -410,12 +425,17 @@ void row_products(Context& ctx, int mode, const RowArgs& a, int64_t nrows, int64
     const int S = (int)std::min<int64_t>(cap, (h[1] + 7) / 8 * 8);
     const int ntiles = (int)((h[1] + S - 1) / S);
     require(ntiles <= 65535, SC_BAD_INPUT, "row products: too many slot tiles");
+    bool small = cands < 16 * std::max<int64_t>(a.annz, 1);
+    if (const char* v = std::getenv("SC_ROWS_THREADS")) small = std::atoi(v) == RP_SMALL;
     if (mode == ROWS_K0)
-        launch_fill<ROWS_K0>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax, meta);
+        launch_fill<ROWS_K0>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax, meta,
+                             small);
     else if (mode == ROWS_TRANSPOSED)
-        launch_fill<ROWS_TRANSPOSED>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax, meta);
+        launch_fill<ROWS_TRANSPOSED>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax,
+                                     meta, small);
     else
-        launch_fill<ROWS_PLAIN>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax, meta);
+        launch_fill<ROWS_PLAIN>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax,
+                                meta, small);
 }
 
 }  // namespace sc
