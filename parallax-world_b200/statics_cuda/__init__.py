@@ -265,16 +265,23 @@ class Solver:
         return d
 
     # ---- voxel pieces -------------------------------------------------------------
-    def solve_grid(self, state, k, opt: Options | None = None, gravity=(0.0, 0.0, -1.0), rho=512.0, loads=None):
+    def solve_grid(self, state, k, opt: Options | None = None, gravity=(0.0, 0.0, -1.0), rho=512.0, loads=None,
+                   out: np.ndarray | None = None):
         """Motions of every node of a voxel piece (n_nodes x 6, reference node order);
-        `loads` (n_nodes x 6) replaces mass * gravity when given."""
+        `loads` (n_nodes x 6) replaces mass * gravity when given. `out`, a C-contiguous
+        float64 array of at least n_nodes x 6 values, receives the motions (a repeated
+        solve then writes into memory it has written before); by default a new array."""
         state = np.ascontiguousarray(state, np.uint8)
         k = np.ascontiguousarray(k, np.float32)
         if loads is not None:
             loads = np.ascontiguousarray(loads, np.float64)
         g = make_grid(state, k, rho=rho, gravity=gravity, loads=loads)
         n_nodes, _ = grid_count(state)
-        out = np.zeros((max(n_nodes, 1), 6))
+        if out is None:
+            out = np.zeros((max(n_nodes, 1), 6))
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size < 6 * n_nodes:
+            raise ValueError("out must be a C-contiguous float64 array of at least n_nodes x 6 values")
+        out = out.reshape(-1, 6) if out.ndim != 2 else out
         info = SolveInfo()
         s = lib().sc_solve_grid(self.h, C.byref(g), C.byref(opt or options()), _ptr(out), out.size, 0,
                                 C.byref(info))

@@ -361,3 +361,18 @@ def test_statuses(solver):
     with pytest.raises(sc.StaticsError) as e:
         solver.solve_grid(st, k, sc.options(max_iter=5000, tol=-1.0))
     assert e.value.status == sc.BAD_INPUT
+
+
+def test_solve_grid_into_caller_buffer(solver):
+    """solve_grid(out=...) writes the motions into the caller's array (a larger one too)
+    and gives the same values as a new array."""
+    st, k = piece(16, 0)
+    opt = sc.options(max_iter=5000, tol=1e-8)
+    u, _ = solver.solve_grid(st, k, opt)
+    buf = np.full((u.shape[0] + 3, 6), np.nan)
+    u2, info = solver.solve_grid(st, k, opt, out=buf)
+    assert info["status"] == sc.OK
+    assert np.shares_memory(u2, buf)
+    assert np.array_equal(u, u2)
+    with pytest.raises(ValueError):
+        solver.solve_grid(st, k, opt, out=np.zeros((2, 6)))
