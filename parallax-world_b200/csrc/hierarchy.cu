@@ -335,34 +335,57 @@ __global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restr
                                                const double* __restrict__ step, const int32_t* __restrict__ piece,
                                                const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
                                                double* __restrict__ pval) {
-    __shared__ double blk_s[8][36];  // K0: the warp's current block
+    // S's blocks of the warp's row are summed in shared memory when the P row has at most
+    // NUM_P_SMEM blocks (else in pval, zeroed beforehand): the same additions, in order
+    constexpr int NUM_P_SMEM = 12;
+    __shared__ double blk_s[8][36];                 // K0: the warp's current block
+    __shared__ double s_s[8][NUM_P_SMEM * 36];
     int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (k >= n) return;
     int lane = threadIdx.x & 31;
     if (up[k] < 0) return;
-    double* blk = blk_s[(threadIdx.x >> 5) & 7];
+    const int w = (threadIdx.x >> 5) & 7;
+    double* blk = blk_s[w];
     K0Row row{};
     if (K0) row = k0_row(k0, k);
-    int64_t p0 = prow[k], p1 = prow[k + 1];
-    for (int64_t e = rowptr[k]; e < rowptr[k + 1]; e++) {
-        int32_t o = col[e];
-        int64_t pos = lower_bound_i32(pcol, p0, p1, up[o]);
-        double rv[3] = {rvec[3 * (int64_t)o], rvec[3 * (int64_t)o + 1], rvec[3 * (int64_t)o + 2]};
-        const double* A = val + 36 * e;
-        if (K0) {
-            uint8_t d = k0.desc[e];
-            for (int t = lane; t < 36; t += 32) blk[t] = k0_entry(k0.tpl_s, row, d, t / 6, t % 6);
-            __syncwarp();
-            A = blk;
+    const int64_t p0 = prow[k], p1 = prow[k + 1];
+    const bool local = p1 - p0 <= NUM_P_SMEM;
+    double* S = local ? s_s[w] : pval + 36 * p0;
+    if (local)
+        for (int t = lane; t < 36 * (int)(p1 - p0); t += 32) S[t] = 0.0;
+    __syncwarp();
+    const int64_t e1 = rowptr[k + 1];
+    for (int64_t eb = rowptr[k]; eb < e1; eb += 32) {
+        // lane t finds its entry's block of P row k (independent searches), then the
+        // warp adds the entries one by one
+        int32_t mo = 0;
+        int mpos = 0;
+        if (eb + lane < e1) {
+            mo = col[eb + lane];
+            mpos = (int)(lower_bound_i32(pcol, p0, p1, up[mo]) - p0);
         }
-        warp_block_mac<false, true>(lane, A, nullptr, rv, pval + 36 * pos);
-        __syncwarp();
+        const int nb = (int)min((int64_t)32, e1 - eb);
+        for (int t = 0; t < nb; t++) {
+            const int64_t e = eb + t;
+            const int32_t o = __shfl_sync(0xffffffffu, mo, t);
+            const int pos = __shfl_sync(0xffffffffu, mpos, t);
+            double rv[3] = {rvec[3 * (int64_t)o], rvec[3 * (int64_t)o + 1], rvec[3 * (int64_t)o + 2]};
+            const double* A = val + 36 * e;
+            if (K0) {
+                uint8_t d = k0.desc[e];
+                for (int q = lane; q < 36; q += 32) blk[q] = k0_entry(k0.tpl_s, row, d, q / 6, q % 6);
+                __syncwarp();
+                A = blk;
+            }
+            warp_block_mac<false, true>(lane, A, nullptr, rv, S + 36 * pos);
+            __syncwarp();
+        }
     }
     double st = step[piece[k]];
     const double* D = inv + 36 * k;
     double rk[3] = {rvec[3 * k], rvec[3 * k + 1], rvec[3 * k + 2]};
     for (int64_t pos = p0; pos < p1; pos++) {
-        double* S = pval + 36 * pos;
+        const double* Sp = S + 36 * (pos - p0);
         double out[2];
 #pragma unroll
         for (int rep = 0; rep < 2; rep++) {
@@ -371,7 +394,7 @@ __global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restr
             if (e < 36) {
                 int r = e / 6, c = e % 6;
                 double s = 0.0;
-                for (int j = 0; j < 6; j++) s = fma(D[r * 6 + j], S[j * 6 + c], s);
+                for (int j = 0; j < 6; j++) s = fma(D[r * 6 + j], Sp[j * 6 + c], s);
                 double rig = 0.0;
                 if (pcol[pos] == up[k]) {
                     if (r == c) rig = 1.0;
@@ -387,8 +410,9 @@ __global__ void __launch_bounds__(256) k_num_P(int64_t n, const int64_t* __restr
             }
         }
         __syncwarp();
-        if (lane < 36) S[lane] = out[0];
-        if (lane + 32 < 36) S[lane + 32] = out[1];
+        double* P = pval + 36 * pos;
+        if (lane < 36) P[lane] = out[0];
+        if (lane + 32 < 36) P[lane + 32] = out[1];
         __syncwarp();
     }
 }
