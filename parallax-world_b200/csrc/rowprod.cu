@@ -182,7 +182,9 @@ struct BEntry {
     double b[6];
 };
 
-template <int MODE, int TH>
+// AREG: each step's A block is copied into registers and held for all the step's rounds
+// (else read from shared memory, where it is read again after every accumulator store)
+template <int MODE, int TH, bool AREG>
 __global__ void __launch_bounds__(TH, TH == RP_THREADS ? 2 : 6) k_rows_fill(int64_t nrows, RowArgs a, const int64_t* __restrict__ first,
                                                            const int64_t* __restrict__ crow,
                                                            int32_t* __restrict__ ccol, double* __restrict__ cval,
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(TH, TH == RP_THREADS ? 2 : 6) k_rows_fill(int6
         for (int j = 0; j < 6; j++) x.b[j] = bb[6 * j + c];
     };
     // acc(slot) column c += A B_f column c, for a B entry in this tile
-    auto add = [&](const double* __restrict__ A, const BEntry& x) {
+    auto add = [&](const double* A, const BEntry& x) {
         const uint32_t col = (uint32_t)(x.col - l);
         if (col >= (uint32_t)(h - l)) return;
         const int w = (int)(col >> 5);
@@ -294,7 +296,13 @@ __global__ void __launch_bounds__(TH, TH == RP_THREADS ? 2 : 6) k_rows_fill(int6
                 Ast[36 * ((m + 1) & 1) + x36] = a_make<MODE>(araw, T, row, x36);
                 if (m + 2 < nm) araw = a_fetch<MODE>(a, s0 + m + 2, ment[m + 2], x36);
             }
+            double Ar[AREG ? 36 : 1];
             const double* A = Ast + 36 * (m & 1);
+            if (AREG) {
+#pragma unroll
+                for (int x = 0; x < 36; x++) Ar[x] = A[x];
+                A = Ar;
+            }
             const BEntry cur = nx;
             const bool hc = hn;
             const int64_t fs = mf0[m] + g, fe = mf0[m] + mlen[m];
@@ -343,27 +351,31 @@ __global__ void k_upper_windows(int64_t nc, const int32_t* __restrict__ cpiece, 
 // staged A entries: first B entry and value block (8 bytes each), count and prefix
 size_t meta_bytes(int meta) { return (size_t)meta * 2 * sizeof(int64_t) + (size_t)(2 * meta + 2) * sizeof(int); }
 
-template <int MODE, int TH>
+template <int MODE, int TH, bool AREG>
 void launch_fill_th(Context& ctx, int64_t nrows, const RowArgs& a, const int64_t* first, const int64_t* crow,
                     int32_t* ccol, double* cval, int S, int ntiles, int nwmax, int meta) {
     meta = std::min(meta, 2 * TH);
     size_t smem = (size_t)S * 36 * sizeof(double) + (MODE == ROWS_K0 ? 36 * 36 * sizeof(double) : 0) +
                   72 * sizeof(double) + meta_bytes(meta) + 2 * (size_t)nwmax * sizeof(uint32_t);
-    SC_CK(cudaFuncSetAttribute(k_rows_fill<MODE, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_rows_fill<MODE, TH><<<dim3((unsigned)nrows, (unsigned)ntiles), TH, smem, ctx.stream>>>(
+    SC_CK(cudaFuncSetAttribute(k_rows_fill<MODE, TH, AREG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_rows_fill<MODE, TH, AREG><<<dim3((unsigned)nrows, (unsigned)ntiles), TH, smem, ctx.stream>>>(
         nrows, a, first, crow, ccol, cval, S, nwmax, meta);
     SC_LAUNCH_CK();
 }
 
-// 64-thread blocks (ten groups) where a step adds fewer than 16 B blocks on average, so
-// more rows run at once and a barrier holds two warps; 192 threads otherwise.
+// By the B blocks a step adds on average: under 16, 64-thread blocks (ten groups), so
+// more rows run at once and a barrier holds two warps; from 40 (three rounds of the 32
+// groups or more), 192 threads holding each A block in registers (fewer shared-memory
+// reads, fewer blocks an SM); 192 threads otherwise.
 template <int MODE>
 void launch_fill(Context& ctx, int64_t nrows, const RowArgs& a, const int64_t* first, const int64_t* crow,
-                 int32_t* ccol, double* cval, int S, int ntiles, int nwmax, int meta, bool small) {
-    if (small)
-        launch_fill_th<MODE, RP_SMALL>(ctx, nrows, a, first, crow, ccol, cval, S, ntiles, nwmax, meta);
+                 int32_t* ccol, double* cval, int S, int ntiles, int nwmax, int meta, int variant) {
+    if (variant == 0)
+        launch_fill_th<MODE, RP_SMALL, false>(ctx, nrows, a, first, crow, ccol, cval, S, ntiles, nwmax, meta);
+    else if (variant == 1)
+        launch_fill_th<MODE, RP_THREADS, false>(ctx, nrows, a, first, crow, ccol, cval, S, ntiles, nwmax, meta);
     else
-        launch_fill_th<MODE, RP_THREADS>(ctx, nrows, a, first, crow, ccol, cval, S, ntiles, nwmax, meta);
+        launch_fill_th<MODE, RP_THREADS, true>(ctx, nrows, a, first, crow, ccol, cval, S, ntiles, nwmax, meta);
 }
 
 }  // namespace
@@ -425,17 +437,18 @@ void row_products(Context& ctx, int mode, const RowArgs& a, int64_t nrows, int64
     const int S = (int)std::min<int64_t>(cap, (h[1] + 7) / 8 * 8);
     const int ntiles = (int)((h[1] + S - 1) / S);
     require(ntiles <= 65535, SC_BAD_INPUT, "row products: too many slot tiles");
-    bool small = cands < 16 * std::max<int64_t>(a.annz, 1);
-    if (const char* v = std::getenv("SC_ROWS_THREADS")) small = std::atoi(v) == RP_SMALL;
+    const int64_t per = cands / std::max<int64_t>(a.annz, 1);
+    int variant = per < 16 ? 0 : per < 40 ? 1 : 2;
+    if (const char* v = std::getenv("SC_ROWS_VARIANT")) variant = std::max(0, std::min(2, std::atoi(v)));
     if (mode == ROWS_K0)
         launch_fill<ROWS_K0>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax, meta,
-                             small);
+                             variant);
     else if (mode == ROWS_TRANSPOSED)
         launch_fill<ROWS_TRANSPOSED>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax,
-                                     meta, small);
+                                     meta, variant);
     else
         launch_fill<ROWS_PLAIN>(ctx, nrows, a, first.get(), crow.get(), ccol.get(), cval.get(), S, ntiles, nwmax,
-                                meta, small);
+                                meta, variant);
 }
 
 }  // namespace sc

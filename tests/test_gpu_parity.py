@@ -179,10 +179,11 @@ def test_batch_mixed(solver):
 
 
 @pytest.mark.parametrize("env", [{}, {"SC_GALERKIN": "rows"},
-                                 {"SC_GALERKIN": "rows", "SC_ROWS_THREADS": "64"},
-                                 {"SC_GALERKIN": "rows", "SC_ROWS_THREADS": "192"},
+                                 {"SC_GALERKIN": "rows", "SC_ROWS_VARIANT": "0"},
+                                 {"SC_GALERKIN": "rows", "SC_ROWS_VARIANT": "1"},
+                                 {"SC_GALERKIN": "rows", "SC_ROWS_VARIANT": "2"},
                                  {"SC_GALERKIN": "rows", "SC_ROWS_SLOTS": "3", "SC_ROWS_META": "5"}],
-                         ids=["default", "rows", "rows-64", "rows-192", "rows-tiled"])
+                         ids=["default", "rows", "rows-64", "rows-192", "rows-areg", "rows-tiled"])
 def test_galerkin_rows_match_sorted(solver, monkeypatch, env):
     """The row-by-row Galerkin products (pieces with at most 65536 coarse parts a level)
     and the sorted-candidate ones add the same products in the same order: the same
