@@ -844,24 +844,26 @@ __global__ void k_cell_piece(int64_t ncells, const int64_t* __restrict__ cell_fl
 
 // x = w D^-1 r with D^-1 matrix-free (pre-smoothing, bodies.rs:386)
 template <class T>
-__global__ void __launch_bounds__(256) k_jacobi_mf(int64_t n, const int8_t* __restrict__ axis,
-                                                   const int32_t* __restrict__ cella, const int32_t* __restrict__ cellb,
+__global__ void __launch_bounds__(256) k_jacobi_mf(int64_t n, const int4* __restrict__ slots,
                                                    const int4* __restrict__ cell, const T* __restrict__ r,
                                                    T* __restrict__ x, T s, const int32_t* __restrict__ piece,
                                                    const double* __restrict__ step, const int32_t* __restrict__ skip_row,
                                                    const int32_t* __restrict__ done) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    // over the stencil's slots (parts grouped by axis inside tiles), so a warp runs one
+    // axis' factors
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 sl = __ldg(slots + i);  // part, lesser cell, greater cell, axis
+    const int32_t k = sl.x, A = sl.y, B = sl.z;
     if (skip_row && skip_row[k]) return;
     int p = piece[k];
     if (done && done[p]) return;
     T w = step ? (T)step[p] : T(1);
-    int32_t A = cella[k], B = cellb[k];
     T kA = A >= 0 ? (T)__int_as_float(__ldg(&cell[2 * A + 1].z)) : T(0);
     T kB = B >= 0 ? (T)__int_as_float(__ldg(&cell[2 * B + 1].z)) : T(0);
     T rv[6], d[6];
-    load6<T>(r, (int32_t)k, rv);
-    int ax = axis[k];
+    load6<T>(r, k, rv);
+    int ax = sl.w;
     if (ax == 0)
         dinv<0, T>(kA, kB, s, rv, d);
     else if (ax == 1)
@@ -1021,9 +1023,8 @@ void level0_down(Context& ctx, const Batch& b, const T* r, T* x, T* left, T* t, 
     double vb = (double)sizeof(T) * 6.0 * (double)L.n;
     {
         ProfScope ps(ctx, sizeof(T) == 8 ? SC_FAM_SMOOTH64 : SC_FAM_SMOOTH32, 2 * vb + 8.0 * L.n);
-        k_jacobi_mf<T><<<grid_for(L.n, 256), 256, 0, ctx.stream>>>(L.n, g.axis.get(), g.cella.get(), g.cellb.get(),
-                                                                   g.cell.get(), r, x, (T)g.s, L.piece.get(),
-                                                                   L.step.get(), skip, done);
+        k_jacobi_mf<T><<<grid_for(L.n, 256), 256, 0, ctx.stream>>>(L.n, g.slots.get(), g.cell.get(), r, x, (T)g.s,
+                                                                   L.piece.get(), L.step.get(), skip, done);
         SC_LAUNCH_CK();
     }
     for (int sweep = 1; sweep < b.sweeps; sweep++) {  // further pre-smoothing sweeps
