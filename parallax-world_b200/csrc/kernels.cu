@@ -150,6 +150,71 @@ __global__ void __launch_bounds__(32 * (WPR > 8 ? WPR : 8)) k_spmv_split(
     }
 }
 
+// The same with half a warp a row (two rows a warp), for rows of a few blocks (the
+// level-1 prolongation: P has about nine blocks a row): lanes 8 g + r of a half, g = 0, 1,
+// take the row's blocks e0 + g, then every two, two in flight.
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) k_spmv_half(int64_t nrows, const int64_t* __restrict__ rowptr,
+                                                   const int32_t* __restrict__ col, const T* __restrict__ val,
+                                                   const T* __restrict__ x, const T* __restrict__ r, T* __restrict__ y,
+                                                   const T* __restrict__ inv, const double* __restrict__ step,
+                                                   const int32_t* __restrict__ piece,
+                                                   const int32_t* __restrict__ skip_row,
+                                                   const int32_t* __restrict__ done) {
+    const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 4;
+    const int lane = threadIdx.x & 31, h = lane & 16, hl = lane & 15;
+    bool active = row < nrows && !(skip_row && skip_row[row]);
+    const int p = active && piece ? piece[row] : 0;
+    if (active && done && done[p]) active = false;
+    const int g = hl >> 3, rr = hl & 7;
+    T acc = T(0);
+    if (active && rr < 6) {
+        const int64_t e1 = rowptr[row + 1];
+        int64_t e = rowptr[row] + g;
+        for (; e + 2 < e1; e += 4) {
+            int32_t j0 = col[e], j1 = col[e + 2];
+            T a0[6], x0[6], a1[6], x1[6];
+            ld6<T>(val + 36 * e + 6 * rr, a0);
+            ld6<T>(val + 36 * (e + 2) + 6 * rr, a1);
+            ld6<T>(x + 6 * (int64_t)j0, x0);
+            ld6<T>(x + 6 * (int64_t)j1, x1);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a0[c], x0[c], acc);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a1[c], x1[c], acc);
+        }
+        if (e < e1) {
+            int32_t j = col[e];
+            T a[6], xv[6];
+            ld6<T>(val + 36 * e + 6 * rr, a);
+            ld6<T>(x + 6 * (int64_t)j, xv);
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc = fma(a[c], xv[c], acc);
+        }
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+    // lanes h + 0..5 hold the half's row values
+    if (MODE == SPMV_Y) {
+        if (active && hl < 6) y[6 * row + hl] = acc;
+    } else if (MODE == SPMV_ADD) {
+        if (active && hl < 6) y[6 * row + hl] += acc;
+    } else if (MODE == SPMV_RES) {
+        if (active && hl < 6) y[6 * row + hl] = r[6 * row + hl] - acc;
+    } else {
+        T left = (active && hl < 6) ? r[6 * row + hl] - acc : T(0);
+        T l6[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) l6[c] = __shfl_sync(0xffffffffu, left, h + c);
+        if (active && hl < 6) {
+            const T* d = inv + 36 * row + 6 * hl;
+            T s = T(0);
+#pragma unroll
+            for (int c = 0; c < 6; c++) s = fma(d[c], l6[c], s);
+            y[6 * row + hl] = x[6 * row + hl] + (T)step[p] * s;
+        }
+    }
+}
+
 template <class T>
 __global__ void k_jacobi(int64_t n, const T* __restrict__ inv, const T* __restrict__ r, T* __restrict__ x,
                          const double* __restrict__ step, const int32_t* __restrict__ piece,
@@ -306,8 +371,9 @@ void launch_split(Context& ctx, int mode, int64_t nrows, const int64_t* rowptr, 
     SC_LAUNCH_CK();
 }
 
-// Warps a row: one, unless the rows are too few to fill the device twice over and each
-// warp would still stream 16 or more blocks (doubling up to 32).
+// Warps a row: half a warp (0) where rows average under 12 blocks; one, unless the rows
+// are too few to fill the device twice over and each warp would still stream 16 or more
+// blocks (doubling up to 32).
 static int warps_per_row(int64_t nrows, int64_t nnz) {
     static int sms = 0;
     if (!sms) {
@@ -317,6 +383,7 @@ static int warps_per_row(int64_t nrows, int64_t nnz) {
     }
     const int64_t target = (int64_t)sms * 64;  // two waves of 32 warps an SM
     const int64_t avg = nnz / std::max<int64_t>(nrows, 1);
+    if (avg < 12) return 0;
     int w = 1;
     while (w < 32 && nrows * w < target && avg >= 32 * w) w *= 2;
     return w;
@@ -328,6 +395,28 @@ void spmv(Context& ctx, int mode, int64_t nrows, const int64_t* rowptr, const in
           const int32_t* done, int64_t nnz) {
     if (nrows <= 0) return;
     const int wpr = nnz > 0 ? warps_per_row(nrows, nnz) : 1;
+    if (wpr == 0) {
+        const unsigned gh = grid_for(nrows * 16, 256);
+        switch (mode) {
+            case SPMV_Y:
+                k_spmv_half<T, SPMV_Y><<<gh, 256, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv, step, piece,
+                                                                   skip_row, done);
+                break;
+            case SPMV_ADD:
+                k_spmv_half<T, SPMV_ADD><<<gh, 256, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv, step,
+                                                                     piece, skip_row, done);
+                break;
+            case SPMV_RES:
+                k_spmv_half<T, SPMV_RES><<<gh, 256, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv, step,
+                                                                     piece, skip_row, done);
+                break;
+            default:
+                k_spmv_half<T, SPMV_RES_SMOOTH><<<gh, 256, 0, ctx.stream>>>(nrows, rowptr, col, val, x, r, y, inv,
+                                                                            step, piece, skip_row, done);
+        }
+        SC_LAUNCH_CK();
+        return;
+    }
     switch (wpr) {
         case 2: return launch_split<T, 2>(ctx, mode, nrows, rowptr, col, val, x, r, y, inv, step, piece, skip_row, done);
         case 4: return launch_split<T, 4>(ctx, mode, nrows, rowptr, col, val, x, r, y, inv, step, piece, skip_row, done);
