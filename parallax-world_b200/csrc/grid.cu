@@ -405,9 +405,12 @@ __device__ __forceinline__ void cell_term(int4 a, int4 b, int32_t self, T kc, co
 // (greater), spacing s: D = s Dm (kA M+ + kB M-) Dm with Dm = diag(1,1,1,s,s,s) and
 // kA M+ + kB M- = V^-T diag(kA lambda + kB) V^-1 (generalised eigenvectors of the two
 // face blocks, template_gen.cuh), so D^-1 v = (1/s) Dm^-1 V diag(1/(kA lambda + kB)) V' Dm^-1 v.
+// (The spacing's powers divide as products with 1/s: one division instead of nine, and
+// the same values, the spacing 1/8 being a power of two.)
 template <int AX, class T>
 __device__ __forceinline__ void dinv(T kA, T kB, T s, const T (&v)[6], T (&y)[6]) {
-    T vt[6] = {v[0], v[1], v[2], v[3] / s, v[4] / s, v[5] / s};
+    const T is = T(1) / s, is2 = is * is;
+    T vt[6] = {v[0], v[1], v[2], v[3] * is, v[4] * is, v[5] * is};
     T w[6];
 #pragma unroll
     for (int i = 0; i < 6; i++) {
@@ -421,7 +424,7 @@ __device__ __forceinline__ void dinv(T kA, T kB, T s, const T (&v)[6], T (&y)[6]
         T acc = T(0);
 #pragma unroll
         for (int j = 0; j < 6; j++) acc = fma((T)JAC_V_DEV[AX][i][j], w[j], acc);
-        y[i] = i < 3 ? acc / s : acc / (s * s);
+        y[i] = i < 3 ? acc * is : acc * is2;
     }
 }
 
