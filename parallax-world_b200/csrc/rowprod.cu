@@ -437,6 +437,8 @@ void row_products(Context& ctx, int mode, const RowArgs& a, int64_t nrows, int64
     const int S = (int)std::min<int64_t>(cap, (h[1] + 7) / 8 * 8);
     const int ntiles = (int)((h[1] + S - 1) / S);
     require(ntiles <= 65535, SC_BAD_INPUT, "row products: too many slot tiles");
+    // the form by the B blocks a step adds on average (see launch_fill); SC_ROWS_VARIANT
+    // = 0, 1 or 2 forces one (to test each)
     const int64_t per = cands / std::max<int64_t>(a.annz, 1);
     int variant = per < 16 ? 0 : per < 40 ? 1 : 2;
     if (const char* v = std::getenv("SC_ROWS_VARIANT")) variant = std::max(0, std::min(2, std::atoi(v)));
