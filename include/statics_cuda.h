@@ -252,14 +252,31 @@ sc_status sc_settle(sc_context* ctx, const sc_lattice* lattice, const sc_strengt
  * solver's deterministic chunked sum, and allocates nothing: its partial sums live in
  * one 512 KB array inside the library, reserved on every GPU that loads it until the
  * process exits. At most SC_NOALLOC_MAX_VALUES values (SC_BAD_INPUT beyond).
- * The first call on a device looks that array up for the device (do it before any
- * stream capture). Every call shares the array: calls whose kernels may overlap on the
+ * The first call on a device looks that array up for the device. Every call shares
+ * the array: calls whose kernels may overlap on the
  * GPU race and can return wrong sums, so order them on one stream. Asynchronous:
  * *compliance is ready when `stream` reaches this point.
  * ------------------------------------------------------------------------- */
 #define SC_NOALLOC_MAX_VALUES (8192LL * 65536LL)
 sc_status sc_compliance_noalloc(const double* loads, const double* motions, int64_t n_values, double* compliance,
                                 void* stream);
+
+/* ---------------------------------------------------------------------------
+ * The engine's solver, mechanics::solve::Solver (mechanics/src/solve.rs:356-538).
+ *
+ * The system: n unknowns with their octree site (3 int64), position `at` (3 doubles)
+ * and 3x3 diagonal block (9 doubles, row-major); npairs pairs (pi, pj, 3x3 block pb:
+ * pb in row pi, column pj, its transpose in row pj, column pi; a pair twice adds). All
+ * host arrays. Makes the levels (Solver::new(system, size): rigid aggregates by octree
+ * cell, their Galerkin blocks, Cholesky inverses with dropped pivots, a direct top) and
+ * solves by PCG from x (3 n doubles, in/out) until r' P r <= tol^2 b' P b, P the V-cycle
+ * preconditioner (Solver::solve). *rounds: the rounds taken (at most 300), or -1 where
+ * the levels do not fit the system (not positive; the reference's None). *levels: the
+ * coarse levels made.
+ * ------------------------------------------------------------------------- */
+sc_status sc_mech_solve(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
+                        int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b,
+                        double* x, double tol, double size, int32_t* rounds, int32_t* levels);
 
 #ifdef __cplusplus
 }

@@ -422,6 +422,22 @@ sc_status sc_grid_count(const sc_grid* g, int64_t* n_nodes, int64_t* n_parts) {
     return SC_OK;
 }
 
+sc_status sc_mech_solve(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
+                        int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b,
+                        double* x, double tol, double size, int32_t* rounds, int32_t* levels) {
+    if (n < 0 || npairs < 0 || !rounds || !levels) return SC_BAD_INPUT;
+    if (n > 0 && (!sites || !at || !diag || !b || !x)) return SC_BAD_INPUT;
+    if (npairs > 0 && (!pi || !pj || !pb)) return SC_BAD_INPUT;
+    if (!(tol > 0.0) || !(size > 0.0)) return SC_BAD_INPUT;
+    for (int64_t p = 0; p < npairs; p++)
+        if ((int64_t)pi[p] >= n || (int64_t)pj[p] >= n || pi[p] == pj[p]) return SC_BAD_INPUT;
+    return guarded(ctx, [&] {
+        ctx->c.last.reset();
+        *levels = 0;
+        *rounds = mech_solve(ctx->c, n, sites, at, diag, npairs, pi, pj, pb, b, x, tol, size, levels);
+    });
+}
+
 sc_status sc_solve_grid(sc_context* ctx, const sc_grid* g, const sc_options* opt, double* motions, int64_t capacity,
                         int32_t motions_on_device, sc_solve_info* info) {
     if (!g || !opt || !motions) return SC_BAD_INPUT;

@@ -1,0 +1,749 @@
+// The engine's solver, mechanics::solve::Solver (mechanics/src/solve.rs:356-538), on the
+// device. Its levels are made on the host, as Solver::new makes them (solve.rs:241-271,
+// 361-386: rigid aggregates of the parts joined within each octree cell a level up, their
+// Galerkin blocks T(r)' M T(s), block inverses by Cholesky with dropped pivots, the turn
+// regularisation, the smoother step by ten power steps, a direct top), and kept on the
+// device as block-sparse rows (3x3 at the cells' nodes, 6x6 above, both triangles). The
+// conjugate gradients and V-cycles (solve.rs:403-538) run there: block products,
+// block-Jacobi smoothing, the rigid restriction and prolongation, the top's dense
+// inverse, and deterministic dot products. Coarse pairs are kept in (a, c) order (the
+// reference collects them from a hash map, solve.rs:249-262): sums over pairs add in
+// another order, equal up to rounding.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <map>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace sc {
+
+namespace {
+
+typedef std::array<double, 3> H3;
+typedef std::array<H3, 3> HM3;
+typedef std::array<double, 6> H6;
+typedef std::array<H6, 6> HM6;
+
+constexpr int MECH_ROUNDS = 300;   // solve.rs:21
+constexpr size_t MECH_DIRECT = 24;  // solve.rs:23
+
+// ---- the levels, on the host ------------------------------------------------------
+struct HPair {
+    uint32_t i, j;
+    HM6 m;
+};
+
+struct HSys {  // the system with its blocks embedded as 6x6 (solve.rs:97-103)
+    std::vector<std::array<int64_t, 3>> keys;
+    std::vector<H3> at;
+    std::vector<HM6> diag;
+    std::vector<HPair> pairs;
+};
+
+HM6 lift6(const HM6& m, const H3& r, const H3& s) {  // solve.rs:77-94
+    auto X = [](const H3& v) { return HM3{H3{0.0, v[2], -v[1]}, H3{-v[2], 0.0, v[0]}, H3{v[1], -v[0], 0.0}}; };
+    const HM3 xr = X(r), xs = X(s);
+    HM6 t = m;
+    for (int row = 0; row < 6; row++)
+        for (int c = 0; c < 3; c++) {
+            double acc = 0.0;
+            for (int k = 0; k < 3; k++) acc += m[row][k] * xs[k][c];
+            t[row][3 + c] += acc;
+        }
+    HM6 out = t;
+    for (int r3 = 0; r3 < 3; r3++)
+        for (int col = 0; col < 6; col++) {
+            double acc = 0.0;
+            for (int k = 0; k < 3; k++) acc += xr[k][r3] * t[k][col];
+            out[3 + r3][col] += acc;
+        }
+    return out;
+}
+
+// L L' in place, pivots below 1e-12 of the largest dropped (solve.rs:138-165)
+std::vector<bool> chol(std::vector<double>& a, size_t n) {
+    double largest = 0.0;
+    for (size_t i = 0; i < n; i++) largest = std::fmax(largest, a[i * n + i]);
+    std::vector<bool> dropped(n, false);
+    for (size_t j = 0; j < n; j++) {
+        double d = a[j * n + j];
+        for (size_t k = 0; k < j; k++) d -= a[j * n + k] * a[j * n + k];
+        if (d <= largest * 1e-12) {
+            dropped[j] = true;
+            for (size_t i = j; i < n; i++) a[i * n + j] = 0.0;
+            continue;
+        }
+        d = std::sqrt(d);
+        a[j * n + j] = d;
+        for (size_t i = j + 1; i < n; i++) {
+            double s = a[i * n + j];
+            for (size_t k = 0; k < j; k++) s -= a[i * n + k] * a[j * n + k];
+            a[i * n + j] = s / d;
+        }
+    }
+    return dropped;
+}
+
+void chol_solve(const std::vector<double>& a, const std::vector<bool>& dropped, size_t n, double* b) {  // :167-186
+    for (size_t i = 0; i < n; i++) {
+        if (dropped[i]) {
+            b[i] = 0.0;
+            continue;
+        }
+        double s = 0.0;
+        for (size_t k = 0; k < i; k++) s += a[i * n + k] * b[k];
+        b[i] = (b[i] - s) / a[i * n + i];
+    }
+    for (size_t i = n; i-- > 0;) {
+        if (dropped[i]) {
+            b[i] = 0.0;
+            continue;
+        }
+        double s = 0.0;
+        for (size_t k = i + 1; k < n; k++) s += a[k * n + i] * b[k];
+        b[i] = (b[i] - s) / a[i * n + i];
+    }
+}
+
+// the inverse operator of a factored n x n matrix: row-major, out[c * n + r] = (A^-1 e_c)[r]
+// as solve.rs:123-135 lays it out (the same matrix, A being symmetric)
+std::vector<double> chol_inverse(std::vector<double> a, size_t n) {
+    std::vector<bool> l = chol(a, n);
+    std::vector<double> out(n * n);
+    std::vector<double> e(n);
+    for (size_t c = 0; c < n; c++) {
+        std::fill(e.begin(), e.end(), 0.0);
+        e[c] = 1.0;
+        chol_solve(a, l, n, e.data());
+        for (size_t r = 0; r < n; r++) out[c * n + r] = e[r];
+    }
+    return out;
+}
+
+size_t uf_find(std::vector<size_t>& up, size_t i) {
+    while (up[i] != i) {
+        up[i] = up[up[i]];
+        i = up[i];
+    }
+    return i;
+}
+
+int64_t half(int64_t v) { return v >= 0 ? v / 2 : -((-v + 1) / 2); }  // div_euclid(2)
+std::array<int64_t, 3> parent_key(const std::array<int64_t, 3>& k) { return {half(k[0]), half(k[1]), half(k[2])}; }
+
+struct HLevel {  // solve.rs:188-203
+    std::vector<uint32_t> of;
+    std::vector<H3> r;
+    HSys sys;  // keys, centres, blocks
+    std::vector<double> inv;  // 36 per part
+    double size = 0.0, step = 1.0;
+    bool direct = false;
+    std::vector<double> top_inv;  // (6n)^2, the direct level's inverse operator
+};
+
+void apply6(const HSys& s, const std::vector<H6>& x, std::vector<H6>& y) {  // solve.rs:306-317
+    for (size_t p = 0; p < s.diag.size(); p++)
+        for (int r = 0; r < 6; r++) {
+            double acc = 0.0;
+            for (int c = 0; c < 6; c++) acc += s.diag[p][r][c] * x[p][c];
+            y[p][r] = acc;
+        }
+    for (const HPair& e : s.pairs)
+        for (int r = 0; r < 6; r++) {
+            double a = 0.0, c2 = 0.0;
+            for (int c = 0; c < 6; c++) a += e.m[r][c] * x[e.j][c];
+            for (int c = 0; c < 6; c++) c2 += e.m[c][r] * x[e.i][c];
+            y[e.i][r] += a;
+            y[e.j][r] += c2;
+        }
+}
+
+// 4/3 over the largest eigenvalue of over(apply), ten power steps from the reference's
+// start (solve.rs:274-296)
+template <size_t N, class Apply, class Over>
+double power_step(size_t n, Apply apply, Over over) {
+    typedef std::array<double, N> VN;
+    auto norm = [](const std::vector<VN>& v) {
+        double s = 0.0;
+        for (const VN& e : v)
+            for (double x : e) s += x * x;
+        return std::sqrt(s);
+    };
+    std::vector<VN> v(n), a(n, VN{}), w(n, VN{});
+    for (size_t k = 0; k < n; k++)
+        for (size_t s = 0; s < N; s++) v[k][s] = 1.0 + (double)((7 * k + 3 * s) % 11) / 11.0;
+    double most = 1.0;
+    for (int it = 0; it < 10; it++) {
+        apply(v, a);
+        over(a, w);
+        const double nw = norm(w), nv = norm(v);
+        if (nw == 0.0) break;
+        most = nw / nv;
+        for (size_t k = 0; k < n; k++)
+            for (size_t s = 0; s < N; s++) v[k][s] = w[k][s] / nw;
+    }
+    return 4.0 / 3.0 / most;
+}
+
+void factor_top(HLevel& L) {  // solve.rs:320-347
+    const size_t n = L.sys.diag.size(), m = 6 * n;
+    std::vector<double> a(36 * n * n, 0.0);
+    for (size_t p = 0; p < n; p++) {
+        const HM6& d = L.sys.diag[p];
+        for (int r = 0; r < 6; r++)
+            for (int c = 0; c < 6; c++) a[(6 * p + r) * m + 6 * p + c] += d[r][c];
+        const double t = (d[0][0] + d[1][1] + d[2][2]) / 3.0;
+        for (int k = 3; k < 6; k++) a[(6 * p + k) * m + 6 * p + k] += 1e-6 * t * L.size * L.size;
+    }
+    for (const HPair& e : L.sys.pairs)
+        for (int r = 0; r < 6; r++)
+            for (int c = 0; c < 6; c++) {
+                a[(6 * e.i + r) * m + 6 * e.j + c] += e.m[r][c];
+                a[(6 * e.j + c) * m + 6 * e.i + r] += e.m[r][c];
+            }
+    L.top_inv = chol_inverse(std::move(a), m);
+    L.direct = true;
+}
+
+HLevel coarsen(const HSys& f, double size) {  // solve.rs:241-271
+    const size_t nf = f.keys.size();
+    std::vector<size_t> up(nf);
+    for (size_t i = 0; i < nf; i++) up[i] = i;
+    for (const HPair& e : f.pairs)
+        if (parent_key(f.keys[e.i]) == parent_key(f.keys[e.j])) {
+            size_t r = uf_find(up, e.i), s = uf_find(up, e.j);
+            up[std::max(r, s)] = std::min(r, s);
+        }
+    HLevel L;
+    L.of.resize(nf);
+    std::vector<uint32_t> index(nf, UINT32_MAX);
+    uint32_t n = 0;
+    for (size_t i = 0; i < nf; i++) {
+        size_t root = uf_find(up, i);
+        if (index[root] == UINT32_MAX) index[root] = n++;
+        L.of[i] = index[root];
+    }
+    HSys& c = L.sys;
+    c.at.assign(n, H3{0.0, 0.0, 0.0});
+    c.keys.assign(n, std::array<int64_t, 3>{0, 0, 0});
+    std::vector<double> count(n, 0.0);
+    for (size_t i = 0; i < nf; i++) {
+        const uint32_t a = L.of[i];
+        for (int k = 0; k < 3; k++) c.at[a][k] = c.at[a][k] + f.at[i][k];
+        count[a] += 1.0;
+        c.keys[a] = parent_key(f.keys[i]);
+    }
+    for (uint32_t a = 0; a < n; a++)
+        for (int k = 0; k < 3; k++) c.at[a][k] = c.at[a][k] * (1.0 / count[a]);
+    L.r.resize(nf);
+    for (size_t i = 0; i < nf; i++)
+        for (int k = 0; k < 3; k++) L.r[i][k] = f.at[i][k] - c.at[L.of[i]][k];
+    c.diag.assign(n, HM6{});
+    auto plus = [](HM6& a, const HM6& b) {
+        for (int r = 0; r < 6; r++)
+            for (int cc = 0; cc < 6; cc++) a[r][cc] += b[r][cc];
+    };
+    auto tr = [](const HM6& m) {
+        HM6 t;
+        for (int r = 0; r < 6; r++)
+            for (int cc = 0; cc < 6; cc++) t[r][cc] = m[cc][r];
+        return t;
+    };
+    for (size_t i = 0; i < nf; i++) plus(c.diag[L.of[i]], lift6(f.diag[i], L.r[i], L.r[i]));
+    std::map<std::pair<uint32_t, uint32_t>, HM6> map;
+    for (const HPair& e : f.pairs) {
+        const uint32_t a = L.of[e.i], b = L.of[e.j];
+        const HM6 m = lift6(e.m, L.r[e.i], L.r[e.j]);
+        if (a == b) {
+            plus(c.diag[a], m);
+            plus(c.diag[a], tr(m));
+        } else if (a < b) {
+            plus(map.emplace(std::make_pair(a, b), HM6{}).first->second, m);
+        } else {
+            plus(map.emplace(std::make_pair(b, a), HM6{}).first->second, tr(m));
+        }
+    }
+    for (auto& kv : map) c.pairs.push_back(HPair{kv.first.first, kv.first.second, kv.second});
+    L.inv.resize(36 * (size_t)n);
+    for (uint32_t p = 0; p < n; p++) {
+        HM6 d = c.diag[p];
+        const double t = (d[0][0] + d[1][1] + d[2][2]) / 3.0;
+        for (int k = 3; k < 6; k++) d[k][k] += 1e-6 * t * size * size;
+        std::vector<double> a(36);
+        for (int r = 0; r < 6; r++)
+            for (int cc = 0; cc < 6; cc++) a[6 * r + cc] = d[r][cc];
+        std::vector<double> iv = chol_inverse(std::move(a), 6);
+        std::copy(iv.begin(), iv.end(), L.inv.begin() + 36 * (size_t)p);
+    }
+    L.size = size;
+    L.step = power_step<6>(
+        n, [&](const std::vector<H6>& x, std::vector<H6>& y) { apply6(c, x, y); },
+        [&](const std::vector<H6>& x, std::vector<H6>& y) {
+            for (uint32_t p = 0; p < n; p++)
+                for (int r = 0; r < 6; r++) {
+                    double acc = 0.0;
+                    for (int cc = 0; cc < 6; cc++) acc += L.inv[36 * (size_t)p + 6 * r + cc] * x[p][cc];
+                    y[p][r] = acc;
+                }
+        });
+    if (n <= MECH_DIRECT) factor_top(L);
+    return L;
+}
+
+// ---- the device ---------------------------------------------------------------------
+struct DLevel {
+    int64_t n = 0;
+    DBuf<int32_t> of;  // finer part -> part here
+    DBuf<double> r;    // 3 per finer part
+    DBuf<int64_t> mptr;
+    DBuf<int32_t> mem;  // each part's finer parts, in order
+    DBuf<int64_t> rowptr;
+    DBuf<int32_t> col;
+    DBuf<double> val, inv, step;
+    int64_t nnzb = 0;
+    bool direct = false;
+    DBuf<double> top_inv;
+    DBuf<double> b, x, res, t;
+};
+
+// full block rows of a 6x6 system: the diagonal and each pair both ways
+void upload_rows(Context& ctx, const HSys& s, DLevel& D) {
+    const int64_t n = (int64_t)s.diag.size();
+    std::vector<std::vector<std::pair<int32_t, HM6>>> rows(n);
+    for (int64_t p = 0; p < n; p++) rows[p].push_back({(int32_t)p, s.diag[p]});
+    for (const HPair& e : s.pairs) {
+        HM6 t;
+        for (int r = 0; r < 6; r++)
+            for (int c = 0; c < 6; c++) t[r][c] = e.m[c][r];
+        rows[e.i].push_back({(int32_t)e.j, e.m});
+        rows[e.j].push_back({(int32_t)e.i, t});
+    }
+    std::vector<int64_t> rp(n + 1, 0);
+    std::vector<int32_t> col;
+    std::vector<double> val;
+    for (int64_t p = 0; p < n; p++) {
+        std::sort(rows[p].begin(), rows[p].end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (auto& e : rows[p]) {
+            col.push_back(e.first);
+            for (int r = 0; r < 6; r++)
+                for (int c = 0; c < 6; c++) val.push_back(e.second[r][c]);
+        }
+        rp[p + 1] = (int64_t)col.size();
+    }
+    D.nnzb = (int64_t)col.size();
+    D.rowptr.alloc(n + 1, ctx.stream, &ctx.mem);
+    D.rowptr.upload(rp.data(), n + 1);
+    D.col.alloc(std::max<int64_t>(D.nnzb, 1), ctx.stream, &ctx.mem);
+    D.col.upload(col.data(), col.size());
+    D.val.alloc(std::max<size_t>(val.size(), 1), ctx.stream, &ctx.mem);
+    D.val.upload(val.data(), val.size());
+}
+
+// y = S x (resid: y = b - S x) over the nodes' 3x3 block rows
+__global__ void k_bsr3(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                       const double* __restrict__ val, const double* __restrict__ x, const double* __restrict__ b,
+                       double* __restrict__ y) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int64_t e = rowptr[i]; e < rowptr[i + 1]; e++) {
+        const double* m = val + 9 * e;
+        const double* xv = x + 3 * (int64_t)col[e];
+        const double x0 = xv[0], x1 = xv[1], x2 = xv[2];
+        a0 += m[0] * x0 + m[1] * x1 + m[2] * x2;
+        a1 += m[3] * x0 + m[4] * x1 + m[5] * x2;
+        a2 += m[6] * x0 + m[7] * x1 + m[8] * x2;
+    }
+    if (b) {
+        y[3 * i] = b[3 * i] - a0;
+        y[3 * i + 1] = b[3 * i + 1] - a1;
+        y[3 * i + 2] = b[3 * i + 2] - a2;
+    } else {
+        y[3 * i] = a0;
+        y[3 * i + 1] = a1;
+        y[3 * i + 2] = a2;
+    }
+}
+
+// out = base + step * inv (v - w) per node (base, w nullable: 0; base may be out)
+__global__ void k_jacobi3(int64_t n, const double* __restrict__ inv, double step, const double* __restrict__ v,
+                          const double* __restrict__ w, const double* base, double* out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d[3];
+    for (int k = 0; k < 3; k++) d[k] = w ? v[3 * i + k] - w[3 * i + k] : v[3 * i + k];
+    const double* m = inv + 9 * i;
+    for (int r = 0; r < 3; r++) {
+        double s = m[3 * r] * d[0] + m[3 * r + 1] * d[1] + m[3 * r + 2] * d[2];
+        out[3 * i + r] = (base ? base[3 * i + r] : 0.0) + s * step;
+    }
+}
+
+// rb[a] = sum over a's members p of (r_t, r_w + rp x r_t); W = 3 (nodes: r_w = 0) or 6
+template <int W>
+__global__ void k_restrict(int64_t nc, const int64_t* __restrict__ mptr, const int32_t* __restrict__ mem,
+                           const double* __restrict__ rr, const double* __restrict__ v, const double* __restrict__ w,
+                           double* __restrict__ rb) {
+    int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (a >= nc) return;
+    double o[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int64_t t = mptr[a]; t < mptr[a + 1]; t++) {
+        const int64_t p = mem[t];
+        double f[6];
+        for (int k = 0; k < W; k++) f[k] = w ? v[W * p + k] - w[W * p + k] : v[W * p + k];
+        const double r0 = rr[3 * p], r1 = rr[3 * p + 1], r2 = rr[3 * p + 2];
+        const double t0 = r1 * f[2] - r2 * f[1], t1 = r2 * f[0] - r0 * f[2], t2 = r0 * f[1] - r1 * f[0];
+        o[0] += f[0];
+        o[1] += f[1];
+        o[2] += f[2];
+        if (W == 6) {
+            o[3] += f[3] + t0;
+            o[4] += f[4] + t1;
+            o[5] += f[5] + t2;
+        } else {
+            o[3] += t0;
+            o[4] += t1;
+            o[5] += t2;
+        }
+    }
+    for (int k = 0; k < 6; k++) rb[6 * a + k] = o[k];
+}
+
+// x[p] += (e_t + e_w x r_p, e_w) of its part (W = 3: the translation only)
+template <int W>
+__global__ void k_prolong(int64_t nf, const int32_t* __restrict__ of, const double* __restrict__ rr,
+                          const double* __restrict__ e, double* __restrict__ x) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= nf) return;
+    const double* ea = e + 6 * (int64_t)of[p];
+    const double r0 = rr[3 * p], r1 = rr[3 * p + 1], r2 = rr[3 * p + 2];
+    const double u0 = ea[4] * r2 - ea[5] * r1, u1 = ea[5] * r0 - ea[3] * r2, u2 = ea[3] * r1 - ea[4] * r0;
+    x[W * p] += ea[0] + u0;
+    x[W * p + 1] += ea[1] + u1;
+    x[W * p + 2] += ea[2] + u2;
+    if (W == 6)
+        for (int k = 3; k < 6; k++) x[W * p + k] += ea[k];
+}
+
+// x = A^-1 b, A^-1 (m x m) laid out as out[c * m + r]
+__global__ void k_top(int64_t m, const double* __restrict__ ainv, const double* __restrict__ b, double* __restrict__ x) {
+    for (int64_t r = threadIdx.x; r < m; r += blockDim.x) {
+        double s = 0.0;
+        for (int64_t c = 0; c < m; c++) s += ainv[c * m + r] * b[c];
+        x[r] = s;
+    }
+}
+
+// per-block partial sums of a . b, a fixed order
+constexpr int MDOT_BLOCKS = 256;
+__global__ void __launch_bounds__(256) k_mdot(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                                              double* __restrict__ part) {
+    __shared__ double red[256];
+    const int64_t per = (n + MDOT_BLOCKS - 1) / MDOT_BLOCKS;
+    const int64_t lo = blockIdx.x * per, hi = min(n, lo + per);
+    double s = 0.0;
+    for (int64_t i = lo + threadIdx.x; i < hi; i += 256) s += a[i] * b[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// x += alpha p, r -= alpha ap; or (update = 1) p = z + beta p
+__global__ void k_mupdate(int64_t n, int update, double s, double* __restrict__ x, double* __restrict__ r,
+                          const double* __restrict__ p, const double* __restrict__ ap) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (update == 0) {
+        x[i] = x[i] + p[i] * s;
+        r[i] = r[i] - ap[i] * s;
+    } else {
+        x[i] = r[i] + x[i] * s;  // x = p, r = z
+    }
+}
+
+struct MechSolver {
+    Context& ctx;
+    int64_t n0 = 0;
+    DBuf<int64_t> rowptr0;
+    DBuf<int32_t> col0;
+    DBuf<double> val0, inv0;
+    double step0 = 1.0;
+    std::vector<DLevel> lv;
+    DBuf<double> part;
+    std::vector<double> hpart;
+
+    explicit MechSolver(Context& c) : ctx(c) {}
+
+    double dot(const double* a, const double* b, int64_t n) {
+        k_mdot<<<MDOT_BLOCKS, 256, 0, ctx.stream>>>(n, a, b, part.get());
+        SC_LAUNCH_CK();
+        part.download(hpart.data(), MDOT_BLOCKS);
+        SC_CK(cudaStreamSynchronize(ctx.stream));
+        double s = 0.0;
+        for (int i = 0; i < MDOT_BLOCKS; i++) s += hpart[i];
+        return s;
+    }
+    void times(const double* x, double* y, const double* b = nullptr) {
+        k_bsr3<<<grid_for(n0, 128), 128, 0, ctx.stream>>>(n0, rowptr0.get(), col0.get(), val0.get(), x, b, y);
+        SC_LAUNCH_CK();
+    }
+    // x = V-cycle of level l for its b (solve.rs:403-447)
+    void cycle(size_t l) {
+        DLevel& L = lv[l];
+        if (L.direct) {
+            k_top<<<1, 256, 0, ctx.stream>>>(6 * L.n, L.top_inv.get(), L.b.get(), L.x.get());
+            SC_LAUNCH_CK();
+            return;
+        }
+        DLevel& U = lv[l + 1];
+        jacobi<double>(ctx, L.n, L.inv.get(), L.b.get(), L.x.get(), L.step.get(), nullptr, nullptr, nullptr);
+        spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), L.x.get(), L.b.get(), L.res.get(),
+                     nullptr, nullptr, nullptr, nullptr, nullptr, L.nnzb);
+        k_restrict<6><<<grid_for(U.n, 128), 128, 0, ctx.stream>>>(U.n, U.mptr.get(), U.mem.get(), U.r.get(),
+                                                                   L.res.get(), nullptr, U.b.get());
+        SC_LAUNCH_CK();
+        cycle(l + 1);
+        k_prolong<6><<<grid_for(L.n, 256), 256, 0, ctx.stream>>>(L.n, U.of.get(), U.r.get(), U.x.get(), L.x.get());
+        SC_LAUNCH_CK();
+        spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), L.x.get(), L.b.get(), L.res.get(),
+                     nullptr, nullptr, nullptr, nullptr, nullptr, L.nnzb);
+        jacobi_add<double>(ctx, L.n, L.inv.get(), L.res.get(), L.x.get(), L.t.get(), L.step.get(), nullptr, nullptr,
+                           nullptr);
+        std::swap(L.x, L.t);
+    }
+    // out = the preconditioner of b (solve.rs:450-476); scratch: 3 n0
+    void precondition(const double* b, double* out, double* scratch) {
+        const unsigned g = grid_for(n0, 256);
+        k_jacobi3<<<g, 256, 0, ctx.stream>>>(n0, inv0.get(), step0, b, nullptr, nullptr, out);
+        SC_LAUNCH_CK();
+        times(out, scratch);
+        DLevel& U = lv[0];
+        k_restrict<3><<<grid_for(U.n, 128), 128, 0, ctx.stream>>>(U.n, U.mptr.get(), U.mem.get(), U.r.get(), b,
+                                                                   scratch, U.b.get());
+        SC_LAUNCH_CK();
+        cycle(0);
+        k_prolong<3><<<g, 256, 0, ctx.stream>>>(n0, U.of.get(), U.r.get(), U.x.get(), out);
+        SC_LAUNCH_CK();
+        times(out, scratch);
+        k_jacobi3<<<g, 256, 0, ctx.stream>>>(n0, inv0.get(), step0, b, scratch, out, out);
+        SC_LAUNCH_CK();
+    }
+};
+
+}  // namespace
+
+// The levels of the system, then PCG from x (solve.rs:356-386, 485-538): the rounds taken,
+// -1 where the levels do not fit the system (not positive).
+int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
+               const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b, double* x, double tol,
+               double size, int32_t* nlevels) {
+    cudaStream_t st = ctx.stream;
+    MemStats* ms = &ctx.mem;
+    if (n == 0) return 0;
+    // level 0 on the host: inverses and the step (solve.rs:362-364)
+    std::vector<double> inv0(9 * (size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+        std::vector<double> a(diag + 9 * i, diag + 9 * i + 9);
+        std::vector<double> iv = chol_inverse(std::move(a), 3);
+        std::copy(iv.begin(), iv.end(), inv0.begin() + 9 * i);
+    }
+    auto times0 = [&](const std::vector<H3>& xv, std::vector<H3>& yv) {  // solve.rs:63-73
+        for (int64_t i = 0; i < n; i++)
+            for (int r = 0; r < 3; r++) {
+                double acc = 0.0;
+                for (int c = 0; c < 3; c++) acc += diag[9 * i + 3 * r + c] * xv[i][c];
+                yv[i][r] = acc;
+            }
+        for (int64_t p = 0; p < npairs; p++) {
+            const double* m = pb + 9 * p;
+            for (int r = 0; r < 3; r++) {
+                double a = 0.0, c2 = 0.0;
+                for (int c = 0; c < 3; c++) a += m[3 * r + c] * xv[pj[p]][c];
+                for (int c = 0; c < 3; c++) c2 += m[3 * c + r] * xv[pi[p]][c];
+                yv[pi[p]][r] += a;
+                yv[pj[p]][r] += c2;
+            }
+        }
+    };
+    const double step0 = power_step<3>(n, times0, [&](const std::vector<H3>& xv, std::vector<H3>& yv) {
+        for (int64_t i = 0; i < n; i++)
+            for (int r = 0; r < 3; r++) {
+                double acc = 0.0;
+                for (int c = 0; c < 3; c++) acc += inv0[9 * i + 3 * r + c] * xv[i][c];
+                yv[i][r] = acc;
+            }
+    });
+    // the coarse levels (solve.rs:365-385)
+    HSys f;
+    f.keys.resize(n);
+    f.at.resize(n);
+    f.diag.assign(n, HM6{});
+    for (int64_t i = 0; i < n; i++) {
+        for (int k = 0; k < 3; k++) {
+            f.keys[i][k] = sites[3 * i + k];
+            f.at[i][k] = at[3 * i + k];
+        }
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) f.diag[i][r][c] = diag[9 * i + 3 * r + c];
+    }
+    for (int64_t p = 0; p < npairs; p++) {
+        HPair e{pi[p], pj[p], HM6{}};
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) e.m[r][c] = pb[9 * p + 3 * r + c];
+        f.pairs.push_back(e);
+    }
+    std::vector<HLevel> levels;
+    double sz = size;
+    HLevel next = coarsen(f, sz * 2.0);
+    for (;;) {
+        sz *= 2.0;
+        const size_t nn = next.sys.diag.size(), before = levels.empty() ? (size_t)n : levels.back().sys.diag.size();
+        if (next.direct) {
+            levels.push_back(std::move(next));
+            break;
+        }
+        if (nn == before) {
+            factor_top(next);
+            levels.push_back(std::move(next));
+            break;
+        }
+        levels.push_back(std::move(next));
+        next = coarsen(levels.back().sys, sz * 2.0);
+    }
+    *nlevels = (int32_t)levels.size();
+    // to the device
+    MechSolver S(ctx);
+    S.n0 = n;
+    S.step0 = step0;
+    {
+        std::vector<std::vector<std::pair<int32_t, std::array<double, 9>>>> rows(n);
+        for (int64_t i = 0; i < n; i++) {
+            std::array<double, 9> d;
+            std::copy(diag + 9 * i, diag + 9 * i + 9, d.begin());
+            rows[i].push_back({(int32_t)i, d});
+        }
+        for (int64_t p = 0; p < npairs; p++) {
+            std::array<double, 9> m, t;
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) {
+                    m[3 * r + c] = pb[9 * p + 3 * r + c];
+                    t[3 * r + c] = pb[9 * p + 3 * c + r];
+                }
+            rows[pi[p]].push_back({(int32_t)pj[p], m});
+            rows[pj[p]].push_back({(int32_t)pi[p], t});
+        }
+        std::vector<int64_t> rp(n + 1, 0);
+        std::vector<int32_t> col;
+        std::vector<double> val;
+        for (int64_t i = 0; i < n; i++) {
+            std::sort(rows[i].begin(), rows[i].end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (auto& e : rows[i]) {
+                col.push_back(e.first);
+                val.insert(val.end(), e.second.begin(), e.second.end());
+            }
+            rp[i + 1] = (int64_t)col.size();
+        }
+        S.rowptr0.alloc(n + 1, st, ms);
+        S.rowptr0.upload(rp.data(), n + 1);
+        S.col0.alloc(col.size(), st, ms);
+        S.col0.upload(col.data(), col.size());
+        S.val0.alloc(val.size(), st, ms);
+        S.val0.upload(val.data(), val.size());
+        S.inv0.alloc(inv0.size(), st, ms);
+        S.inv0.upload(inv0.data(), inv0.size());
+    }
+    S.lv.resize(levels.size());
+    for (size_t l = 0; l < levels.size(); l++) {
+        const HLevel& H = levels[l];
+        DLevel& D = S.lv[l];
+        D.n = (int64_t)H.sys.diag.size();
+        const int64_t nf = (int64_t)H.of.size();
+        D.of.alloc(nf, st, ms);
+        D.of.upload(reinterpret_cast<const int32_t*>(H.of.data()), nf);
+        std::vector<double> rr(3 * (size_t)nf);
+        for (int64_t i = 0; i < nf; i++)
+            for (int k = 0; k < 3; k++) rr[3 * i + k] = H.r[i][k];
+        D.r.alloc(rr.size(), st, ms);
+        D.r.upload(rr.data(), rr.size());
+        std::vector<int64_t> mp(D.n + 1, 0);
+        for (int64_t i = 0; i < nf; i++) mp[H.of[i] + 1]++;
+        for (int64_t a = 0; a < D.n; a++) mp[a + 1] += mp[a];
+        std::vector<int32_t> mem(nf);
+        std::vector<int64_t> fill(mp.begin(), mp.end() - 1);
+        for (int64_t i = 0; i < nf; i++) mem[fill[H.of[i]]++] = (int32_t)i;
+        D.mptr.alloc(D.n + 1, st, ms);
+        D.mptr.upload(mp.data(), D.n + 1);
+        D.mem.alloc(nf, st, ms);
+        D.mem.upload(mem.data(), nf);
+        D.b.alloc(6 * D.n, st, ms);
+        D.x.alloc(6 * D.n, st, ms);
+        D.res.alloc(6 * D.n, st, ms);
+        D.t.alloc(6 * D.n, st, ms);
+        D.direct = H.direct;
+        if (H.direct) {
+            D.top_inv.alloc(H.top_inv.size(), st, ms);
+            D.top_inv.upload(H.top_inv.data(), H.top_inv.size());
+        } else {
+            upload_rows(ctx, H.sys, D);
+            D.inv.alloc(H.inv.size(), st, ms);
+            D.inv.upload(H.inv.data(), H.inv.size());
+            D.step.alloc(1, st, ms);
+            D.step.upload(&H.step, 1);
+        }
+    }
+    S.part.alloc(MDOT_BLOCKS, st, ms);
+    S.hpart.resize(MDOT_BLOCKS);
+    // PCG from x (solve.rs:485-538)
+    const int64_t m = 3 * n;
+    DBuf<double> db, dx, r, z, p, ap, scratch;
+    for (DBuf<double>* v : {&db, &dx, &r, &z, &p, &ap, &scratch}) v->alloc(m, st, ms);
+    db.upload(b, m);
+    dx.upload(x, m);
+    S.precondition(db.get(), z.get(), scratch.get());
+    const double target = tol * tol * S.dot(db.get(), z.get(), m);
+    int rounds = -1;
+    if (!(std::isnan(target) || target < 0.0)) {
+        S.times(dx.get(), r.get(), db.get());  // r = b - S x
+        S.precondition(r.get(), z.get(), scratch.get());
+        SC_CK(cudaMemcpyAsync(p.get(), z.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        double rz = S.dot(r.get(), z.get(), m);
+        const unsigned g = grid_for(m, 256);
+        rounds = MECH_ROUNDS;
+        for (int round = 0; round < MECH_ROUNDS; round++) {
+            if (rz < 0.0) {
+                rounds = -1;
+                break;
+            }
+            if (rz <= target) {
+                rounds = round;
+                break;
+            }
+            S.times(p.get(), ap.get());
+            const double pap = S.dot(p.get(), ap.get(), m);
+            if (pap <= 0.0) {
+                rounds = round;
+                break;
+            }
+            const double alpha = rz / pap;
+            k_mupdate<<<g, 256, 0, st>>>(m, 0, alpha, dx.get(), r.get(), p.get(), ap.get());
+            SC_LAUNCH_CK();
+            S.precondition(r.get(), z.get(), scratch.get());
+            const double nx = S.dot(r.get(), z.get(), m);
+            const double beta = nx / rz;
+            rz = nx;
+            k_mupdate<<<g, 256, 0, st>>>(m, 1, beta, p.get(), z.get(), nullptr, nullptr);
+            SC_LAUNCH_CK();
+        }
+    }
+    dx.download(x, m);
+    SC_CK(cudaStreamSynchronize(st));
+    return rounds;
+}
+
+}  // namespace sc

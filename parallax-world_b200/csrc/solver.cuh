@@ -143,6 +143,11 @@ void level0_smooth(Context& ctx, const Batch& b, const T* r, const T* x, T* z, c
 void lattice_level0(Context& ctx, Batch& b, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,
                     const double* loads);
 
+// --- mech.cu: the engine's solver (mechanics/src/solve.rs) -----------------------------
+int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
+               const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b, double* x, double tol,
+               double size, int32_t* nlevels);
+
 // --- capi.cu / settle.cu -----------------------------------------------------------------
 // motions of a lattice into out_dev (6 per node, device); the solve's status
 sc_status lattice_motions(Context& ctx, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,

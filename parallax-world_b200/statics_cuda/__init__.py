@@ -122,6 +122,8 @@ def lib():
         L.sc_launches.restype = C.c_int64
         L.sc_launches.argtypes = []
         L.sc_context_stream.argtypes = [P, C.POINTER(P)]
+        L.sc_mech_solve.argtypes = [P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, C.c_double, C.c_double,
+                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.sc_used_standing.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
                                        C.POINTER(SolveInfo)]
         L.sc_settle.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
@@ -187,8 +189,8 @@ NOALLOC_MAX_VALUES = 8192 * 65536
 def compliance_noalloc(loads_ptr: int, motions_ptr: int, n_values: int, out_ptr: int, stream: int = 0) -> int:
     """C = f . u of two device arrays into a device double, allocating no device memory
     (sc_compliance_noalloc). For callers that cannot let the library allocate: engines
-    that own the GPU's memory, code inside a graph capture, frame loops. Returns the
-    status; the result is ready when `stream` gets there."""
+    that own the GPU's memory, frame loops. Returns the status; the result is ready
+    when `stream` gets there."""
     return int(lib().sc_compliance_noalloc(C.c_void_p(loads_ptr), C.c_void_p(motions_ptr), n_values,
                                            C.c_void_p(out_ptr), C.c_void_p(stream or None)))
 
@@ -289,6 +291,27 @@ class Solver:
         d = info.as_dict()
         d["status"] = s
         return out[:n_nodes], d
+
+    def mech_solve(self, system: dict, b=None, x0=None, tol: float = 1e-3, size: float | None = None):
+        """The engine's solver (mechanics::solve::Solver::new then solve, solve.rs:356-538)
+        on a system given as arrays: sites (n x 3 int64), at (n x 3), diag (n x 3 x 3),
+        pi, pj (uint32) and pb (m x 3 x 3) for the pairs, h (the cells' size, the
+        default `size`). Solves from x0 (zeros by default) for b (the system's "b" by
+        default). Returns (x, rounds or -1, coarse levels)."""
+        n = len(system["sites"])
+        sites = np.ascontiguousarray(system["sites"], np.int64)
+        at = np.ascontiguousarray(system["at"], np.float64)
+        diag = np.ascontiguousarray(system["diag"], np.float64)
+        pi = np.ascontiguousarray(system["pi"], np.uint32)
+        pj = np.ascontiguousarray(system["pj"], np.uint32)
+        pb = np.ascontiguousarray(system["pb"], np.float64)
+        b = np.ascontiguousarray(system["b"] if b is None else b, np.float64)
+        x = np.zeros((n, 3)) if x0 is None else np.array(x0, np.float64, copy=True)
+        rounds, levels = C.c_int32(), C.c_int32()
+        s = lib().sc_mech_solve(self.h, n, _ptr(sites), _ptr(at), _ptr(diag), len(pi), _ptr(pi), _ptr(pj), _ptr(pb),
+                                _ptr(b), _ptr(x), tol, size or system["h"], C.byref(rounds), C.byref(levels))
+        self._check(s, "sc_mech_solve")
+        return x, rounds.value, levels.value
 
     def solve_grid_batch(self, pieces, opt: Options | None = None):
         """pieces: list of (state, k). Returns ([motions], [info])."""
