@@ -334,6 +334,28 @@ def run_probe(args):
     import numpy as np
 
     import statics_cuda as sc
+    if args.probe == "mech":
+        # the engine's solver (sc_mech_solve) on voxel pieces at rest (E = 1e9 U[0.5, 2],
+        # h = 1/8 m, dt = 1/60 s), to 1e-8 in its energy norm; beside it, the CPU baseline:
+        # the oracle's restatement of the same solver on one host core (pieces up to 48^3)
+        solver = sc.Solver(0)
+        for n in (32, 48, 64):
+            st, k = sc.generate_piece(n, n, n, 4, sc.K_UNIFORM)
+            s = sc.mech_voxel_system(st, k * 1e9, h=0.125, dt=1 / 60, mass=2000 * 0.125 ** 3)
+            solver.mech_solve(s, tol=1e-8)  # warm-up
+            t = time.perf_counter()
+            x, rounds, levels = solver.mech_solve(s, tol=1e-8)
+            out = {"probe": "mech", "grid": [n, n, n], "unknowns": len(s["sites"]), "pairs": len(s["pi"]),
+                   "rounds": rounds, "levels": levels, "gpu_s": time.perf_counter() - t}
+            if n <= 48:
+                from oracle import mechanics as M
+                t = time.perf_counter()
+                xr, rr, _, _ = M.solve(s, tol=1e-8)
+                out.update(cpu_s=time.perf_counter() - t, cpu_rounds=rr,
+                           rel_diff=float(np.linalg.norm(x - xr) / np.linalg.norm(xr)))
+            print(json.dumps(out), flush=True)
+        solver.close()
+        return
     if args.probe == "large":
         # the large configuration: a 256^3 piece, lognormal k (mu 0, sigma 0.5) clipped to
         # [0.1, 10]; mixed-precision forward solve plus the compliance adjoint, checked
@@ -502,7 +524,8 @@ def main():
     ap.add_argument("--probe-n", type=int, default=N, help="edge of the --probe solve / stencil piece")
     ap.add_argument("--precision", choices=["all", "mixed", "fp64"], default="all",
                     help="the --probe solve precisions: all three twice, or two solves of one")
-    ap.add_argument("--probe", choices=["stencil", "solve", "batch", "large"], help="run one kernel or one solve alone (profiling)")
+    ap.add_argument("--probe", choices=["stencil", "solve", "batch", "large", "mech"],
+                    help="run one kernel or one solve alone (profiling); mech: the engine's solver")
     args = ap.parse_args()
     if args.probe:
         run_probe(args)

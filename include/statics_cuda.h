@@ -274,6 +274,15 @@ sc_status sc_compliance_noalloc(const double* loads, const double* motions, int6
  * the levels do not fit the system (not positive; the reference's None). *levels: the
  * coarse levels made.
  * ------------------------------------------------------------------------- */
+/* A voxel piece at rest as such a system (mechanics/src/lib.rs:375-423, 638-676): each free
+ * cell (state 1; 0 empty, 2 held; x-major) an 8-node element of the unit cube's
+ * stiffness (Poisson's ratio 0.3) times e[cell] h, welded to its free neighbours; corners
+ * touching a held cell held; diagonal m I + (dt^2 + 0.3 dt) E h K_aa (m: `mass` / 8 from
+ * each cell at a corner); b = m (0, -9.81 dt, 0). Call with sites = NULL for the counts
+ * (*n, *npairs), then with arrays of those sizes (*n, *npairs set to their capacity). */
+sc_status sc_mech_voxel_system(const uint8_t* state, const float* e, int32_t nx, int32_t ny, int32_t nz, double h,
+                               double dt, double mass, int64_t* n, int64_t* npairs, int64_t* sites, double* at,
+                               double* diag, uint32_t* pi, uint32_t* pj, double* pb, double* b);
 sc_status sc_mech_solve(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
                         int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b,
                         double* x, double tol, double size, int32_t* rounds, int32_t* levels);

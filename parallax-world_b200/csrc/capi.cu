@@ -422,6 +422,34 @@ sc_status sc_grid_count(const sc_grid* g, int64_t* n_nodes, int64_t* n_parts) {
     return SC_OK;
 }
 
+sc_status sc_mech_voxel_system(const uint8_t* state, const float* e, int32_t nx, int32_t ny, int32_t nz, double h,
+                               double dt, double mass, int64_t* n, int64_t* npairs, int64_t* sites, double* at,
+                               double* diag, uint32_t* pi, uint32_t* pj, double* pb, double* b) {
+    if (!state || !e || nx <= 0 || ny <= 0 || nz <= 0 || !n || !npairs || !(h > 0.0) || !(dt > 0.0)) return SC_BAD_INPUT;
+    try {
+        std::vector<int64_t> s;
+        std::vector<double> a, d, p, bb;
+        std::vector<uint32_t> i, j;
+        mech_voxel_system(state, e, nx, ny, nz, h, dt, mass, s, a, d, i, j, p, bb);
+        const int64_t nn = (int64_t)s.size() / 3, mm = (int64_t)i.size();
+        if (sites) {
+            if (*n < nn || *npairs < mm || !at || !diag || !b || (mm > 0 && (!pi || !pj || !pb))) return SC_BAD_INPUT;
+            std::copy(s.begin(), s.end(), sites);
+            std::copy(a.begin(), a.end(), at);
+            std::copy(d.begin(), d.end(), diag);
+            std::copy(bb.begin(), bb.end(), b);
+            std::copy(i.begin(), i.end(), pi);
+            std::copy(j.begin(), j.end(), pj);
+            std::copy(p.begin(), p.end(), pb);
+        }
+        *n = nn;
+        *npairs = mm;
+        return SC_OK;
+    } catch (const std::exception&) {
+        return SC_CUDA;
+    }
+}
+
 sc_status sc_mech_solve(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
                         int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b,
                         double* x, double tol, double size, int32_t* rounds, int32_t* levels) {

@@ -538,6 +538,165 @@ struct MechSolver {
 
 }  // namespace
 
+// ---- a voxel piece at rest as a system (mechanics/src/lib.rs:375-423, 638-676) ----------
+// Every free cell an 8-node element of the unit cube's stiffness (element.rs:44-69, a
+// Poisson's ratio of 0.3) times E h, welded to its free neighbours (corners at one lattice
+// point are one node, numbered by the first cell and corner that reach it); a corner
+// touching a held cell is held. Unknowns: the other nodes in order; diagonal blocks
+// m I + (dt^2 + 0.3 dt) E h K_aa; pairs in first-encounter order over cells and corner
+// pairs, (min, max), their blocks transposed where the first node is the greater;
+// b = m (0, -9.81 dt, 0) (at rest, gravity along -y).
+namespace {
+const int MCORNERS[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+typedef std::array<std::array<HM3, 8>, 8> HUnit;
+const HUnit& unit_cube() {
+    static HUnit k = [] {
+        HUnit k{};
+        const double NU = 0.3, g = 1.0 / std::sqrt(3.0);
+        auto sgn = [](int c) {
+            return H3{(double)(2 * MCORNERS[c][0] - 1), (double)(2 * MCORNERS[c][1] - 1),
+                      (double)(2 * MCORNERS[c][2] - 1)};
+        };
+        auto strain = [&](int a, const H3& at) {  // rows xx, yy, zz, 2yz, 2xz, 2xy
+            H3 s = sgn(a), gr;
+            for (int q = 0; q < 3; q++) {
+                double prod = 1.0;
+                for (int j = 0; j < 3; j++)
+                    if (j != q) prod *= 1.0 + s[j] * at[j];
+                gr[q] = s[q] / 4.0 * prod;
+            }
+            return std::array<H3, 6>{H3{gr[0], 0.0, 0.0}, H3{0.0, gr[1], 0.0}, H3{0.0, 0.0, gr[2]},
+                                     H3{0.0, gr[2], gr[1]}, H3{gr[2], 0.0, gr[0]}, H3{gr[1], gr[0], 0.0}};
+        };
+        const double l = NU / ((1.0 + NU) * (1.0 - 2.0 * NU)), m = 1.0 / (2.0 * (1.0 + NU));
+        for (int p = 0; p < 8; p++) {
+            const H3 s = sgn(p), at{s[0] * g, s[1] * g, s[2] * g};
+            std::array<std::array<H3, 6>, 8> b;
+            for (int a = 0; a < 8; a++) b[a] = strain(a, at);
+            for (int a = 0; a < 8; a++)
+                for (int c = 0; c < 8; c++)
+                    for (int j = 0; j < 3; j++) {
+                        double e[6];
+                        for (int r = 0; r < 6; r++) e[r] = b[c][r][j];
+                        const double tr = e[0] + e[1] + e[2];
+                        const double st[6] = {l * tr + 2.0 * m * e[0], l * tr + 2.0 * m * e[1], l * tr + 2.0 * m * e[2],
+                                              m * e[3], m * e[4], m * e[5]};
+                        for (int i = 0; i < 3; i++) {
+                            double acc = 0.0;
+                            for (int r = 0; r < 6; r++) acc += b[a][r][i] * st[r];
+                            k[a][c][i][j] += acc / 8.0;
+                        }
+                    }
+        }
+        return k;
+    }();
+    return k;
+}
+}  // namespace
+
+void mech_voxel_system(const uint8_t* state, const float* e, int nx, int ny, int nz, double h, double dt,
+                       double mass, std::vector<int64_t>& sites, std::vector<double>& at, std::vector<double>& diag,
+                       std::vector<uint32_t>& pi, std::vector<uint32_t>& pj, std::vector<double>& pb,
+                       std::vector<double>& b) {
+    auto st = [&](int x, int y, int z) -> int {
+        if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return 0;
+        return state[((int64_t)x * ny + y) * nz + z];
+    };
+    std::vector<std::array<int, 3>> cells;
+    std::vector<double> ke;
+    for (int x = 0; x < nx; x++)
+        for (int y = 0; y < ny; y++)
+            for (int z = 0; z < nz; z++)
+                if (st(x, y, z) == 1) {
+                    cells.push_back({x, y, z});
+                    ke.push_back((double)e[((int64_t)x * ny + y) * nz + z]);
+                }
+    const int64_t NY = ny + 1, NZ = nz + 1;
+    std::vector<int64_t> node_of((size_t)((int64_t)(nx + 1) * NY * NZ), -1);
+    std::vector<std::array<int64_t, 3>> nsite;
+    std::vector<double> nmass;
+    std::vector<char> nheld;
+    std::vector<std::array<uint32_t, 8>> corners(cells.size());
+    for (size_t i = 0; i < cells.size(); i++)
+        for (int c = 0; c < 8; c++) {
+            const int px = cells[i][0] + MCORNERS[c][0], py = cells[i][1] + MCORNERS[c][1],
+                      pz = cells[i][2] + MCORNERS[c][2];
+            const int64_t g = (px * NY + py) * NZ + pz;
+            if (node_of[g] < 0) {
+                node_of[g] = (int64_t)nsite.size();
+                nsite.push_back({px, py, pz});
+                nmass.push_back(0.0);
+                bool held = false;
+                for (int dx = -1; dx <= 0; dx++)
+                    for (int dy = -1; dy <= 0; dy++)
+                        for (int dz = -1; dz <= 0; dz++) held = held || st(px + dx, py + dy, pz + dz) == 2;
+                nheld.push_back(held);
+            }
+            corners[i][c] = (uint32_t)node_of[g];
+            nmass[node_of[g]] += mass / 8.0;
+        }
+    const uint32_t NONE = UINT32_MAX, TURNED = 1u << 31;
+    std::vector<uint32_t> fr(nsite.size());
+    uint32_t count = 0;
+    for (size_t k = 0; k < nsite.size(); k++) fr[k] = nheld[k] ? NONE : count++;
+    sites.clear(), at.clear(), diag.clear(), pi.clear(), pj.clear(), pb.clear(), b.clear();
+    for (size_t k = 0; k < nsite.size(); k++) {
+        if (fr[k] == NONE) continue;
+        for (int q = 0; q < 3; q++) {
+            sites.push_back(nsite[k][q]);
+            at.push_back(nsite[k][q] * h);
+        }
+        const double m = nmass[k];
+        const double d[9] = {m, 0.0, 0.0, 0.0, m, 0.0, 0.0, 0.0, m};
+        diag.insert(diag.end(), d, d + 9);
+        b.push_back(0.0 * m);
+        b.push_back(-9.81 * dt * m);
+        b.push_back(0.0 * m);
+    }
+    std::map<std::pair<uint32_t, uint32_t>, uint32_t> index;
+    std::vector<std::array<uint32_t, 64>> slots(cells.size());
+    for (size_t i = 0; i < cells.size(); i++) {
+        slots[i].fill(NONE);
+        for (int a = 0; a < 8; a++)
+            for (int c = a + 1; c < 8; c++) {
+                const uint32_t p = fr[corners[i][a]], q = fr[corners[i][c]];
+                if (p == NONE || q == NONE) continue;
+                const auto key = std::make_pair(std::min(p, q), std::max(p, q));
+                auto it = index.find(key);
+                uint32_t k;
+                if (it == index.end()) {
+                    k = (uint32_t)pi.size();
+                    index.emplace(key, k);
+                    pi.push_back(key.first);
+                    pj.push_back(key.second);
+                    pb.insert(pb.end(), 9, 0.0);
+                } else {
+                    k = it->second;
+                }
+                slots[i][8 * a + c] = k | (p > q ? TURNED : 0u);
+            }
+    }
+    const double stiff = dt * dt + 0.3 * dt;
+    const HUnit& K = unit_cube();
+    for (size_t i = 0; i < cells.size(); i++) {
+        const double k = ke[i] * h;
+        for (int a = 0; a < 8; a++) {
+            const uint32_t p = fr[corners[i][a]];
+            if (p != NONE)
+                for (int r = 0; r < 3; r++)
+                    for (int c = 0; c < 3; c++) diag[9 * (size_t)p + 3 * r + c] += K[a][a][r][c] * k * stiff;
+            for (int c = a + 1; c < 8; c++) {
+                const uint32_t slot = slots[i][8 * a + c];
+                if (slot == NONE) continue;
+                double* into = pb.data() + 9 * (size_t)(slot & ~TURNED);
+                const bool turned = (slot & TURNED) != 0;
+                for (int r = 0; r < 3; r++)
+                    for (int cc = 0; cc < 3; cc++) into[3 * r + cc] += (turned ? K[a][c][cc][r] : K[a][c][r][cc]) * k * stiff;
+            }
+        }
+    }
+}
+
 // The levels of the system, then PCG from x (solve.rs:356-386, 485-538): the rounds taken,
 // -1 where the levels do not fit the system (not positive).
 int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,

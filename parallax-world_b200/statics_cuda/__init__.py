@@ -122,6 +122,9 @@ def lib():
         L.sc_launches.restype = C.c_int64
         L.sc_launches.argtypes = []
         L.sc_context_stream.argtypes = [P, C.POINTER(P)]
+        L.sc_mech_voxel_system.argtypes = [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                           C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), P, P, P, P, P,
+                                           P, P]
         L.sc_mech_solve.argtypes = [P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, C.c_double, C.c_double,
                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.sc_used_standing.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
@@ -176,6 +179,28 @@ def make_grid(state: np.ndarray, k: np.ndarray, g_over_e=0.4, rho=512.0, gravity
     g.loads = _ptr(loads)
     g._keep = (state, k, loads)
     return g
+
+
+def mech_voxel_system(state, e, h: float = 0.125, dt: float = 1.0 / 60.0, mass: float = 1.0) -> dict:
+    """A voxel piece at rest as the engine's system (sc_mech_voxel_system): sites, at,
+    diag (n x 3 x 3), pi, pj, pb (m x 3 x 3) for the pairs, b (n x 3), h."""
+    state = np.ascontiguousarray(state, np.uint8)
+    e = np.ascontiguousarray(e, np.float32)
+    nx, ny, nz = state.shape
+    n, m = C.c_int64(), C.c_int64()
+    s = lib().sc_mech_voxel_system(_ptr(state), _ptr(e), nx, ny, nz, h, dt, mass, C.byref(n), C.byref(m), None, None,
+                                   None, None, None, None, None)
+    if s != OK:
+        raise StaticsError(s, "sc_mech_voxel_system")
+    out = {"sites": np.zeros((n.value, 3), np.int64), "at": np.zeros((n.value, 3)), "diag": np.zeros((n.value, 3, 3)),
+           "pi": np.zeros(m.value, np.uint32), "pj": np.zeros(m.value, np.uint32), "pb": np.zeros((m.value, 3, 3)),
+           "b": np.zeros((n.value, 3)), "h": h}
+    s = lib().sc_mech_voxel_system(_ptr(state), _ptr(e), nx, ny, nz, h, dt, mass, C.byref(n), C.byref(m),
+                                   _ptr(out["sites"]), _ptr(out["at"]), _ptr(out["diag"]), _ptr(out["pi"]),
+                                   _ptr(out["pj"]), _ptr(out["pb"]), _ptr(out["b"]))
+    if s != OK:
+        raise StaticsError(s, "sc_mech_voxel_system")
+    return out
 
 
 def launches() -> int:

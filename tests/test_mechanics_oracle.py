@@ -73,3 +73,15 @@ def test_solver_converges_and_warm_starts(E):
     assert np.linalg.norm(r) <= 1e-6 * np.linalg.norm(s["b"])
     _, again, _, _ = M.solve(s, x0=x, tol=1e-8)
     assert again == 0
+
+
+@pytest.mark.parametrize("n,seed", [(6, 0), (12, 5)])
+def test_library_system_matches_oracle(n, seed):
+    """The library's voxel system (sc_mech_voxel_system, host code: no GPU) is the
+    oracle's, value for value."""
+    st, k = sc.generate_piece(n, n + 1, n, seed, sc.K_UNIFORM)
+    a = M.system(st, k * 1e8, h=0.125, dt=1 / 60, mass=2.0)
+    b = sc.mech_voxel_system(st, k * 1e8, h=0.125, dt=1 / 60, mass=2.0)
+    for key in ("sites", "at", "diag", "pi", "pj", "pb", "b"):
+        assert a[key].shape == b[key].shape, key
+        assert np.array_equal(a[key], b[key]), key
