@@ -705,6 +705,7 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
     cudaStream_t st = ctx.stream;
     MemStats* ms = &ctx.mem;
     if (n == 0) return 0;
+    PhaseTimer pt(ctx);  // SC_TIMING=1 prints the phases
     // level 0 on the host: inverses and the step (solve.rs:362-364)
     std::vector<double> inv0(9 * (size_t)n);
     for (int64_t i = 0; i < n; i++) {
@@ -776,6 +777,7 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
         next = coarsen(levels.back().sys, sz * 2.0);
     }
     *nlevels = (int32_t)levels.size();
+    pt.mark("mech: levels (host)");
     // to the device
     MechSolver S(ctx);
     S.n0 = n;
@@ -858,6 +860,8 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
     }
     S.part.alloc(MDOT_BLOCKS, st, ms);
     S.hpart.resize(MDOT_BLOCKS);
+    SC_CK(cudaStreamSynchronize(st));
+    pt.mark("mech: levels to the device");
     // PCG from x (solve.rs:485-538)
     const int64_t m = 3 * n;
     DBuf<double> db, dx, r, z, p, ap, scratch;
@@ -902,6 +906,8 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
     }
     dx.download(x, m);
     SC_CK(cudaStreamSynchronize(st));
+    pt.note("mech: %d rounds", rounds);
+    pt.mark("mech: conjugate gradients");
     return rounds;
 }
 
