@@ -283,6 +283,12 @@ sc_status sc_compliance_noalloc(const double* loads, const double* motions, int6
 sc_status sc_mech_voxel_system(const uint8_t* state, const float* e, int32_t nx, int32_t ny, int32_t nz, double h,
                                double dt, double mass, int64_t* n, int64_t* npairs, int64_t* sites, double* at,
                                double* diag, uint32_t* pi, uint32_t* pj, double* pb, double* b);
+/* Only the levels (Solver::new, host code, no device): *nlevels coarse levels, the parts
+ * of each (sizes, up to max_levels), and the smoother steps: steps[0] the nodes', steps[l
+ * + 1] coarse level l's (0 for the direct top); steps holds max_levels + 1 values. */
+sc_status sc_mech_levels(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
+                         const uint32_t* pi, const uint32_t* pj, const double* pb, double size, int32_t max_levels,
+                         int64_t* sizes, double* steps, int32_t* nlevels);
 sc_status sc_mech_solve(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
                         int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b,
                         double* x, double tol, double size, int32_t* rounds, int32_t* levels);

@@ -76,3 +76,13 @@ def solve(s, b=None, x0=None, tol=1e-8, size=None):
     rounds = lib.mo_solve(*_args(s), _p(b, _F64), _p(x, _F64), C.c_double(tol), C.c_double(size or s["h"]), 64,
                           _p(sizes, _I64), C.byref(nl), C.byref(step))
     return x, rounds, list(sizes[:nl.value]), step.value
+
+
+def levels(s, size=None):
+    """Solver::new only: (coarse level sizes, steps: the nodes' then each level's, 0 at a
+    direct top)."""
+    sizes, steps = np.zeros(64, np.int64), np.zeros(65)
+    lib = _lib()
+    lib.mo_levels.restype = C.c_int
+    nl = lib.mo_levels(*_args(s), C.c_double(size or s["h"]), 64, _p(sizes, _I64), _p(steps, _F64))
+    return list(sizes[:nl]), list(steps[:nl + 1])

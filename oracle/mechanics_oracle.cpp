@@ -741,6 +741,22 @@ void mo_times(int64_t n, const int64_t* sites, const double* at, const double* d
         for (int k = 0; k < 3; k++) y[3 * i + k] = yv[i][k];
 }
 
+// Solver::new only: the coarse levels' sizes and the steps (the nodes', then each level's,
+// 0 at a direct top)
+int mo_levels(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
+              const uint32_t* pi, const uint32_t* pj, const double* pb, double size, int max_levels,
+              int64_t* level_sizes, double* steps) {
+    mech::System s = make(n, sites, at, diag, npairs, pi, pj, pb);
+    mech::Solver solver(s, size);
+    steps[0] = solver.step;
+    int l = 0;
+    for (; l < (int)solver.levels.size() && l < max_levels; l++) {
+        level_sizes[l] = (int64_t)solver.levels[l].centre.size();
+        steps[l + 1] = solver.levels[l].direct ? 0.0 : solver.levels[l].step;
+    }
+    return (int)solver.levels.size();
+}
+
 // Solver::new then solve from x (in/out): rounds, or -1 (the levels do not fit); the
 // level sizes (parts per coarse level, up to max_levels) and the fine smoothing step
 int mo_solve(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,

@@ -697,17 +697,19 @@ void mech_voxel_system(const uint8_t* state, const float* e, int nx, int ny, int
     }
 }
 
-// The levels of the system, then PCG from x (solve.rs:356-386, 485-538): the rounds taken,
-// -1 where the levels do not fit the system (not positive).
-int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
-               const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b, double* x, double tol,
-               double size, int32_t* nlevels) {
-    cudaStream_t st = ctx.stream;
-    MemStats* ms = &ctx.mem;
-    if (n == 0) return 0;
-    PhaseTimer pt(ctx);  // SC_TIMING=1 prints the phases
-    // level 0 on the host: inverses and the step (solve.rs:362-364)
-    std::vector<double> inv0(9 * (size_t)n);
+// Solver::new on the host (solve.rs:361-386): level 0's block inverses and step, then the
+// coarse levels.
+struct HostLevels {
+    std::vector<double> inv0;
+    double step0 = 1.0;
+    std::vector<HLevel> levels;
+};
+
+static HostLevels make_levels(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
+                              const uint32_t* pi, const uint32_t* pj, const double* pb, double size) {
+    HostLevels H;
+    std::vector<double>& inv0 = H.inv0;
+    inv0.resize(9 * (size_t)n);
     for (int64_t i = 0; i < n; i++) {
         std::vector<double> a(diag + 9 * i, diag + 9 * i + 9);
         std::vector<double> iv = chol_inverse(std::move(a), 3);
@@ -731,7 +733,7 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
             }
         }
     };
-    const double step0 = power_step<3>(n, times0, [&](const std::vector<H3>& xv, std::vector<H3>& yv) {
+    H.step0 = power_step<3>(n, times0, [&](const std::vector<H3>& xv, std::vector<H3>& yv) {
         for (int64_t i = 0; i < n; i++)
             for (int r = 0; r < 3; r++) {
                 double acc = 0.0;
@@ -752,13 +754,14 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
         for (int r = 0; r < 3; r++)
             for (int c = 0; c < 3; c++) f.diag[i][r][c] = diag[9 * i + 3 * r + c];
     }
+    f.pairs.reserve(npairs);
     for (int64_t p = 0; p < npairs; p++) {
         HPair e{pi[p], pj[p], HM6{}};
         for (int r = 0; r < 3; r++)
             for (int c = 0; c < 3; c++) e.m[r][c] = pb[9 * p + 3 * r + c];
         f.pairs.push_back(e);
     }
-    std::vector<HLevel> levels;
+    std::vector<HLevel>& levels = H.levels;
     double sz = size;
     HLevel next = coarsen(f, sz * 2.0);
     for (;;) {
@@ -776,6 +779,34 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
         levels.push_back(std::move(next));
         next = coarsen(levels.back().sys, sz * 2.0);
     }
+    return H;
+}
+
+void mech_levels(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
+                 const uint32_t* pi, const uint32_t* pj, const double* pb, double size, std::vector<int64_t>& sizes,
+                 std::vector<double>& steps) {
+    HostLevels H = make_levels(n, sites, at, diag, npairs, pi, pj, pb, size);
+    sizes.clear();
+    steps.assign(1, H.step0);
+    for (const HLevel& L : H.levels) {
+        sizes.push_back((int64_t)L.sys.diag.size());
+        steps.push_back(L.direct ? 0.0 : L.step);
+    }
+}
+
+// The levels of the system, then PCG from x (solve.rs:356-386, 485-538): the rounds taken,
+// -1 where the levels do not fit the system (not positive).
+int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
+               const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b, double* x, double tol,
+               double size, int32_t* nlevels) {
+    cudaStream_t st = ctx.stream;
+    MemStats* ms = &ctx.mem;
+    if (n == 0) return 0;
+    PhaseTimer pt(ctx);  // SC_TIMING=1 prints the phases
+    HostLevels HL = make_levels(n, sites, at, diag, npairs, pi, pj, pb, size);
+    const std::vector<double>& inv0 = HL.inv0;
+    const double step0 = HL.step0;
+    std::vector<HLevel>& levels = HL.levels;
     *nlevels = (int32_t)levels.size();
     pt.mark("mech: levels (host)");
     // to the device

@@ -125,6 +125,8 @@ def lib():
         L.sc_mech_voxel_system.argtypes = [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                            C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), P, P, P, P, P,
                                            P, P]
+        L.sc_mech_levels.argtypes = [C.c_int64, P, P, P, C.c_int64, P, P, P, C.c_double, C.c_int32, P, P,
+                                     C.POINTER(C.c_int32)]
         L.sc_mech_solve.argtypes = [P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, C.c_double, C.c_double,
                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.sc_used_standing.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
@@ -201,6 +203,24 @@ def mech_voxel_system(state, e, h: float = 0.125, dt: float = 1.0 / 60.0, mass: 
     if s != OK:
         raise StaticsError(s, "sc_mech_voxel_system")
     return out
+
+
+def mech_levels(system: dict, size: float | None = None):
+    """Only the levels the engine's solver makes for `system` (sc_mech_levels, host code):
+    (parts of each coarse level, smoother steps: the nodes' then each level's, 0 at the
+    direct top)."""
+    sites = np.ascontiguousarray(system["sites"], np.int64)
+    at = np.ascontiguousarray(system["at"], np.float64)
+    diag = np.ascontiguousarray(system["diag"], np.float64)
+    pi = np.ascontiguousarray(system["pi"], np.uint32)
+    pj = np.ascontiguousarray(system["pj"], np.uint32)
+    pb = np.ascontiguousarray(system["pb"], np.float64)
+    sizes, steps, nl = np.zeros(64, np.int64), np.zeros(65), C.c_int32()
+    s = lib().sc_mech_levels(len(sites), _ptr(sites), _ptr(at), _ptr(diag), len(pi), _ptr(pi), _ptr(pj), _ptr(pb),
+                             size or system["h"], 64, _ptr(sizes), _ptr(steps), C.byref(nl))
+    if s != OK:
+        raise StaticsError(s, "sc_mech_levels")
+    return list(sizes[:nl.value]), list(steps[:nl.value + 1])
 
 
 def launches() -> int:

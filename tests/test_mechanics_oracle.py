@@ -85,3 +85,16 @@ def test_library_system_matches_oracle(n, seed):
     for key in ("sites", "at", "diag", "pi", "pj", "pb", "b"):
         assert a[key].shape == b[key].shape, key
         assert np.array_equal(a[key], b[key]), key
+
+
+@pytest.mark.parametrize("n,E,seed", [(10, 1e6, 0), (16, 1e9, 4), (20, 1e9, 7)])
+def test_library_levels_match_oracle(n, E, seed):
+    """The levels the library makes on the host for the GPU solve (sc_mech_levels, no
+    device) are the oracle's Solver::new: the same parts on every level and the same
+    smoother steps, bit for bit (the same additions in the same order)."""
+    st, k = sc.generate_piece(n, n, n + 2, seed, sc.K_UNIFORM)
+    s = sc.mech_voxel_system(st, k * E, h=0.125, dt=1 / 60, mass=2000 * 0.125 ** 3)
+    sizes, steps = sc.mech_levels(s)
+    want_sizes, want_steps = M.levels(s)
+    assert [int(v) for v in sizes] == [int(v) for v in want_sizes]
+    assert steps == want_steps
