@@ -252,20 +252,32 @@ HLevel coarsen(const HSys& f, double size) {  // solve.rs:241-271
         return t;
     };
     for (size_t i = 0; i < nf; i++) plus(c.diag[L.of[i]], lift6(f.diag[i], L.r[i], L.r[i]));
-    std::map<std::pair<uint32_t, uint32_t>, HM6> map;
-    for (const HPair& e : f.pairs) {
+    // pairs within an aggregate go to its diagonal; the others are grouped by their (lesser,
+    // greater) parts, in (a, c) order, each group summed in the fine pairs' order (as a map
+    // from the key to a running sum would add them)
+    std::vector<std::pair<uint64_t, uint32_t>> across;
+    for (size_t q = 0; q < f.pairs.size(); q++) {
+        const HPair& e = f.pairs[q];
         const uint32_t a = L.of[e.i], b = L.of[e.j];
-        const HM6 m = lift6(e.m, L.r[e.i], L.r[e.j]);
         if (a == b) {
+            const HM6 m = lift6(e.m, L.r[e.i], L.r[e.j]);
             plus(c.diag[a], m);
             plus(c.diag[a], tr(m));
-        } else if (a < b) {
-            plus(map.emplace(std::make_pair(a, b), HM6{}).first->second, m);
         } else {
-            plus(map.emplace(std::make_pair(b, a), HM6{}).first->second, tr(m));
+            across.push_back({((uint64_t)std::min(a, b) << 32) | std::max(a, b), (uint32_t)q});
         }
     }
-    for (auto& kv : map) c.pairs.push_back(HPair{kv.first.first, kv.first.second, kv.second});
+    std::sort(across.begin(), across.end());
+    for (size_t g = 0; g < across.size();) {
+        const uint64_t key = across[g].first;
+        HM6 acc{};
+        for (; g < across.size() && across[g].first == key; g++) {
+            const HPair& e = f.pairs[across[g].second];
+            const HM6 m = lift6(e.m, L.r[e.i], L.r[e.j]);
+            plus(acc, L.of[e.i] < L.of[e.j] ? m : tr(m));
+        }
+        c.pairs.push_back(HPair{(uint32_t)(key >> 32), (uint32_t)key, acc});
+    }
     L.inv.resize(36 * (size_t)n);
     for (uint32_t p = 0; p < n; p++) {
         HM6 d = c.diag[p];
@@ -308,30 +320,71 @@ struct DLevel {
     DBuf<double> b, x, res, t;
 };
 
-// full block rows of a 6x6 system: the diagonal and each pair both ways
-void upload_rows(Context& ctx, const HSys& s, DLevel& D) {
-    const int64_t n = (int64_t)s.diag.size();
-    std::vector<std::vector<std::pair<int32_t, HM6>>> rows(n);
-    for (int64_t p = 0; p < n; p++) rows[p].push_back({(int32_t)p, s.diag[p]});
-    for (const HPair& e : s.pairs) {
-        HM6 t;
-        for (int r = 0; r < 6; r++)
-            for (int c = 0; c < 6; c++) t[r][c] = e.m[c][r];
-        rows[e.i].push_back({(int32_t)e.j, e.m});
-        rows[e.j].push_back({(int32_t)e.i, t});
+// Full block rows (B x B blocks) of a symmetric system from its diagonal blocks and its
+// pairs (i, j, M: M in row i, column j, M' in row j, column i), columns in order: counted,
+// placed, then each row's few entries sorted by column.
+template <int B, class DiagAt, class PairAt>
+void block_rows(int64_t n, int64_t npairs, const uint32_t* pi, const uint32_t* pj, DiagAt diag_at, PairAt pair_at,
+                std::vector<int64_t>& rp, std::vector<int32_t>& col, std::vector<double>& val) {
+    rp.assign(n + 1, 0);
+    for (int64_t p = 0; p < n; p++) rp[p + 1] = 1;
+    for (int64_t e = 0; e < npairs; e++) {
+        rp[pi[e] + 1]++;
+        rp[pj[e] + 1]++;
     }
-    std::vector<int64_t> rp(n + 1, 0);
+    for (int64_t p = 0; p < n; p++) rp[p + 1] += rp[p];
+    const int64_t nnz = rp[n];
+    // per entry: its column and its source (2 e + 1: pair e transposed; 2 e: pair e; -1 - p: diagonal p)
+    std::vector<int32_t> c(nnz);
+    std::vector<int64_t> src(nnz);
+    std::vector<int64_t> pos(rp.begin(), rp.end() - 1);
+    for (int64_t p = 0; p < n; p++) {
+        c[pos[p]] = (int32_t)p;
+        src[pos[p]++] = -1 - p;
+    }
+    for (int64_t e = 0; e < npairs; e++) {
+        c[pos[pi[e]]] = (int32_t)pj[e];
+        src[pos[pi[e]]++] = 2 * e;
+        c[pos[pj[e]]] = (int32_t)pi[e];
+        src[pos[pj[e]]++] = 2 * e + 1;
+    }
+    std::vector<int64_t> idx;
+    col.resize(nnz);
+    val.resize((size_t)nnz * B * B);
+    for (int64_t p = 0; p < n; p++) {
+        idx.resize(rp[p + 1] - rp[p]);
+        for (size_t t = 0; t < idx.size(); t++) idx[t] = rp[p] + (int64_t)t;
+        std::sort(idx.begin(), idx.end(), [&](int64_t u, int64_t v) { return c[u] < c[v]; });
+        for (size_t t = 0; t < idx.size(); t++) {
+            const int64_t k = rp[p] + (int64_t)t, from = src[idx[t]];
+            col[k] = c[idx[t]];
+            double* out = val.data() + (size_t)k * B * B;
+            if (from < 0) {
+                for (int r = 0; r < B; r++)
+                    for (int q = 0; q < B; q++) out[B * r + q] = diag_at(-1 - from, r, q);
+            } else {
+                const int64_t e = from >> 1;
+                const bool t2 = from & 1;
+                for (int r = 0; r < B; r++)
+                    for (int q = 0; q < B; q++) out[B * r + q] = t2 ? pair_at(e, q, r) : pair_at(e, r, q);
+            }
+        }
+    }
+}
+
+void upload_rows(Context& ctx, const HSys& s, DLevel& D) {
+    const int64_t n = (int64_t)s.diag.size(), m = (int64_t)s.pairs.size();
+    std::vector<uint32_t> pi(m), pj(m);
+    for (int64_t e = 0; e < m; e++) {
+        pi[e] = s.pairs[e].i;
+        pj[e] = s.pairs[e].j;
+    }
+    std::vector<int64_t> rp;
     std::vector<int32_t> col;
     std::vector<double> val;
-    for (int64_t p = 0; p < n; p++) {
-        std::sort(rows[p].begin(), rows[p].end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-        for (auto& e : rows[p]) {
-            col.push_back(e.first);
-            for (int r = 0; r < 6; r++)
-                for (int c = 0; c < 6; c++) val.push_back(e.second[r][c]);
-        }
-        rp[p + 1] = (int64_t)col.size();
-    }
+    block_rows<6>(
+        n, m, pi.data(), pj.data(), [&](int64_t p, int r, int q) { return s.diag[p][r][q]; },
+        [&](int64_t e, int r, int q) { return s.pairs[e].m[r][q]; }, rp, col, val);
     D.nnzb = (int64_t)col.size();
     D.rowptr.alloc(n + 1, ctx.stream, &ctx.mem);
     D.rowptr.upload(rp.data(), n + 1);
@@ -814,33 +867,12 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
     S.n0 = n;
     S.step0 = step0;
     {
-        std::vector<std::vector<std::pair<int32_t, std::array<double, 9>>>> rows(n);
-        for (int64_t i = 0; i < n; i++) {
-            std::array<double, 9> d;
-            std::copy(diag + 9 * i, diag + 9 * i + 9, d.begin());
-            rows[i].push_back({(int32_t)i, d});
-        }
-        for (int64_t p = 0; p < npairs; p++) {
-            std::array<double, 9> m, t;
-            for (int r = 0; r < 3; r++)
-                for (int c = 0; c < 3; c++) {
-                    m[3 * r + c] = pb[9 * p + 3 * r + c];
-                    t[3 * r + c] = pb[9 * p + 3 * c + r];
-                }
-            rows[pi[p]].push_back({(int32_t)pj[p], m});
-            rows[pj[p]].push_back({(int32_t)pi[p], t});
-        }
-        std::vector<int64_t> rp(n + 1, 0);
+        std::vector<int64_t> rp;
         std::vector<int32_t> col;
         std::vector<double> val;
-        for (int64_t i = 0; i < n; i++) {
-            std::sort(rows[i].begin(), rows[i].end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-            for (auto& e : rows[i]) {
-                col.push_back(e.first);
-                val.insert(val.end(), e.second.begin(), e.second.end());
-            }
-            rp[i + 1] = (int64_t)col.size();
-        }
+        block_rows<3>(
+            n, npairs, pi, pj, [&](int64_t p, int r, int q) { return diag[9 * p + 3 * r + q]; },
+            [&](int64_t e, int r, int q) { return pb[9 * e + 3 * r + q]; }, rp, col, val);
         S.rowptr0.alloc(n + 1, st, ms);
         S.rowptr0.upload(rp.data(), n + 1);
         S.col0.alloc(col.size(), st, ms);
