@@ -13,6 +13,8 @@
 #include <array>
 #include <cmath>
 #include <map>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -143,23 +145,6 @@ struct HLevel {  // solve.rs:188-203
     std::vector<double> top_inv;  // (6n)^2, the direct level's inverse operator
 };
 
-void apply6(const HSys& s, const std::vector<H6>& x, std::vector<H6>& y) {  // solve.rs:306-317
-    for (size_t p = 0; p < s.diag.size(); p++)
-        for (int r = 0; r < 6; r++) {
-            double acc = 0.0;
-            for (int c = 0; c < 6; c++) acc += s.diag[p][r][c] * x[p][c];
-            y[p][r] = acc;
-        }
-    for (const HPair& e : s.pairs)
-        for (int r = 0; r < 6; r++) {
-            double a = 0.0, c2 = 0.0;
-            for (int c = 0; c < 6; c++) a += e.m[r][c] * x[e.j][c];
-            for (int c = 0; c < 6; c++) c2 += e.m[c][r] * x[e.i][c];
-            y[e.i][r] += a;
-            y[e.j][r] += c2;
-        }
-}
-
 // 4/3 over the largest eigenvalue of over(apply), ten power steps from the reference's
 // start (solve.rs:274-296)
 template <size_t N, class Apply, class Over>
@@ -207,13 +192,123 @@ void factor_top(HLevel& L) {  // solve.rs:320-347
     L.direct = true;
 }
 
-HLevel coarsen(const HSys& f, double size) {  // solve.rs:241-271
-    const size_t nf = f.keys.size();
+// The finer level seen by coarsen: a coarse HSys, or the nodes' arrays with their 3x3
+// blocks embedded as 6x6 when read (solve.rs:97-103) rather than stored.
+struct FineHSys {
+    const HSys& s;
+    size_t n() const { return s.keys.size(); }
+    size_t npairs() const { return s.pairs.size(); }
+    const std::array<int64_t, 3>& key(size_t i) const { return s.keys[i]; }
+    H3 at(size_t i) const { return s.at[i]; }
+    HM6 diag(size_t i) const { return s.diag[i]; }
+    uint32_t pi(size_t q) const { return s.pairs[q].i; }
+    uint32_t pj(size_t q) const { return s.pairs[q].j; }
+    HM6 pair(size_t q) const { return s.pairs[q].m; }
+};
+struct FineNodes {
+    int64_t nn, np;
+    const int64_t* sites;
+    const double *at_, *diag_;
+    const uint32_t *pi_, *pj_;
+    const double* pb;
+    std::vector<std::array<int64_t, 3>> keys;
+    FineNodes(int64_t n, const int64_t* s, const double* a, const double* d, int64_t m, const uint32_t* i,
+              const uint32_t* j, const double* b)
+        : nn(n), np(m), sites(s), at_(a), diag_(d), pi_(i), pj_(j), pb(b), keys(n) {
+        for (int64_t q = 0; q < n; q++) keys[q] = {s[3 * q], s[3 * q + 1], s[3 * q + 2]};
+    }
+    static HM6 embed(const double* m) {
+        HM6 e{};
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) e[r][c] = m[3 * r + c];
+        return e;
+    }
+    size_t n() const { return (size_t)nn; }
+    size_t npairs() const { return (size_t)np; }
+    const std::array<int64_t, 3>& key(size_t i) const { return keys[i]; }
+    H3 at(size_t i) const { return H3{at_[3 * i], at_[3 * i + 1], at_[3 * i + 2]}; }
+    HM6 diag(size_t i) const { return embed(diag_ + 9 * i); }
+    uint32_t pi(size_t q) const { return pi_[q]; }
+    uint32_t pj(size_t q) const { return pj_[q]; }
+    HM6 pair(size_t q) const { return embed(pb + 9 * q); }
+};
+
+// f(lo, hi) over [0, n) split among the host's cores
+template <class F>
+void parallel_ranges(size_t n, F f) {
+    const size_t T = std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+    if (n < 4096 || T == 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < T; t++) th.emplace_back(f, n * t / T, n * (t + 1) / T);
+    for (auto& x : th) x.join();
+}
+
+// Each part's pairs in pair order (entry 2 q + side: side 0 where the part is the pair's
+// first, 1 its second), so a product can run part by part on the host's cores and still
+// add each part's terms in the order the reference's pair loop adds them
+// (solve.rs:63-73, 306-317): the same values, bit for bit.
+struct Incidence {
+    std::vector<int64_t> ptr;
+    std::vector<uint64_t> ent;
+    template <class PI, class PJ>
+    Incidence(size_t n, size_t np, PI pi, PJ pj) : ptr(n + 1, 0), ent(2 * np) {
+        for (size_t q = 0; q < np; q++) {
+            ptr[pi(q) + 1]++;
+            ptr[pj(q) + 1]++;
+        }
+        for (size_t i = 0; i < n; i++) ptr[i + 1] += ptr[i];
+        std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+        for (size_t q = 0; q < np; q++) {
+            ent[fill[pi(q)]++] = 2 * (uint64_t)q;
+            ent[fill[pj(q)]++] = 2 * (uint64_t)q + 1;
+        }
+    }
+};
+
+// y = S x over B-vectors: diag(i, r, c) the diagonal blocks, pair(q, r, c) the pairs'
+template <int B, class Diag, class Pair, class PI, class PJ>
+void apply_rows(size_t n, const Incidence& inc, Diag diag, Pair pair, PI pi, PJ pj,
+                const std::vector<std::array<double, B>>& x, std::vector<std::array<double, B>>& y) {
+    parallel_ranges(n, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; i++) {
+            for (int r = 0; r < B; r++) {
+                double acc = 0.0;
+                for (int c = 0; c < B; c++) acc += diag(i, r, c) * x[i][c];
+                y[i][r] = acc;
+            }
+            for (int64_t t = inc.ptr[i]; t < inc.ptr[i + 1]; t++) {
+                const size_t q = (size_t)(inc.ent[t] >> 1);
+                if ((inc.ent[t] & 1) == 0) {
+                    const size_t j = pj(q);
+                    for (int r = 0; r < B; r++) {
+                        double a = 0.0;
+                        for (int c = 0; c < B; c++) a += pair(q, r, c) * x[j][c];
+                        y[i][r] += a;
+                    }
+                } else {
+                    const size_t j = pi(q);
+                    for (int r = 0; r < B; r++) {
+                        double a = 0.0;
+                        for (int c = 0; c < B; c++) a += pair(q, c, r) * x[j][c];
+                        y[i][r] += a;
+                    }
+                }
+            }
+        }
+    });
+}
+
+template <class Fine>
+HLevel coarsen(const Fine& f, double size) {  // solve.rs:241-271
+    const size_t nf = f.n();
     std::vector<size_t> up(nf);
     for (size_t i = 0; i < nf; i++) up[i] = i;
-    for (const HPair& e : f.pairs)
-        if (parent_key(f.keys[e.i]) == parent_key(f.keys[e.j])) {
-            size_t r = uf_find(up, e.i), s = uf_find(up, e.j);
+    for (size_t q = 0; q < f.npairs(); q++)
+        if (parent_key(f.key(f.pi(q))) == parent_key(f.key(f.pj(q)))) {
+            size_t r = uf_find(up, f.pi(q)), s = uf_find(up, f.pj(q));
             up[std::max(r, s)] = std::min(r, s);
         }
     HLevel L;
@@ -231,15 +326,18 @@ HLevel coarsen(const HSys& f, double size) {  // solve.rs:241-271
     std::vector<double> count(n, 0.0);
     for (size_t i = 0; i < nf; i++) {
         const uint32_t a = L.of[i];
-        for (int k = 0; k < 3; k++) c.at[a][k] = c.at[a][k] + f.at[i][k];
+        const H3 x = f.at(i);
+        for (int k = 0; k < 3; k++) c.at[a][k] = c.at[a][k] + x[k];
         count[a] += 1.0;
-        c.keys[a] = parent_key(f.keys[i]);
+        c.keys[a] = parent_key(f.key(i));
     }
     for (uint32_t a = 0; a < n; a++)
         for (int k = 0; k < 3; k++) c.at[a][k] = c.at[a][k] * (1.0 / count[a]);
     L.r.resize(nf);
-    for (size_t i = 0; i < nf; i++)
-        for (int k = 0; k < 3; k++) L.r[i][k] = f.at[i][k] - c.at[L.of[i]][k];
+    for (size_t i = 0; i < nf; i++) {
+        const H3 x = f.at(i);
+        for (int k = 0; k < 3; k++) L.r[i][k] = x[k] - c.at[L.of[i]][k];
+    }
     c.diag.assign(n, HM6{});
     auto plus = [](HM6& a, const HM6& b) {
         for (int r = 0; r < 6; r++)
@@ -251,32 +349,69 @@ HLevel coarsen(const HSys& f, double size) {  // solve.rs:241-271
             for (int cc = 0; cc < 6; cc++) t[r][cc] = m[cc][r];
         return t;
     };
-    for (size_t i = 0; i < nf; i++) plus(c.diag[L.of[i]], lift6(f.diag[i], L.r[i], L.r[i]));
-    // pairs within an aggregate go to its diagonal; the others are grouped by their (lesser,
-    // greater) parts, in (a, c) order, each group summed in the fine pairs' order (as a map
-    // from the key to a running sum would add them)
-    std::vector<std::pair<uint64_t, uint32_t>> across;
-    for (size_t q = 0; q < f.pairs.size(); q++) {
-        const HPair& e = f.pairs[q];
-        const uint32_t a = L.of[e.i], b = L.of[e.j];
-        if (a == b) {
-            const HM6 m = lift6(e.m, L.r[e.i], L.r[e.j]);
-            plus(c.diag[a], m);
-            plus(c.diag[a], tr(m));
-        } else {
-            across.push_back({((uint64_t)std::min(a, b) << 32) | std::max(a, b), (uint32_t)q});
-        }
+    // Each aggregate's block: its members' lifted blocks in member order, then its inner
+    // pairs' (m + m') in pair order; each pair across two aggregates (a < c) summed in
+    // pair order into block (a, c); blocks in (a, c) order. That is the order the
+    // reference adds them in (solve.rs:254-262), here computed aggregate by aggregate and
+    // group by group on the host's cores.
+    std::vector<std::pair<uint64_t, uint32_t>> pairs_by;  // ((lesser, greater) part, fine pair)
+    pairs_by.reserve(f.npairs());
+    for (size_t q = 0; q < f.npairs(); q++) {
+        const uint32_t a = L.of[f.pi(q)], b = L.of[f.pj(q)];
+        pairs_by.push_back({((uint64_t)std::min(a, b) << 32) | std::max(a, b), (uint32_t)q});
     }
-    std::sort(across.begin(), across.end());
-    for (size_t g = 0; g < across.size();) {
-        const uint64_t key = across[g].first;
-        HM6 acc{};
-        for (; g < across.size() && across[g].first == key; g++) {
-            const HPair& e = f.pairs[across[g].second];
-            const HM6 m = lift6(e.m, L.r[e.i], L.r[e.j]);
-            plus(acc, L.of[e.i] < L.of[e.j] ? m : tr(m));
+    std::sort(pairs_by.begin(), pairs_by.end());
+    std::vector<int64_t> mptr(n + 1, 0);
+    for (size_t i = 0; i < nf; i++) mptr[L.of[i] + 1]++;
+    for (uint32_t a = 0; a < n; a++) mptr[a + 1] += mptr[a];
+    std::vector<uint32_t> mem(nf);
+    {
+        std::vector<int64_t> fill(mptr.begin(), mptr.end() - 1);
+        for (size_t i = 0; i < nf; i++) mem[fill[L.of[i]]++] = (uint32_t)i;
+    }
+    parallel_ranges(n, [&](size_t lo, size_t hi) {
+        for (size_t a = lo; a < hi; a++)
+            for (int64_t t = mptr[a]; t < mptr[a + 1]; t++) {
+                const uint32_t i = mem[t];
+                plus(c.diag[a], lift6(f.diag(i), L.r[i], L.r[i]));
+            }
+    });
+    // group starts, then the groups on the cores (each thread's blocks in order)
+    std::vector<size_t> gstart;
+    for (size_t g = 0; g < pairs_by.size(); g++)
+        if (g == 0 || pairs_by[g].first != pairs_by[g - 1].first) gstart.push_back(g);
+    gstart.push_back(pairs_by.size());
+    const size_t ng = gstart.size() - 1;
+    std::vector<std::vector<HPair>> part_pairs(std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency())));
+    std::vector<size_t> part_of_lo;
+    std::mutex mu;
+    parallel_ranges(ng, [&](size_t lo, size_t hi) {
+        std::vector<HPair> mine;
+        for (size_t gi = lo; gi < hi; gi++) {
+            const uint64_t key = pairs_by[gstart[gi]].first;
+            const uint32_t a = (uint32_t)(key >> 32), b = (uint32_t)key;
+            HM6 acc{};
+            for (size_t g = gstart[gi]; g < gstart[gi + 1]; g++) {
+                const uint32_t q = pairs_by[g].second;
+                const HM6 m = lift6(f.pair(q), L.r[f.pi(q)], L.r[f.pj(q)]);
+                if (a == b) {
+                    plus(c.diag[a], m);
+                    plus(c.diag[a], tr(m));
+                } else {
+                    plus(acc, L.of[f.pi(q)] < L.of[f.pj(q)] ? m : tr(m));
+                }
+            }
+            if (a != b) mine.push_back(HPair{a, b, acc});
         }
-        c.pairs.push_back(HPair{(uint32_t)(key >> 32), (uint32_t)key, acc});
+        std::lock_guard<std::mutex> lock(mu);
+        part_of_lo.push_back(lo);
+        part_pairs[part_of_lo.size() - 1] = std::move(mine);
+    });
+    {
+        std::vector<size_t> order(part_of_lo.size());
+        for (size_t t = 0; t < order.size(); t++) order[t] = t;
+        std::sort(order.begin(), order.end(), [&](size_t u, size_t v) { return part_of_lo[u] < part_of_lo[v]; });
+        for (size_t t : order) c.pairs.insert(c.pairs.end(), part_pairs[t].begin(), part_pairs[t].end());
     }
     L.inv.resize(36 * (size_t)n);
     for (uint32_t p = 0; p < n; p++) {
@@ -290,8 +425,16 @@ HLevel coarsen(const HSys& f, double size) {  // solve.rs:241-271
         std::copy(iv.begin(), iv.end(), L.inv.begin() + 36 * (size_t)p);
     }
     L.size = size;
+    const Incidence inc(n, c.pairs.size(), [&](size_t q) { return c.pairs[q].i; },
+                        [&](size_t q) { return c.pairs[q].j; });
     L.step = power_step<6>(
-        n, [&](const std::vector<H6>& x, std::vector<H6>& y) { apply6(c, x, y); },
+        n,
+        [&](const std::vector<H6>& x, std::vector<H6>& y) {
+            apply_rows<6>(
+                n, inc, [&](size_t i, int r, int cc) { return c.diag[i][r][cc]; },
+                [&](size_t q, int r, int cc) { return c.pairs[q].m[r][cc]; }, [&](size_t q) { return c.pairs[q].i; },
+                [&](size_t q) { return c.pairs[q].j; }, x, y);
+        },
         [&](const std::vector<H6>& x, std::vector<H6>& y) {
             for (uint32_t p = 0; p < n; p++)
                 for (int r = 0; r < 6; r++) {
@@ -768,23 +911,12 @@ static HostLevels make_levels(int64_t n, const int64_t* sites, const double* at,
         std::vector<double> iv = chol_inverse(std::move(a), 3);
         std::copy(iv.begin(), iv.end(), inv0.begin() + 9 * i);
     }
+    const Incidence inc0((size_t)n, (size_t)npairs, [&](size_t q) { return pi[q]; }, [&](size_t q) { return pj[q]; });
     auto times0 = [&](const std::vector<H3>& xv, std::vector<H3>& yv) {  // solve.rs:63-73
-        for (int64_t i = 0; i < n; i++)
-            for (int r = 0; r < 3; r++) {
-                double acc = 0.0;
-                for (int c = 0; c < 3; c++) acc += diag[9 * i + 3 * r + c] * xv[i][c];
-                yv[i][r] = acc;
-            }
-        for (int64_t p = 0; p < npairs; p++) {
-            const double* m = pb + 9 * p;
-            for (int r = 0; r < 3; r++) {
-                double a = 0.0, c2 = 0.0;
-                for (int c = 0; c < 3; c++) a += m[3 * r + c] * xv[pj[p]][c];
-                for (int c = 0; c < 3; c++) c2 += m[3 * c + r] * xv[pi[p]][c];
-                yv[pi[p]][r] += a;
-                yv[pj[p]][r] += c2;
-            }
-        }
+        apply_rows<3>(
+            (size_t)n, inc0, [&](size_t i, int r, int c) { return diag[9 * i + 3 * r + c]; },
+            [&](size_t q, int r, int c) { return pb[9 * q + 3 * r + c]; }, [&](size_t q) { return pi[q]; },
+            [&](size_t q) { return pj[q]; }, xv, yv);
     };
     H.step0 = power_step<3>(n, times0, [&](const std::vector<H3>& xv, std::vector<H3>& yv) {
         for (int64_t i = 0; i < n; i++)
@@ -795,28 +927,9 @@ static HostLevels make_levels(int64_t n, const int64_t* sites, const double* at,
             }
     });
     // the coarse levels (solve.rs:365-385)
-    HSys f;
-    f.keys.resize(n);
-    f.at.resize(n);
-    f.diag.assign(n, HM6{});
-    for (int64_t i = 0; i < n; i++) {
-        for (int k = 0; k < 3; k++) {
-            f.keys[i][k] = sites[3 * i + k];
-            f.at[i][k] = at[3 * i + k];
-        }
-        for (int r = 0; r < 3; r++)
-            for (int c = 0; c < 3; c++) f.diag[i][r][c] = diag[9 * i + 3 * r + c];
-    }
-    f.pairs.reserve(npairs);
-    for (int64_t p = 0; p < npairs; p++) {
-        HPair e{pi[p], pj[p], HM6{}};
-        for (int r = 0; r < 3; r++)
-            for (int c = 0; c < 3; c++) e.m[r][c] = pb[9 * p + 3 * r + c];
-        f.pairs.push_back(e);
-    }
     std::vector<HLevel>& levels = H.levels;
     double sz = size;
-    HLevel next = coarsen(f, sz * 2.0);
+    HLevel next = coarsen(FineNodes(n, sites, at, diag, npairs, pi, pj, pb), sz * 2.0);
     for (;;) {
         sz *= 2.0;
         const size_t nn = next.sys.diag.size(), before = levels.empty() ? (size_t)n : levels.back().sys.diag.size();
@@ -830,7 +943,7 @@ static HostLevels make_levels(int64_t n, const int64_t* sites, const double* at,
             break;
         }
         levels.push_back(std::move(next));
-        next = coarsen(levels.back().sys, sz * 2.0);
+        next = coarsen(FineHSys{levels.back().sys}, sz * 2.0);
     }
     return H;
 }
