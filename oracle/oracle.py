@@ -56,6 +56,12 @@ def lib():
         L.or_invert.argtypes = [pd, pd]
         L.or_coarse_site.argtypes = [pi64, C.c_uint32, pi64]
         L.or_coarse_site.restype = I64
+        L.or_block.restype = P
+        L.or_block.argtypes = [C.c_int, pd, pd, pd, C.c_int]
+        L.or_gather.restype = P
+        L.or_gather.argtypes = [P, C.c_int]
+        L.or_full.argtypes = [C.c_int, pd]
+        L.or_materials.argtypes = [P, pi32, pi32, pd]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_threads.restype = C.c_int
         _lib = L
@@ -94,6 +100,15 @@ class Lattice:
     def scene(cls, kind: str, mat: int = STONE, a: float = 0, b: float = 0, c: float = 0, level: int = 0):
         kinds = {"cantilever": 0, "tree": 1, "portico": 2, "rock": 3, "tower": 4, "pendant": 5}
         return cls(lib().or_scene(kinds[kind], mat, a, b, c, level))
+
+    @classmethod
+    def block(cls, mat: int, lo, hi, half, level: int = 0):
+        """Every site of solids(level, lo, hi) whose centre lies strictly inside the box
+        |x_k| < half[k], of material `mat`, free (lattice.rs:87-163)."""
+        lo, hi, half = (np.ascontiguousarray(v, dtype=np.float64) for v in (lo, hi, half))
+        lat = cls(lib().or_block(int(mat), _p(lo, C.c_double), _p(hi, C.c_double), _p(half, C.c_double), level))
+        lat.level = level
+        return lat
 
     @classmethod
     def grid(cls, state: np.ndarray, k: np.ndarray, g_over_e: float = 0.4, rho: float = 512.0):
@@ -185,11 +200,35 @@ class Lattice:
     def as_generated(self, generated: "Lattice") -> None:
         lib().or_as_generated(self.h, generated.h)
 
+    def gathered(self, against_full: bool = True) -> "Lattice":
+        """gather.rs:193-195 (or measured(fine, false), gather.rs:230-395): the next
+        level up, each coarse cell's beams measured from this lattice's matter."""
+        lat = Lattice(lib().or_gather(self.h, 1 if against_full else 0))
+        lat.level = getattr(self, "level", 0) + 1
+        return lat
+
+    def materials(self) -> dict:
+        """Per node its material (index into STONE..LEAVES, -1 other); per bond its
+        material and its strength over the material's own (Mat::stronger)."""
+        out = dict(node=np.zeros(self.n_nodes, np.int32), bond=np.zeros(self.n_bonds, np.int32),
+                   stronger=np.zeros(self.n_bonds))
+        lib().or_materials(self.h, _p(out["node"], C.c_int32), _p(out["bond"], C.c_int32),
+                           _p(out["stronger"], C.c_double))
+        return out
+
     def level0_apply(self, x_parts: np.ndarray) -> np.ndarray:
         x_parts = np.ascontiguousarray(x_parts, dtype=np.float64)
         y = np.zeros_like(x_parts)
         lib().or_level0_apply(self.h, x_parts.shape[0], _p(x_parts, C.c_double), _p(y, C.c_double))
         return y
+
+
+def full(mat: int) -> np.ndarray:
+    """gather.rs:203-226: a full cell of `mat` measured a level up, by class (180°,
+    90°): rows of (section / s^2, strength / the material's)."""
+    out = np.zeros(4)
+    lib().or_full(int(mat), _p(out, C.c_double))
+    return out.reshape(2, 2)
 
 
 def invert(m: np.ndarray) -> np.ndarray:

@@ -1,7 +1,9 @@
 // ORACLE — test infrastructure only. A flat C interface over the restatement so that
 // tests/ and bench.py's CPU-baseline leg can drive it through ctypes.
 #include <chrono>
+#include <cmath>
 #include <cstring>
+#include <exception>
 #include <memory>
 
 #include "statics_oracle.hpp"
@@ -40,6 +42,23 @@ void* or_scene(int kind, int mat, double a, double b, double c, int level) {
     auto* h = new Handle;
     h->lat = s.build_at((uint32_t)level);
     return h;
+}
+
+// build(level, solids(level, lo, hi, fill)) (lattice.rs:87-163) with the fill taking
+// every site whose centre x has |x_k| < half[k] on each axis, of material `mat`, free:
+// the steel bar of gather.rs:403-405 and the full block of statics.rs:352.
+void* or_block(int mat, const double* lo, const double* hi, const double* half, int level) {
+    const Mat m = *mat_of(mat);
+    V3 h{half[0], half[1], half[2]};
+    Fill fill = [m, h](V3 x, Mat& out, bool& held) {
+        if (!(std::fabs(x[0]) < h[0] && std::fabs(x[1]) < h[1] && std::fabs(x[2]) < h[2])) return false;
+        out = m;
+        held = false;
+        return true;
+    };
+    auto* hd = new Handle;
+    hd->lat = build((uint32_t)level, solids((uint32_t)level, V3{lo[0], lo[1], lo[2]}, V3{hi[0], hi[1], hi[2]}, fill));
+    return hd;
 }
 
 void* or_grid(int nx, int ny, int nz, const uint8_t* state, const float* k, double g_over_e, double rho) {
@@ -213,6 +232,47 @@ void or_invert(const double* m, double* out) {
     M6 inv = invert(a);
     for (int r = 0; r < 6; r++)
         for (int c = 0; c < 6; c++) out[6 * r + c] = inv[r][c];
+}
+
+// gather.rs:193-195 (against_full != 0) or measured(fine, false), gather.rs:230-395:
+// the next level up, as a new lattice handle (NULL where the restatement throws).
+void* or_gather(void* p, int against_full) {
+    try {
+        auto* h = new Handle;
+        h->lat = measured(static_cast<Handle*>(p)->lat, against_full != 0);
+        return h;
+    } catch (const std::exception&) {
+        return nullptr;
+    }
+}
+
+// gather.rs:203-226 for material `mat`: per class (180°, 90°) the section over the
+// spacing squared and the strength over the material's; out holds 4 values.
+void or_full(int mat, double* out) {
+    Full f = full(*mat_of(mat));
+    for (int k = 0; k < 2; k++) {
+        out[2 * k] = f[k].first;
+        out[2 * k + 1] = f[k].second;
+    }
+}
+
+// Each node's material as an index into (stone, wood, masonry, soil, steel, leaves),
+// -1 for another; each bond's tensile strength over its material's own (Mat::stronger).
+void or_materials(void* p, int32_t* node_mat, int32_t* bond_mat, double* bond_stronger) {
+    static const Mat* all[6] = {&STONE, &WOOD, &MASONRY, &SOIL, &STEEL, &LEAVES};
+    auto index = [&](const Mat& m) {
+        for (int k = 0; k < 6; k++)
+            if (std::strcmp(all[k]->name, m.name) == 0) return k;
+        return -1;
+    };
+    const Lattice& L = static_cast<Handle*>(p)->lat;
+    for (size_t v = 0; v < L.nodes.size(); v++)
+        if (node_mat) node_mat[v] = index(L.nodes[v].mat);
+    for (size_t b = 0; b < L.bonds.size(); b++) {
+        int k = index(L.bonds[b].mat);
+        if (bond_mat) bond_mat[b] = k;
+        if (bond_stronger) bond_stronger[b] = k >= 0 ? L.bonds[b].mat.ft / all[k]->ft : 0.0;
+    }
 }
 
 int64_t or_coarse_site(const int64_t* p, uint32_t l, int64_t* out) {

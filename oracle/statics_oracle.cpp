@@ -242,26 +242,6 @@ int threads() {
     return h ? (int)h : 1;
 }
 
-// bodies.rs:51-69: contiguous chunks over the threads, sequential below 256.
-template <class T, class F>
-static std::vector<T> each(size_t n, const F& f) {
-    size_t th = (size_t)threads();
-    std::vector<T> out(n);
-    if (n < 256 || th == 1) {
-        for (size_t i = 0; i < n; i++) out[i] = f(i);
-        return out;
-    }
-    size_t size = (n + th - 1) / th;
-    std::vector<std::thread> pool;
-    for (size_t start = 0; start < n; start += size) {
-        size_t end = std::min(n, start + size);
-        pool.emplace_back([&, start, end] {
-            for (size_t i = start; i < end; i++) out[i] = f(i);
-        });
-    }
-    for (auto& t : pool) t.join();
-    return out;
-}
 
 // Rust's `(0..6).map(..).sum()`: a left fold (from -0.0; 0.0 here, which differs
 // only in the sign of an all-zero sum).
@@ -699,7 +679,7 @@ static std::vector<Six> cycle(const std::vector<Level>& levels, size_t l, const 
     return x;
 }
 
-static size_t find(std::vector<size_t>& p, size_t a) {  // bodies.rs:628-634
+size_t find(std::vector<size_t>& p, size_t a) {  // bodies.rs:628-634
     while (p[a] != a) {
         p[a] = p[p[a]];
         a = p[a];

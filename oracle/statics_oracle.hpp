@@ -12,12 +12,15 @@
 // by the reference's `cells_nest` test (statics/src/lattice.rs:170-181) and by the
 // known answers its docs publish (docs/statics.md:236-247), reproduced in tests/.
 #pragma once
+#include <algorithm>
 #include <array>
 #include <cstdint>
 #include <functional>
 #include <memory>
 #include <optional>
 #include <string>
+#include <thread>
+#include <tuple>
 #include <vector>
 
 namespace oracle {
@@ -108,6 +111,29 @@ Six shift(Six x, V3 r);  // bodies.rs:44-47
 void set_threads(int n);
 int threads();
 
+// bodies.rs:51-69: contiguous chunks over the threads, sequential below 256.
+template <class T, class F>
+std::vector<T> each(size_t n, const F& f) {
+    size_t th = (size_t)threads();
+    std::vector<T> out(n);
+    if (n < 256 || th == 1) {
+        for (size_t i = 0; i < n; i++) out[i] = f(i);
+        return out;
+    }
+    size_t size = (n + th - 1) / th;
+    std::vector<std::thread> pool;
+    for (size_t start = 0; start < n; start += size) {
+        size_t end = std::min(n, start + size);
+        pool.emplace_back([&, start, end] {
+            for (size_t i = start; i < end; i++) out[i] = f(i);
+        });
+    }
+    for (auto& t : pool) t.join();
+    return out;
+}
+
+size_t find(std::vector<size_t>& p, size_t a);  // bodies.rs:628-634
+
 /// What one `motions` call built and did, for parity checks against the GPU path.
 struct Hierarchy {
     std::vector<size_t> counts;             // parts per level
@@ -148,6 +174,20 @@ void as_generated(Lattice& lattice, const Lattice& generated);  // bodies.rs:611
 M6 invert(const M6& m);                  // bodies.rs:576-602
 /// Level 0's operator alone (Level::new + apply), all bonds alive, no node gone.
 std::vector<Six> level0_apply(const Lattice& lattice, const std::vector<Six>& x_parts);
+
+// ---- statics/src/gather.rs -----------------------------------------------------
+/// A full cell's beams by class (180°, 90°): section over the spacing squared, and
+/// how much stronger than the material (gather.rs:199-226).
+using Full = std::array<std::pair<double, double>, 2>;
+Full full(const Mat& mat);                                 // gather.rs:203-226
+Lattice measured(const Lattice& fine, bool against_full);  // gather.rs:230-395
+Lattice gathered(const Lattice& fine);                     // gather.rs:193-195
+/// gather.rs:164-184: Gauss–Jordan with `rhs` right-hand columns; rows of the answer.
+std::vector<std::vector<double>> gather_solve(std::vector<std::vector<double>> a, size_t rhs);
+/// gather.rs:119-161: (a, b, stiffness) of the beams nearest the handles' stiffness k.
+std::vector<std::tuple<size_t, size_t, double>> gather_beams(const std::vector<std::vector<double>>& k,
+                                                             const std::vector<V3>& at,
+                                                             const std::function<bool(size_t, size_t)>& joined);
 
 // ---- restated example scenes (statics/examples/statics.rs) ---------------------
 struct Scene {
