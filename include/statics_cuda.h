@@ -242,6 +242,49 @@ sc_status sc_settle(sc_context* ctx, const sc_lattice* lattice, const sc_strengt
                     uint8_t* gone, sc_settle_info* out);
 
 /* ---------------------------------------------------------------------------
+ * Coarser levels measured from finer ones: statics::gather (statics/src/gather.rs).
+ *
+ * A material's values as the gather uses them (statics/src/model.rs:43-51: E, G and the
+ * tensile, compressive and shear strengths). Nodes name their material by its index in a
+ * caller's table; a material is its index (the reference tells materials by name).
+ * ------------------------------------------------------------------------- */
+typedef struct sc_material {
+    double e, g, ft, fc, fs;
+} sc_material;
+
+typedef struct sc_gathered sc_gathered;
+
+/* Replaces statics::gather::gathered (statics/src/gather.rs:193-195; against_full != 0)
+ * and measured(fine, false) (gather.rs:230-395; against_full == 0): the next level up of
+ * `fine`, each coarse cell's beams measured from its matter (each face a rigid handle
+ * moved alone along each axis, the free parts at rest, the handles' reactions fitted by
+ * non-negative least squares with beams between faces, each beam's strength from the
+ * finer bonds' use when it is pulled alone) and its weight shared out on its faces.
+ * `strength` gives each node's mass and each bond's strengths; node_mat (n_nodes) each
+ * node's material in `materials` (n_materials entries). Host arrays; runs on the host's
+ * cores (threads: 0 = all). The result is the reference's bit for bit: nodes in the order
+ * of their face keys, four bonds a beam. *out receives a handle to read with
+ * sc_gathered_read and free with sc_gathered_free; *n_nodes, *n_bonds its sizes.
+ * SC_BAD_INPUT for a bond whose ends share no cell (the reference panics), indexes out of
+ * range, or non-finite or non-positive bond or material values. */
+sc_status sc_gather(const sc_lattice* fine, const sc_strength* strength, const int32_t* node_mat,
+                    const sc_material* materials, int32_t n_materials, int32_t against_full, int32_t threads,
+                    sc_gathered** out, int64_t* n_nodes, int64_t* n_bonds);
+/* Copies a gathered level out; any pointer may be NULL. Per node: x (3), m, held, around
+ * (6: the two coarse sites it lies between, lesser first), mat (index in the table). Per
+ * bond: ends, p (3), n (3), a, d, E, G and the strengths ft, fc, fs (the cell's material
+ * made stronger by the beam's measured factor, Mat::stronger, model.rs:71-73). */
+sc_status sc_gathered_read(const sc_gathered* g, int32_t* level, double* x, double* m, uint8_t* held,
+                           int64_t* around, int32_t* mat, int64_t* bond_i, int64_t* bond_j, double* bond_p,
+                           double* bond_n, double* bond_a, double* bond_d, double* bond_e, double* bond_g,
+                           double* ft, double* fc, double* fs);
+void sc_gathered_free(sc_gathered* g);
+/* gather.rs:203-226: a full cell of `m` measured a level up, per class (180°, 90°):
+ * out[2 k] its beams' section over the spacing squared, out[2 k + 1] their strength over
+ * the material's. The calibration sc_gather applies when against_full != 0. */
+sc_status sc_gather_full(const sc_material* m, double* out);
+
+/* ---------------------------------------------------------------------------
  * Compliance without device allocation. No counterpart in the reference.
  *
  * For callers that must not have the library allocate device memory: an engine that

@@ -12,6 +12,10 @@
 #include "kernels.cuh"
 #include "template_gen.cuh"
 
+struct sc_gathered {
+    sc::Gathered g;
+};
+
 struct sc_context {
     sc::Context c;
 };
@@ -444,6 +448,100 @@ sc_status sc_mech_voxel_system(const uint8_t* state, const float* e, int32_t nx,
         }
         *n = nn;
         *npairs = mm;
+        return SC_OK;
+    } catch (const std::exception&) {
+        return SC_CUDA;
+    }
+}
+
+sc_status sc_gather(const sc_lattice* fine, const sc_strength* strength, const int32_t* node_mat,
+                    const sc_material* materials, int32_t n_materials, int32_t against_full, int32_t threads,
+                    sc_gathered** out, int64_t* n_nodes, int64_t* n_bonds) {
+    if (!fine || !strength || !materials || !out || !n_nodes || !n_bonds || n_materials < 1) return SC_BAD_INPUT;
+    const sc_lattice& L = *fine;
+    const sc_strength& S = *strength;
+    const int64_t nn = L.n_nodes, nb = L.n_bonds;
+    if (nn < 0 || nb < 0 || L.level < 0 || L.level > 60) return SC_BAD_INPUT;
+    if (nn > 0 && (!L.x || !L.held || !L.around || !S.m || !node_mat)) return SC_BAD_INPUT;
+    if (nb > 0 && (!L.bond_i || !L.bond_j || !L.bond_p || !L.bond_n || !L.bond_a || !L.bond_d || !L.bond_e ||
+                   !L.bond_g || !S.ft || !S.fc || !S.fs))
+        return SC_BAD_INPUT;
+    auto positive = [](double v) { return std::isfinite(v) && v > 0.0; };
+    for (int32_t k = 0; k < n_materials; k++) {
+        const sc_material& m = materials[k];
+        if (!positive(m.e) || !positive(m.g) || !positive(m.ft) || !positive(m.fc) || !positive(m.fs))
+            return SC_BAD_INPUT;
+    }
+    for (int64_t v = 0; v < nn; v++) {
+        if (node_mat[v] < 0 || node_mat[v] >= n_materials || !std::isfinite(S.m[v])) return SC_BAD_INPUT;
+        for (int q = 0; q < 3; q++)
+            if (!std::isfinite(L.x[3 * v + q])) return SC_BAD_INPUT;
+    }
+    for (int64_t b = 0; b < nb; b++) {
+        if (L.bond_i[b] < 0 || L.bond_i[b] >= nn || L.bond_j[b] < 0 || L.bond_j[b] >= nn) return SC_BAD_INPUT;
+        for (int q = 0; q < 3; q++)
+            if (!std::isfinite(L.bond_p[3 * b + q]) || !std::isfinite(L.bond_n[3 * b + q])) return SC_BAD_INPUT;
+        if (!positive(L.bond_a[b]) || !positive(L.bond_d[b]) || !positive(L.bond_e[b]) || !positive(L.bond_g[b]) ||
+            !positive(S.ft[b]) || !positive(S.fc[b]) || !positive(S.fs[b]))
+            return SC_BAD_INPUT;
+    }
+    try {
+        auto* g = new sc_gathered;
+        try {
+            sc::gather_level(L, S, node_mat, materials, n_materials, against_full != 0, threads, g->g);
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        *out = g;
+        *n_nodes = (int64_t)g->g.m.size();
+        *n_bonds = (int64_t)g->g.bi.size();
+        return SC_OK;
+    } catch (const sc::Error& e) {
+        return e.status;
+    } catch (const std::exception&) {
+        return SC_CUDA;
+    }
+}
+
+sc_status sc_gathered_read(const sc_gathered* gp, int32_t* level, double* x, double* m, uint8_t* held,
+                           int64_t* around, int32_t* mat, int64_t* bond_i, int64_t* bond_j, double* bond_p,
+                           double* bond_n, double* bond_a, double* bond_d, double* bond_e, double* bond_g,
+                           double* ft, double* fc, double* fs) {
+    if (!gp) return SC_BAD_INPUT;
+    const sc::Gathered& g = gp->g;
+    auto put = [](auto* dst, const auto& src) {
+        if (dst && !src.empty()) std::memcpy(dst, src.data(), src.size() * sizeof(src[0]));
+    };
+    if (level) *level = g.level;
+    put(x, g.x);
+    put(m, g.m);
+    put(held, g.held);
+    put(around, g.around);
+    put(mat, g.mat);
+    put(bond_i, g.bi);
+    put(bond_j, g.bj);
+    put(bond_p, g.p);
+    put(bond_n, g.n);
+    put(bond_a, g.a);
+    put(bond_d, g.d);
+    put(bond_e, g.e);
+    put(bond_g, g.g);
+    put(ft, g.ft);
+    put(fc, g.fc);
+    put(fs, g.fs);
+    return SC_OK;
+}
+
+void sc_gathered_free(sc_gathered* g) { delete g; }
+
+sc_status sc_gather_full(const sc_material* m, double* out) {
+    if (!m || !out) return SC_BAD_INPUT;
+    auto positive = [](double v) { return std::isfinite(v) && v > 0.0; };
+    if (!positive(m->e) || !positive(m->g) || !positive(m->ft) || !positive(m->fc) || !positive(m->fs))
+        return SC_BAD_INPUT;
+    try {
+        sc::gather_full(*m, out);
         return SC_OK;
     } catch (const std::exception&) {
         return SC_CUDA;

@@ -1,0 +1,763 @@
+// statics::gather (statics/src/gather.rs:193-395): a coarser level measured from a finer
+// one, on the host's cores.
+//
+// Each coarse cell of 2^l Z^3 becomes a small problem of its own: its free parts (finer
+// nodes inside it, 6 unknowns each), one rigid handle per face (3 unknowns each) and the
+// finer bonds between them. Measuring it is one Gauss–Jordan elimination of the free
+// parts against every handle axis at once, the handles' reactions, a non-negative
+// least-squares fit of beams between the faces, and, beam by beam, the finer bonds' use
+// when the beam is pulled alone. In a full lattice a cell has at most 12 free parts and 6
+// handles (a 72 x 90 elimination, 480 bonds), so the cells form a batch of fixed-shape
+// dense problems. The indexing around them (coarse cells by first appearance, faces in
+// key order, handles by first use) is sequential, as the reference's is.
+//
+// Every floating-point operation is the reference's, in its order, so the gathered
+// lattice is the reference's bit for bit (the CPU restatement checks it). Two places
+// differ in form only: row swaps are a permutation of row indices, and the beams' Gram
+// products skip the entries where a beam's unit stiffness is zero (adding a zero product
+// never changes a non-zero sum; only the sign of an all-zero sum could differ).
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "solver.cuh"
+
+namespace sc {
+namespace gth {
+
+using V3 = std::array<double, 3>;
+using Site = std::array<int64_t, 3>;
+
+// statics/src/model.rs:16-36, in its operation order
+inline V3 add(V3 a, V3 b) { return {a[0] + b[0], a[1] + b[1], a[2] + b[2]}; }
+inline V3 sub(V3 a, V3 b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+inline V3 mul(V3 a, double s) { return {a[0] * s, a[1] * s, a[2] * s}; }
+inline double dot(V3 a, V3 b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline V3 cross(V3 a, V3 b) { return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]}; }
+inline double norm(V3 a) { return std::sqrt(dot(a, a)); }
+inline V3 unit(V3 a) { return mul(a, 1.0 / norm(a)); }
+
+constexpr double UNIT = 0.125;                 // lattice.rs:16
+constexpr double SECTION[2] = {0.336, 0.336};  // lattice.rs:25
+constexpr double PI = 3.14159265358979323846;
+
+inline double spacing(int level) { return UNIT * (double)(uint64_t(1) << level); }  // lattice.rs:34-36
+inline V3 centre(const Site& s, int level) {                                         // lattice.rs:39-41
+    V3 c;
+    for (int k = 0; k < 3; k++) c[k] = ((double)s[k] + 0.5 * (double)(uint64_t(1) << level)) * UNIT;
+    return c;
+}
+inline Site coarse_site(const Site& p, int level) {  // lattice.rs:45-47
+    Site q;
+    for (int k = 0; k < 3; k++) q[k] = p[k] & ~((int64_t(1) << level) - 1);
+    return q;
+}
+inline size_t beam_class(V3 a, V3 b, V3 c) {  // lattice.rs:29-32
+    V3 u = sub(a, c), v = sub(b, c);
+    return (size_t)std::round(1.0 + dot(u, v) / (norm(u) * norm(v)));
+}
+
+struct Mat {  // the values of statics/src/model.rs:43-51 the gather uses
+    double e, g, ft, fc, fs;
+    double used(double s1, double s3) const {  // model.rs:66-68
+        return std::fmax(std::fmax(s1 / ft, -s3 / fc), (s1 - s3) / (2.0 * fs));
+    }
+};
+
+// A finer bond inside one cell's problem: its ends renumbered to the cell's places.
+struct LBond {
+    size_t i, j;
+    V3 p, n;
+    double a, d, e, g, ft, fc, fs;
+    V3 force(V3 delta) const {  // model.rs:115-119
+        double along = dot(delta, n);
+        double k = a / d;
+        return add(mul(n, e * k * along), mul(sub(delta, mul(n, along)), g * k));
+    }
+    double used(V3 f) const {  // model.rs:123-129
+        V3 t = mul(f, 1.0 / a);
+        double sigma = dot(t, n);
+        double tau2 = std::fmax(dot(t, t) - sigma * sigma, 0.0);
+        double r = std::sqrt(sigma * sigma / 4.0 + tau2);
+        return Mat{e, g, ft, fc, fs}.used(sigma / 2.0 + r, sigma / 2.0 - r);
+    }
+    double energy(V3 f) const {  // model.rs:132-136
+        double k = a / d;
+        double along = dot(f, n);
+        return 0.5 * (along * along / (e * k) + (dot(f, f) - along * along) / (g * k));
+    }
+};
+
+// Rust's f64::total_cmp as an integer key.
+inline int64_t total_key(double v) {
+    int64_t i;
+    std::memcpy(&i, &v, 8);
+    return i ^ (int64_t)(((uint64_t)(i >> 63)) >> 1);
+}
+
+size_t find(std::vector<size_t>& p, size_t a) {  // bodies.rs:628-634
+    while (p[a] != a) {
+        p[a] = p[p[a]];
+        a = p[a];
+    }
+    return a;
+}
+
+// gather.rs:164-184 on a row-major n x (n + rhs) matrix: Gauss–Jordan with the largest
+// pivot (the last of equals), a pivot below 1e-12 of the largest diagonal skipped; the
+// answer's rows into x (n x rhs), 0 where the pivot was skipped.
+void eliminate(std::vector<double>& a, size_t n, size_t rhs, std::vector<size_t>& row, std::vector<double>& x) {
+    const size_t w = n + rhs;
+    double scale = 0.0;
+    for (size_t r = 0; r < n; r++) scale = std::fmax(scale, std::fabs(a[r * w + r]));
+    auto small = [&](double v) { return std::fabs(v) <= 1e-12 * scale; };
+    row.resize(n);
+    for (size_t r = 0; r < n; r++) row[r] = r;
+    for (size_t c = 0; c < n; c++) {
+        size_t p = c;
+        int64_t best = total_key(std::fabs(a[row[c] * w + c]));
+        for (size_t q = c + 1; q < n; q++) {
+            int64_t k = total_key(std::fabs(a[row[q] * w + c]));
+            if (k >= best) {
+                best = k;
+                p = q;
+            }
+        }
+        std::swap(row[c], row[p]);
+        const double* piv = &a[row[c] * w];
+        if (small(piv[c])) continue;
+        for (size_t r = 0; r < n; r++) {
+            if (r == c) continue;
+            double* ar = &a[row[r] * w];
+            double f = ar[c] / piv[c];
+            if (f != 0.0)
+                for (size_t k = c; k < w; k++) ar[k] -= f * piv[k];
+        }
+    }
+    x.assign(n * rhs, 0.0);
+    for (size_t r = 0; r < n; r++) {
+        const double* ar = &a[row[r] * w];
+        for (size_t k = 0; k < rhs; k++) x[r * rhs + k] = small(ar[r]) ? 0.0 : ar[n + k] / ar[r];
+    }
+}
+
+// One coarse cell's problem: places 0..nf-1 its free parts, nf.. its handles (one a face).
+struct CellProblem {
+    size_t nf = 0;
+    std::vector<V3> place;  // each place's position: a free part's node centre, a handle's face centre
+    std::vector<LBond> bonds;
+};
+
+struct Beam {
+    size_t a, b;
+    double k, stronger;
+};
+
+using Full = std::array<std::pair<double, double>, 2>;
+
+struct Scratch {
+    std::vector<double> a, x, k, g, sol, target, forces;
+    std::vector<size_t> row;
+};
+
+// gather.rs:119-161: the beams (a < b, their stiffness along them) nearest the handles'
+// stiffness k (m x m, m = 3 handles), none negative, only between joined handles.
+template <class J>
+std::vector<std::tuple<size_t, size_t, double>> fit_beams(const std::vector<double>& k, const std::vector<V3>& at,
+                                                          J joined, Scratch& s) {
+    const size_t nh = at.size(), n = 3 * nh;
+    std::vector<std::pair<size_t, size_t>> pairs;
+    for (size_t a = 0; a < nh; a++)
+        for (size_t b = a + 1; b < nh; b++)
+            if (joined(a, b)) pairs.push_back({a, b});
+    // A unit of each beam's stiffness: four 3x3 blocks, kept as (flat index, value) in
+    // flat order, the order the dense products add them in.
+    std::vector<std::vector<std::pair<size_t, double>>> units(pairs.size());
+    for (size_t q = 0; q < pairs.size(); q++) {
+        auto [a, b] = pairs[q];
+        V3 e = unit(sub(at[b], at[a]));
+        auto& u = units[q];
+        for (int half = 0; half < 2; half++) {
+            size_t r0 = half == 0 ? 3 * a : 3 * b;
+            for (size_t r = 0; r < 3; r++) {
+                // row r0 + r: column blocks a then b (a < b), + on the diagonal block
+                for (int side = 0; side < 2; side++) {
+                    size_t c0 = side == 0 ? 3 * a : 3 * b;
+                    double sign = (side == half) ? 1.0 : -1.0;
+                    for (size_t c = 0; c < 3; c++) {
+                        double v = e[r] * e[c];
+                        u.push_back({(r0 + r) * n + c0 + c, sign > 0 ? 0.0 + v : 0.0 - v});
+                    }
+                }
+            }
+        }
+    }
+    s.target.resize(n * n);
+    for (size_t i = 0; i < n * n; i++) s.target[i] = 0.5 * (k[(i / n) * n + i % n] + k[(i % n) * n + i / n]);
+    auto udot = [](const std::vector<std::pair<size_t, double>>& p, const std::vector<std::pair<size_t, double>>& q) {
+        double acc = 0.0;
+        size_t i = 0, j = 0;
+        while (i < p.size() && j < q.size()) {
+            if (p[i].first < q[j].first)
+                i++;
+            else if (q[j].first < p[i].first)
+                j++;
+            else {
+                acc += p[i].second * q[j].second;
+                i++;
+                j++;
+            }
+        }
+        return acc;
+    };
+    std::vector<bool> on(pairs.size(), true);
+    std::vector<size_t> idx;
+    for (;;) {
+        idx.clear();
+        for (size_t p = 0; p < pairs.size(); p++)
+            if (on[p]) idx.push_back(p);
+        const size_t m = idx.size();
+        s.g.assign(m * (m + 1), 0.0);
+        for (size_t r = 0; r < m; r++) {
+            for (size_t c = 0; c < m; c++) s.g[r * (m + 1) + c] = udot(units[idx[r]], units[idx[c]]);
+            double acc = 0.0;
+            for (const auto& [f, v] : units[idx[r]]) acc += v * s.target[f];
+            s.g[r * (m + 1) + m] = acc;
+        }
+        eliminate(s.g, m, 1, s.row, s.sol);
+        int64_t worst = -1;  // the most negative, the first of equals
+        for (size_t r = 0; r < m; r++)
+            if (s.sol[r] < 0.0 && (worst < 0 || total_key(s.sol[r]) < total_key(s.sol[(size_t)worst]))) worst = (int64_t)r;
+        if (worst >= 0) {
+            on[idx[(size_t)worst]] = false;
+            continue;
+        }
+        std::vector<std::tuple<size_t, size_t, double>> out;
+        for (size_t r = 0; r < m; r++)
+            if (s.sol[r] > 0.0) out.emplace_back(pairs[idx[r]].first, pairs[idx[r]].second, s.sol[r]);
+        return out;
+    }
+}
+
+// gather.rs:58-114 and 321-361: one cell measured. `at` = its handles' positions.
+std::vector<Beam> measure_cell(const CellProblem& cp, const std::vector<V3>& at, const Mat& mat, const Full& full,
+                               V3 middle, double s, bool against_full, Scratch& sc) {
+    const size_t nf = cp.nf, nh = at.size(), n = 6 * nf, m = 3 * nh, w = n + m, nb = cp.bonds.size();
+    auto column = [&](size_t v, size_t d, V3 p) -> V3 {
+        V3 e{0.0, 0.0, 0.0};
+        e[d % 3] = 1.0;
+        return d < 3 ? e : cross(e, sub(p, cp.place[v]));
+    };
+    auto dof = [&](size_t v, size_t d) -> int64_t {
+        if (v < nf) return (int64_t)(6 * v + d);
+        if (d < 3) return (int64_t)(n + 3 * (v - nf) + d);
+        return -1;
+    };
+    // The free parts' rows: their stiffness, the handles' columns on the right side.
+    sc.a.assign(n * w, 0.0);
+    for (const LBond& b : cp.bonds) {
+        const double k = b.a / b.d;
+        V3 srow[3];
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) {
+                double nn = b.n[r] * b.n[c];
+                srow[r][c] = b.e * k * nn + b.g * k * ((r == c ? 1.0 : 0.0) - nn);
+            }
+        const std::pair<size_t, double> ends[2] = {{b.i, -1.0}, {b.j, 1.0}};
+        for (const auto& [v, sv] : ends)
+            for (size_t d = 0; d < 6; d++) {
+                int64_t r = dof(v, d);
+                if (r < 0 || (size_t)r >= n) continue;
+                V3 cv = column(v, d, b.p);
+                V3 scv{dot(srow[0], cv), dot(srow[1], cv), dot(srow[2], cv)};
+                for (const auto& [u, su] : ends)
+                    for (size_t e = 0; e < 6; e++) {
+                        int64_t c = dof(u, e);
+                        if (c < 0) continue;
+                        double sign = (size_t)c < n ? 1.0 : -1.0;
+                        sc.a[(size_t)r * w + (size_t)c] += sign * sv * su * dot(scv, column(u, e, b.p));
+                    }
+            }
+    }
+    eliminate(sc.a, n, m, sc.row, sc.x);
+    // Each handle axis moved alone: the finer bonds' forces (bodies.rs:420-423), case-major.
+    sc.forces.resize(m * nb * 3);
+    for (size_t c = 0; c < m; c++) {
+        auto motion_at = [&](size_t v, V3 p) -> V3 {
+            V3 t{0.0, 0.0, 0.0}, r{0.0, 0.0, 0.0};
+            if (v < nf) {
+                for (int q = 0; q < 3; q++) {
+                    t[q] = sc.x[(6 * v + q) * m + c];
+                    r[q] = sc.x[(6 * v + 3 + q) * m + c];
+                }
+            } else if (v - nf == c / 3) {
+                t[c % 3] = 1.0;
+            }
+            return add(t, cross(r, sub(p, cp.place[v])));  // bodies.rs:44-47
+        };
+        for (size_t q = 0; q < nb; q++) {
+            const LBond& b = cp.bonds[q];
+            V3 f = b.force(sub(motion_at(b.j, b.p), motion_at(b.i, b.p)));
+            for (int t = 0; t < 3; t++) sc.forces[(c * nb + q) * 3 + t] = f[t];
+        }
+    }
+    auto force = [&](size_t c, size_t q) -> V3 {
+        const double* f = &sc.forces[(c * nb + q) * 3];
+        return {f[0], f[1], f[2]};
+    };
+    // The stiffness between handles: what holds each, each case.
+    sc.k.assign(m * m, 0.0);
+    for (size_t c = 0; c < m; c++)
+        for (size_t q = 0; q < nb; q++) {
+            V3 f = force(c, q);
+            const std::pair<size_t, double> sides[2] = {{cp.bonds[q].j, 1.0}, {cp.bonds[q].i, -1.0}};
+            for (const auto& [v, sign] : sides)
+                if (v >= nf)
+                    for (size_t t = 0; t < 3; t++) sc.k[(3 * (v - nf) + t) * m + c] += sign * f[t];
+        }
+    // Which handles the cell's matter joins (gather.rs:43-51).
+    std::vector<size_t> parent(nf + nh);
+    for (size_t t = 0; t < parent.size(); t++) parent[t] = t;
+    for (const LBond& b : cp.bonds) {
+        size_t x = find(parent, b.i), y = find(parent, b.j);
+        parent[x] = y;
+    }
+    std::vector<size_t> piece(nh);
+    for (size_t h = 0; h < nh; h++) piece[h] = find(parent, nf + h);
+    std::vector<Beam> found;
+    std::vector<V3> pulled(nb);
+    for (const auto& [a, b, stiff] : fit_beams(sc.k, at, [&](size_t p, size_t q) { return piece[p] == piece[q]; }, sc)) {
+        // The beam pulled alone, a unit apart; each finer bond as much as it holds of
+        // the work done.
+        V3 e = unit(sub(at[b], at[a]));
+        for (size_t q = 0; q < nb; q++) {
+            V3 f{0.0, 0.0, 0.0};
+            for (size_t t = 0; t < 3; t++)
+                f = add(f, add(mul(force(3 * b + t, q), e[t] / 2.0), mul(force(3 * a + t, q), -e[t] / 2.0)));
+            pulled[q] = f;
+        }
+        double hold = 0.0, work = 0.0;
+        for (size_t q = 0; q < nb; q++) {
+            double u = cp.bonds[q].used(pulled[q]);
+            double wq = cp.bonds[q].energy(pulled[q]);
+            hold += wq * u;
+            work += wq;
+        }
+        double fine_used = work > 0.0 ? hold / work : 0.0;
+        double length = norm(sub(at[b], at[a]));
+        double own = mat.used(mat.e / length, 0.0);
+        double stronger = fine_used > 0.0 ? own / fine_used : 1.0;
+        size_t cls = beam_class(at[a], at[b], middle);
+        double section = stiff * length / mat.e / (s * s);
+        if (against_full) section = section * SECTION[cls] / full[cls].first;
+        found.push_back(Beam{a, b, section * s * s * mat.e / length, stronger / full[cls].second});
+    }
+    return found;
+}
+
+struct FineView {
+    int level;
+    int64_t nn, nb;
+    const double *x, *m;
+    const uint8_t* held;
+    const int64_t* around;
+    const int32_t* mat;
+    const int64_t *bi, *bj;
+    const double *p, *n, *a, *d, *e, *g, *ft, *fc, *fs;
+    Site site(int64_t v, int s) const { return {around[6 * v + 3 * s], around[6 * v + 3 * s + 1], around[6 * v + 3 * s + 2]}; }
+};
+
+struct SiteHash {
+    size_t operator()(const Site& s) const {
+        uint64_t h = 1469598103934665603ull;
+        for (int k = 0; k < 3; k++) h = (h ^ (uint64_t)s[k]) * 1099511628211ull;
+        return (size_t)(h ^ (h >> 29));
+    }
+};
+
+Full full_of(const Mat& mat);
+
+// gather.rs:230-395
+void measured(const FineView& F, const std::vector<Mat>& table, bool against_full, int threads, Gathered& out) {
+    const int level = F.level + 1;
+    std::unordered_map<Site, size_t, SiteHash> index;
+    std::vector<Site> sites;
+    auto cell_of = [&](const Site& s) {
+        Site key = coarse_site(s, level);
+        auto it = index.find(key);
+        if (it != index.end()) return it->second;
+        sites.push_back(key);
+        index.emplace(key, sites.size() - 1);
+        return sites.size() - 1;
+    };
+    std::vector<std::array<size_t, 2>> between((size_t)F.nn);
+    for (int64_t v = 0; v < F.nn; v++) {
+        size_t x = cell_of(F.site(v, 0));
+        size_t y = cell_of(F.site(v, 1));
+        between[(size_t)v] = {x, y};
+    }
+    std::vector<size_t> lies((size_t)F.nb);
+    for (int64_t b = 0; b < F.nb; b++) {
+        int64_t i = F.bi[b], j = F.bj[b];
+        Site si[2] = {F.site(i, 0), F.site(i, 1)}, sj[2] = {F.site(j, 0), F.site(j, 1)};
+        int k = (si[0] == sj[0] || si[0] == sj[1]) ? 0 : (si[1] == sj[0] || si[1] == sj[1]) ? 1 : -1;
+        require(k >= 0, SC_BAD_INPUT, "a bond whose ends share no cell");
+        lies[(size_t)b] = cell_of(si[k]);
+    }
+    const size_t n = sites.size();
+    auto face = [&](size_t a, size_t b) { return sites[a] < sites[b] ? std::make_pair(a, b) : std::make_pair(b, a); };
+    // Faces: every (cell, cell across) a node lies between or a bond reaches, in key order.
+    std::vector<std::pair<size_t, size_t>> keys;
+    for (int64_t v = 0; v < F.nn; v++)
+        if (between[(size_t)v][0] != between[(size_t)v][1]) keys.push_back(face(between[(size_t)v][0], between[(size_t)v][1]));
+    // Cells: free parts in node order, materials by first appearance, their weight summed
+    // in node order (gather.rs:263-279).
+    std::vector<std::vector<size_t>> free(n);
+    std::vector<std::vector<std::pair<int32_t, double>>> mats(n);
+    auto weigh = [](std::vector<std::pair<int32_t, double>>& list, int32_t mat, double w) {
+        for (auto& e : list)
+            if (e.first == mat) {
+                e.second += w;
+                return;
+            }
+        list.push_back({mat, w});
+    };
+    for (int64_t v = 0; v < F.nn; v++) {
+        size_t x = between[(size_t)v][0], y = between[(size_t)v][1];
+        weigh(mats[x], F.mat[v], F.m[v]);
+        if (x != y) weigh(mats[y], F.mat[v], F.m[v]);
+        if (x == y) free[x].push_back((size_t)v);
+    }
+    std::vector<size_t> place((size_t)F.nn, SIZE_MAX);
+    for (size_t c = 0; c < n; c++)
+        for (size_t k = 0; k < free[c].size(); k++) place[free[c][k]] = k;
+    // Each bond into its cell's problem; handles numbered by first use (gather.rs:285-294).
+    std::vector<std::vector<size_t>> across(n);
+    std::vector<std::vector<std::array<size_t, 3>>> cbonds(n);
+    for (int64_t b = 0; b < F.nb; b++) {
+        size_t c = lies[(size_t)b];
+        auto at = [&](int64_t v) {
+            size_t x = between[(size_t)v][0], y = between[(size_t)v][1];
+            if (x == c && y == c) return place[(size_t)v];
+            size_t other = x == c ? y : x;
+            auto& ac = across[c];
+            size_t k = (size_t)(std::find(ac.begin(), ac.end(), other) - ac.begin());
+            if (k == ac.size()) ac.push_back(other);
+            return free[c].size() + k;
+        };
+        size_t i = at(F.bi[b]);
+        size_t j = at(F.bj[b]);
+        cbonds[c].push_back({i, j, (size_t)b});
+    }
+    std::vector<uint8_t> held(n);
+    for (size_t c = 0; c < n; c++) {
+        bool all = !free[c].empty();
+        for (size_t v : free[c]) all = all && F.held[v];
+        held[c] = all;
+    }
+    for (size_t c = 0; c < n; c++)
+        for (size_t o : across[c]) keys.push_back(face(c, o));
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    auto node_of = [&](size_t a, size_t b) {
+        return (size_t)(std::lower_bound(keys.begin(), keys.end(), face(a, b)) - keys.begin());
+    };
+    const size_t nn = keys.size();
+    std::vector<double> fmass(nn, 0.0);
+    std::vector<uint8_t> fheld(nn, 0);
+    for (int64_t v = 0; v < F.nn; v++) {
+        size_t x = between[(size_t)v][0], y = between[(size_t)v][1];
+        if (x == y) continue;
+        size_t k = node_of(x, y);
+        fmass[k] += F.m[v];
+        fheld[k] = fheld[k] || F.held[v];
+    }
+    auto mat_of = [&](std::initializer_list<size_t> cs) -> int32_t {  // gather.rs:301-310
+        std::vector<std::pair<int32_t, double>> all;
+        for (size_t c : cs)
+            for (const auto& [mt, wt] : mats[c]) weigh(all, mt, wt);
+        if (all.empty()) return -1;  // STONE
+        size_t best = 0;
+        for (size_t k = 1; k < all.size(); k++)
+            if (total_key(all[k].second) >= total_key(all[best].second)) best = k;
+        return all[best].first;
+    };
+    out.level = level;
+    out.x.resize(3 * nn);
+    out.m.resize(nn);
+    out.held.resize(nn);
+    out.around.resize(6 * nn);
+    out.mat.resize(nn);
+    for (size_t k = 0; k < nn; k++) {
+        auto [a, b] = keys[k];
+        V3 x = mul(add(centre(sites[a], level), centre(sites[b], level)), 0.5);
+        for (int t = 0; t < 3; t++) {
+            out.x[3 * k + t] = x[t];
+            out.around[6 * k + t] = sites[a][t];
+            out.around[6 * k + 3 + t] = sites[b][t];
+        }
+        out.m[k] = fmass[k];
+        out.mat[k] = mat_of({a, b});
+        out.held[k] = fheld[k] || held[a] || held[b];
+    }
+    const double s = spacing(level);
+    std::vector<std::vector<size_t>> ends(n);
+    std::vector<std::vector<V3>> at(n);
+    std::vector<int32_t> cmat(n);
+    for (size_t c = 0; c < n; c++) {
+        for (size_t o : across[c]) {
+            size_t k = node_of(c, o);
+            ends[c].push_back(k);
+            at[c].push_back({out.x[3 * k], out.x[3 * k + 1], out.x[3 * k + 2]});
+        }
+        cmat[c] = mat_of({c});
+    }
+    // A cell without matter of a known material measures as stone (gather.rs:310); the
+    // table's first entry stands for it only where such a cell has beams to measure.
+    auto mat_value = [&](int32_t k) -> const Mat& { return table[(size_t)std::max<int32_t>(k, 0)]; };
+    std::vector<Full> fulls(n, Full{std::make_pair(1.0, 1.0), std::make_pair(1.0, 1.0)});
+    if (against_full)
+        for (size_t c = 0; c < n; c++)
+            if (!held[c] && !at[c].empty()) fulls[c] = full_of(mat_value(cmat[c]));
+    // Every cell measured, over the host's threads (cells are independent).
+    std::vector<std::vector<Beam>> found(n);
+    auto work = [&](size_t lo, size_t hi) {
+        Scratch scr;
+        CellProblem cp;
+        for (size_t c = lo; c < hi; c++) {
+            if (held[c] || at[c].empty()) continue;
+            cp.nf = free[c].size();
+            cp.place.clear();
+            for (size_t v : free[c]) cp.place.push_back({F.x[3 * v], F.x[3 * v + 1], F.x[3 * v + 2]});
+            for (const V3& h : at[c]) cp.place.push_back(h);
+            cp.bonds.clear();
+            for (const auto& t : cbonds[c]) {
+                size_t b = t[2];
+                cp.bonds.push_back(LBond{t[0], t[1], {F.p[3 * b], F.p[3 * b + 1], F.p[3 * b + 2]},
+                                         {F.n[3 * b], F.n[3 * b + 1], F.n[3 * b + 2]}, F.a[b], F.d[b], F.e[b], F.g[b],
+                                         F.ft[b], F.fc[b], F.fs[b]});
+            }
+            found[c] = measure_cell(cp, at[c], mat_value(cmat[c]), fulls[c], centre(sites[c], level), s, against_full,
+                                    scr);
+        }
+    };
+    size_t T = threads > 0 ? (size_t)threads : std::max<size_t>(1, std::thread::hardware_concurrency());
+    if (n < 64 || T == 1) {
+        work(0, n);
+    } else {
+        // Interleaved blocks of cells: a level's cells with matter cluster by first
+        // appearance, so contiguous halves would leave threads idle.
+        std::vector<std::thread> pool;
+        const size_t chunk = 16;
+        std::atomic<size_t> next{0};
+        for (size_t t = 0; t < T; t++)
+            pool.emplace_back([&] {
+                for (;;) {
+                    size_t lo = next.fetch_add(chunk);
+                    if (lo >= n) return;
+                    work(lo, std::min(n, lo + chunk));
+                }
+            });
+        for (auto& th : pool) th.join();
+    }
+    // Each cell's weight on its faces, as much as each is joined; its beams (gather.rs:370-392).
+    out.bi.clear();
+    for (size_t c = 0; c < n; c++) {
+        double mass = 0.0;
+        for (size_t v : free[c]) mass += F.m[v];
+        const size_t nh = at[c].size();
+        std::vector<double> joined(nh, 0.0);
+        for (const Beam& bm : found[c]) {
+            joined[bm.a] += bm.k;
+            joined[bm.b] += bm.k;
+        }
+        double total = 0.0;
+        for (double j : joined) total += j;
+        for (size_t h = 0; h < nh; h++) out.m[ends[c][h]] += mass * (total > 0.0 ? joined[h] / total : 1.0 / (double)nh);
+        const Mat& mt = mat_value(cmat[c]);
+        for (const Beam& bm : found[c]) {
+            size_t ia = ends[c][bm.a], ib = ends[c][bm.b];
+            if (out.held[ia] && out.held[ib]) continue;
+            V3 pa = at[c][bm.a], pb = at[c][bm.b];
+            double length = norm(sub(pb, pa));
+            double area = bm.k * length / mt.e;
+            // lattice.rs:76-84: four bonds at radius sqrt(A / 2 pi) about the middle
+            V3 nrm = unit(sub(pb, pa));
+            V3 e1 = unit(cross(nrm, std::fabs(nrm[0]) < 0.9 ? V3{1.0, 0.0, 0.0} : V3{0.0, 1.0, 0.0}));
+            V3 e2 = cross(nrm, e1);
+            double r = std::sqrt(area / (2.0 * PI));
+            V3 middle = mul(add(pa, pb), 0.5);
+            double d = norm(sub(pb, pa));
+            const V3 offs[4] = {mul(e1, r), mul(e1, -r), mul(e2, r), mul(e2, -r)};
+            for (const V3& o : offs) {
+                V3 p = add(middle, o);
+                out.bi.push_back((int64_t)ia);
+                out.bj.push_back((int64_t)ib);
+                for (int t = 0; t < 3; t++) {
+                    out.p.push_back(p[t]);
+                    out.n.push_back(nrm[t]);
+                }
+                out.a.push_back(area / 4.0);
+                out.d.push_back(d);
+                out.e.push_back(mt.e);
+                out.g.push_back(mt.g);
+                out.ft.push_back(mt.ft * bm.stronger);  // Mat::stronger, model.rs:71-73
+                out.fc.push_back(mt.fc * bm.stronger);
+                out.fs.push_back(mt.fs * bm.stronger);
+            }
+        }
+    }
+}
+
+// A full block of `mat` at level 0, 6 cells a side about the origin, all free, as
+// lattice.rs:87-163 builds it (sites x-major, then y, then z; nodes by first touch; the
+// 15 beams of a cell in face-pair order).
+struct Block {
+    std::vector<double> x, m, p, n, a, d, e, g, ft, fc, fs;
+    std::vector<uint8_t> held;
+    std::vector<int64_t> around, bi, bj;
+    std::vector<int32_t> mat;
+};
+
+Block full_block(const Mat& mt) {
+    static const int FACES[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+    Block B;
+    const double s = spacing(0);
+    std::unordered_map<uint64_t, size_t> index;
+    auto pack = [](const Site& a, const Site& b) {
+        uint64_t h = 0;
+        for (int k = 0; k < 3; k++) h = h * 64 + (uint64_t)(a[k] + 16);
+        for (int k = 0; k < 3; k++) h = h * 64 + (uint64_t)(b[k] + 16);
+        return h;
+    };
+    for (int64_t i = -3; i < 3; i++)
+        for (int64_t j = -3; j < 3; j++)
+            for (int64_t k = -3; k < 3; k++) {
+                Site site{i, j, k};
+                size_t ends[6];
+                for (int f = 0; f < 6; f++) {
+                    Site other{i + FACES[f][0], j + FACES[f][1], k + FACES[f][2]};
+                    Site lo = site < other ? site : other, hi = site < other ? other : site;
+                    uint64_t key = pack(lo, hi);
+                    auto it = index.find(key);
+                    if (it == index.end()) {
+                        V3 x = mul(add(centre(site, 0), centre(other, 0)), 0.5);
+                        for (int t = 0; t < 3; t++) {
+                            B.x.push_back(x[t]);
+                            B.around.push_back(lo[t]);
+                        }
+                        for (int t = 0; t < 3; t++) B.around.push_back(hi[t]);
+                        B.m.push_back(0.0);
+                        B.held.push_back(0);
+                        B.mat.push_back(0);
+                        it = index.emplace(key, B.m.size() - 1).first;
+                    }
+                    B.m[it->second] += 1.0 / 6.0;
+                    ends[f] = it->second;
+                }
+                V3 middle = centre(site, 0);
+                for (int fa = 0; fa < 6; fa++)
+                    for (int fb = fa + 1; fb < 6; fb++) {
+                        size_t ia = ends[fa], ib = ends[fb];
+                        V3 pa{B.x[3 * ia], B.x[3 * ia + 1], B.x[3 * ia + 2]};
+                        V3 pb{B.x[3 * ib], B.x[3 * ib + 1], B.x[3 * ib + 2]};
+                        double area = SECTION[beam_class(pa, pb, middle)] * s * s;
+                        V3 nrm = unit(sub(pb, pa));
+                        V3 e1 = unit(cross(nrm, std::fabs(nrm[0]) < 0.9 ? V3{1.0, 0.0, 0.0} : V3{0.0, 1.0, 0.0}));
+                        V3 e2 = cross(nrm, e1);
+                        double r = std::sqrt(area / (2.0 * PI));
+                        V3 mid = mul(add(pa, pb), 0.5);
+                        double d = norm(sub(pb, pa));
+                        const V3 offs[4] = {mul(e1, r), mul(e1, -r), mul(e2, r), mul(e2, -r)};
+                        for (const V3& o : offs) {
+                            V3 p = add(mid, o);
+                            B.bi.push_back((int64_t)ia);
+                            B.bj.push_back((int64_t)ib);
+                            for (int t = 0; t < 3; t++) {
+                                B.p.push_back(p[t]);
+                                B.n.push_back(nrm[t]);
+                            }
+                            B.a.push_back(area / 4.0);
+                            B.d.push_back(d);
+                            B.e.push_back(mt.e);
+                            B.g.push_back(mt.g);
+                            B.ft.push_back(mt.ft);
+                            B.fc.push_back(mt.fc);
+                            B.fs.push_back(mt.fs);
+                        }
+                    }
+            }
+    return B;
+}
+
+// gather.rs:203-226: a full cell of `mat` measured a level up, by class: its beams'
+// section over the spacing squared and strength over the material's, kept per material.
+Full full_of(const Mat& mt) {
+    static std::mutex lock;
+    static std::vector<std::pair<Mat, Full>> known;
+    {
+        std::lock_guard<std::mutex> g(lock);
+        for (const auto& [k, f] : known)
+            if (std::memcmp(&k, &mt, sizeof(Mat)) == 0) return f;
+    }
+    Block B = full_block(mt);
+    FineView F{0, (int64_t)B.m.size(), (int64_t)B.bi.size(), B.x.data(), B.m.data(), B.held.data(), B.around.data(),
+               B.mat.data(), B.bi.data(), B.bj.data(), B.p.data(), B.n.data(), B.a.data(), B.d.data(), B.e.data(),
+               B.g.data(), B.ft.data(), B.fc.data(), B.fs.data()};
+    Gathered coarse;
+    measured(F, std::vector<Mat>{mt}, false, 1, coarse);
+    const double s = spacing(1);
+    double sum[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    auto touches = [&](size_t v) {
+        const int64_t* a = &coarse.around[6 * v];
+        return (a[0] == 0 && a[1] == 0 && a[2] == 0) || (a[3] == 0 && a[4] == 0 && a[5] == 0);
+    };
+    for (size_t q = 0; q + 4 <= coarse.bi.size(); q += 4) {
+        size_t i = (size_t)coarse.bi[q], j = (size_t)coarse.bj[q];
+        if (touches(i) && touches(j)) {
+            V3 xi{coarse.x[3 * i], coarse.x[3 * i + 1], coarse.x[3 * i + 2]};
+            V3 xj{coarse.x[3 * j], coarse.x[3 * j + 1], coarse.x[3 * j + 2]};
+            size_t k = beam_class(xi, xj, centre(Site{0, 0, 0}, 1));
+            sum[k][0] += 4.0 * coarse.a[q] / (s * s);
+            sum[k][1] += coarse.ft[q] / mt.ft;
+            sum[k][2] += 1.0;
+        }
+    }
+    Full f;
+    for (int k = 0; k < 2; k++)
+        f[k] = sum[k][2] > 0.0 ? std::make_pair(sum[k][0] / sum[k][2], sum[k][1] / sum[k][2]) : std::make_pair(1.0, 1.0);
+    std::lock_guard<std::mutex> g(lock);
+    known.push_back({mt, f});
+    return f;
+}
+
+}  // namespace gth
+
+void gather_level(const sc_lattice& L, const sc_strength& S, const int32_t* node_mat, const sc_material* materials,
+                  int32_t n_materials, bool against_full, int32_t threads, Gathered& out) {
+    std::vector<gth::Mat> table((size_t)n_materials);
+    for (int32_t k = 0; k < n_materials; k++)
+        table[(size_t)k] = gth::Mat{materials[k].e, materials[k].g, materials[k].ft, materials[k].fc, materials[k].fs};
+    gth::FineView F{L.level,  L.n_nodes,  L.n_bonds,  L.x,        S.m,        L.held,     L.around,
+                    node_mat, L.bond_i,   L.bond_j,   L.bond_p,   L.bond_n,   L.bond_a,   L.bond_d,
+                    L.bond_e, L.bond_g,   S.ft,       S.fc,       S.fs};
+    gth::measured(F, table, against_full, threads, out);
+}
+
+void gather_full(const sc_material& m, double* out) {
+    auto f = gth::full_of(gth::Mat{m.e, m.g, m.ft, m.fc, m.fs});
+    for (int k = 0; k < 2; k++) {
+        out[2 * k] = f[k].first;
+        out[2 * k + 1] = f[k].second;
+    }
+}
+
+}  // namespace sc

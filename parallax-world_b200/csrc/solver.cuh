@@ -155,6 +155,20 @@ void mech_voxel_system(const uint8_t* state, const float* e, int nx, int ny, int
                        std::vector<uint32_t>& pi, std::vector<uint32_t>& pj, std::vector<double>& pb,
                        std::vector<double>& b);
 
+// --- gather.cu: a coarser level measured from a finer one (statics/src/gather.rs) --------
+struct Gathered {
+    int32_t level = 0;
+    std::vector<double> x, m;
+    std::vector<uint8_t> held;
+    std::vector<int64_t> around;
+    std::vector<int32_t> mat;
+    std::vector<int64_t> bi, bj;
+    std::vector<double> p, n, a, d, e, g, ft, fc, fs;
+};
+void gather_level(const sc_lattice& L, const sc_strength& S, const int32_t* node_mat, const sc_material* materials,
+                  int32_t n_materials, bool against_full, int32_t threads, Gathered& out);
+void gather_full(const sc_material& m, double* out);
+
 // --- capi.cu / settle.cu -----------------------------------------------------------------
 // motions of a lattice into out_dev (6 per node, device); the solve's status
 sc_status lattice_motions(Context& ctx, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,

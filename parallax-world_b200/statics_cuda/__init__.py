@@ -125,6 +125,12 @@ def lib():
         L.sc_mech_voxel_system.argtypes = [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                            C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), P, P, P, P, P,
                                            P, P]
+        L.sc_gather.argtypes = [C.POINTER(LatticeC), C.POINTER(Strength), P, P, C.c_int32, C.c_int32, C.c_int32,
+                                C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.sc_gathered_read.argtypes = [P, C.POINTER(C.c_int32)] + [P] * 16
+        L.sc_gathered_free.argtypes = [P]
+        L.sc_gathered_free.restype = None
+        L.sc_gather_full.argtypes = [P, P]
         L.sc_mech_levels.argtypes = [C.c_int64, P, P, P, C.c_int64, P, P, P, C.c_double, C.c_int32, P, P,
                                      C.POINTER(C.c_int32)]
         L.sc_mech_solve.argtypes = [P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, C.c_double, C.c_double,
@@ -221,6 +227,66 @@ def mech_levels(system: dict, size: float | None = None):
     if s != OK:
         raise StaticsError(s, "sc_mech_levels")
     return list(sizes[:nl.value]), list(steps[:nl.value + 1])
+
+
+# The reference's materials (statics/src/model.rs:53-58): E, G, and the tensile,
+# compressive and shear strengths, in the order sc_gather's tables take them.
+MATERIALS = {
+    "stone": (30e9, 12e9, 5e6, 100e6, 10e6),
+    "wood": (10e9, 4e9, 40e6, 30e6, 6e6),
+    "masonry": (5e9, 2e9, 0.2e6, 10e6, 0.4e6),
+    "soil": (50e6, 20e6, 5e3, 0.3e6, 20e3),
+    "steel": (200e9, 80e9, 250e6, 250e6, 145e6),
+    "leaves": (0.2e9, 0.08e9, 5e6, 5e6, 1e6),
+}
+
+
+def _material_table(materials) -> np.ndarray:
+    rows = [MATERIALS[m] if isinstance(m, str) else tuple(m) for m in materials]
+    return np.ascontiguousarray(np.array(rows, np.float64).reshape(-1, 5))
+
+
+def gather(lattice: dict, materials, against_full: bool = True, threads: int = 0) -> dict:
+    """statics::gather::gathered (statics/src/gather.rs:193-195), or measured(fine, false)
+    with against_full=False: the next level up of `lattice` (a lattice dict with masses m,
+    bond strengths ft/fc/fs and each node's material index `mat` into `materials`, a list
+    of names of MATERIALS or (E, G, ft, fc, fs) rows). Host code (sc_gather, no device).
+    Returns a lattice dict of the same keys, the gathered level's."""
+    L, keep = _lattice_c(lattice)
+    S, keep_s = _strength_c(lattice)
+    table = _material_table(materials)
+    node_mat = np.ascontiguousarray(lattice["mat"], np.int32)
+    h, nn, nb = C.c_void_p(), C.c_int64(), C.c_int64()
+    s = lib().sc_gather(C.byref(L), C.byref(S), _ptr(node_mat), _ptr(table), len(table), 1 if against_full else 0,
+                        int(threads), C.byref(h), C.byref(nn), C.byref(nb))
+    if s != OK:
+        raise StaticsError(s, "sc_gather")
+    try:
+        n, b = nn.value, nb.value
+        out = dict(x=np.zeros((n, 3)), m=np.zeros(n), held=np.zeros(n, np.uint8), around=np.zeros((n, 2, 3), np.int64),
+                   mat=np.zeros(n, np.int32), bi=np.zeros(b, np.int64), bj=np.zeros(b, np.int64), p=np.zeros((b, 3)),
+                   n=np.zeros((b, 3)), a=np.zeros(b), d=np.zeros(b), e=np.zeros(b), g=np.zeros(b), ft=np.zeros(b),
+                   fc=np.zeros(b), fs=np.zeros(b))
+        level = C.c_int32()
+        lib().sc_gathered_read(h, C.byref(level), *(_ptr(out[k]) for k in
+                                                     ("x", "m", "held", "around", "mat", "bi", "bj", "p", "n", "a",
+                                                      "d", "e", "g", "ft", "fc", "fs")))
+        out["level"] = level.value
+        return out
+    finally:
+        lib().sc_gathered_free(h)
+
+
+def gather_full(material) -> np.ndarray:
+    """gather.rs:203-226: a full cell of `material` (a name of MATERIALS or an (E, G, ft,
+    fc, fs) row) measured a level up; rows (180°, 90°) of (section / s^2, strength / the
+    material's). The calibration `gather` applies against a full cell."""
+    table = _material_table([material])
+    out = np.zeros(4)
+    s = lib().sc_gather_full(_ptr(table), _ptr(out))
+    if s != OK:
+        raise StaticsError(s, "sc_gather_full")
+    return out.reshape(2, 2)
 
 
 def launches() -> int:

@@ -1,0 +1,90 @@
+"""The library's statics::gather (sc_gather: host code, no device) against the CPU
+restatement of statics/src/gather.rs: the same gathered lattice, array for array and bit for
+bit, level after level, on the reference's own bar (gather.rs:403-405) and example scenes
+(statics/examples/statics.rs), measured against a full cell and as it is."""
+import numpy as np
+import pytest
+
+import statics_cuda as sc
+from oracle import oracle as O
+
+NAMES = list(sc.MATERIALS)  # the oracle's material indexes (STONE..LEAVES) in the same order
+KEYS = ("x", "m", "held", "around", "bi", "bj", "p", "n", "a", "d", "e", "g", "ft", "fc", "fs")
+
+
+def _dict(lat, level):
+    d = lat.export()
+    d.update(lat.strengths())
+    d["mat"] = lat.materials()["node"]
+    d["level"] = level
+    return d
+
+
+def _scene(name):
+    if name == "bar":
+        return O.Lattice.block(O.STEEL, [-4.5, -1.0, -1.0], [4.5, 1.0, 1.0], [4.0, 0.2, 0.2])
+    if name == "cantilever":
+        return O.Lattice.scene("cantilever", O.STONE, 0.5, 3.0)
+    return O.Lattice.scene("portico", O.STONE, 1, 0.5)
+
+
+@pytest.mark.parametrize("against_full", [True, False])
+@pytest.mark.parametrize("name", ["bar", "cantilever", "portico"])
+def test_library_gather_is_the_oracles(name, against_full):
+    ora = _scene(name)
+    lib = _dict(ora, 0)
+    for level in (1, 2, 3):
+        ora = ora.gathered(against_full)
+        lib = sc.gather(lib, NAMES, against_full)
+        want = _dict(ora, level)
+        assert lib["level"] == level
+        for key in KEYS + ("mat",):
+            assert lib[key].shape == np.asarray(want[key]).shape, (level, key)
+            assert np.array_equal(lib[key], want[key]), (level, key)
+
+
+def test_library_full_is_the_oracles():
+    """gather.rs:203-226 for every reference material, bit for bit."""
+    for k, name in enumerate(NAMES):
+        assert np.array_equal(sc.gather_full(name), O.full(k)), name
+
+
+def test_library_bar_weighs_as_much():
+    """gather.rs:401-412 through the library."""
+    lat = _dict(_scene("bar"), 0)
+    whole = lat["m"].sum()
+    for _ in range(3):
+        lat = sc.gather(lat, NAMES)
+        assert abs(lat["m"].sum() / whole - 1.0) < 1e-9
+
+
+def test_library_gather_on_any_threads():
+    lat = _dict(_scene("portico"), 0)
+    one = sc.gather(lat, NAMES, threads=1)
+    many = sc.gather(lat, NAMES, threads=7)
+    for key in KEYS + ("mat",):
+        assert np.array_equal(one[key], many[key]), key
+
+
+def test_library_gather_rejects_bad_input():
+    lat = _dict(_scene("cantilever"), 0)
+    bad = dict(lat, mat=lat["mat"].copy())
+    bad["mat"][0] = len(NAMES)  # a material not in the table
+    with pytest.raises(sc.StaticsError):
+        sc.gather(bad, NAMES)
+    bad = dict(lat, a=lat["a"].copy())
+    bad["a"][5] = 0.0  # a bond without section
+    with pytest.raises(sc.StaticsError):
+        sc.gather(bad, NAMES)
+    # a bond between two nodes that share no cell (the reference panics: "a beam is inside a cell")
+    around = lat["around"]
+    far = next(v for v in range(len(around))
+               if not ({tuple(s) for s in around[v]} & {tuple(s) for s in around[lat["bi"][0]]}))
+    bad = dict(lat, bj=lat["bj"].copy())
+    bad["bj"][0] = far
+    with pytest.raises(sc.StaticsError):
+        sc.gather(bad, NAMES)
+    bad = dict(lat, bi=lat["bi"].copy())
+    bad["bi"][0] = len(around)  # out of range
+    with pytest.raises(sc.StaticsError):
+        sc.gather(bad, NAMES)
