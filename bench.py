@@ -356,6 +356,33 @@ def run_probe(args):
             print(json.dumps(out), flush=True)
         solver.close()
         return
+    if args.probe == "gather":
+        # statics::gather (sc_gather, the host's cores) on the reference's timing scene, an
+        # uncut tree (statics/examples/statics.rs:373-391), gathered to levels 1-4; beside it
+        # the oracle's restatement on the same cores, and whether the two levels are the
+        # same bit for bit. The tree itself is built by the oracle's lattice.rs restatement
+        # (the library builds level 0 of voxel pieces only, on the device).
+        from oracle import oracle as O
+        names = list(sc.MATERIALS)
+        sc.gather_full("stone"), O.full(O.STONE)  # both full-cell calibrations made once
+        ora = O.Lattice.scene("tree", O.STONE, 8.0, 1.0, 0.0)
+        lat = dict(ora.export(), **ora.strengths(), mat=ora.materials()["node"], level=0)
+        for level in range(1, 5):
+            t = time.perf_counter()
+            nxt = sc.gather(lat, names)
+            lib_s = time.perf_counter() - t
+            t = time.perf_counter()
+            ora = ora.gathered()
+            ora_s = time.perf_counter() - t
+            want = dict(ora.export(), **ora.strengths())
+            same = all(np.array_equal(nxt[k], want[k]) for k in
+                       ("x", "m", "held", "around", "bi", "bj", "p", "n", "a", "d", "e", "g", "ft", "fc", "fs"))
+            print(json.dumps({"probe": "gather", "scene": "tree(8, 1, 0)", "level": level,
+                              "fine_nodes": int(len(lat["m"])), "fine_bonds": int(len(lat["bi"])),
+                              "nodes": int(len(nxt["m"])), "bonds": int(len(nxt["bi"])), "library_s": lib_s,
+                              "oracle_s": ora_s, "cores": os.cpu_count(), "identical": bool(same)}), flush=True)
+            lat = nxt
+        return
     if args.probe == "large":
         # the large configuration: a 256^3 piece, lognormal k (mu 0, sigma 0.5) clipped to
         # [0.1, 10]; mixed-precision forward solve plus the compliance adjoint, checked
@@ -524,8 +551,9 @@ def main():
     ap.add_argument("--probe-n", type=int, default=N, help="edge of the --probe solve / stencil piece")
     ap.add_argument("--precision", choices=["all", "mixed", "fp64"], default="all",
                     help="the --probe solve precisions: all three twice, or two solves of one")
-    ap.add_argument("--probe", choices=["stencil", "solve", "batch", "large", "mech"],
-                    help="run one kernel or one solve alone (profiling); mech: the engine's solver")
+    ap.add_argument("--probe", choices=["stencil", "solve", "batch", "large", "mech", "gather"],
+                    help="run one kernel or one solve alone (profiling); mech: the engine's solver; "
+                         "gather: statics::gather on the host's cores")
     args = ap.parse_args()
     if args.probe:
         run_probe(args)

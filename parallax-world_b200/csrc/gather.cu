@@ -19,7 +19,10 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -385,8 +388,21 @@ struct SiteHash {
 
 Full full_of(const Mat& mat);
 
+// SC_TIMING=1: each phase's host milliseconds on stderr.
+struct HostPhases {
+    bool on = std::getenv("SC_TIMING") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void mark(const char* phase) {
+        if (!on) return;
+        auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[gather] %-10s %8.2f ms\n", phase, std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
+
 // gather.rs:230-395
 void measured(const FineView& F, const std::vector<Mat>& table, bool against_full, int threads, Gathered& out) {
+    HostPhases ph;
     const int level = F.level + 1;
     std::unordered_map<Site, size_t, SiteHash> index;
     std::vector<Site> sites;
@@ -404,13 +420,15 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
         size_t y = cell_of(F.site(v, 1));
         between[(size_t)v] = {x, y};
     }
+    // The site a bond's ends share is one of its first end's, whose coarse cell the node
+    // pass above has numbered already: no bond adds a cell.
     std::vector<size_t> lies((size_t)F.nb);
     for (int64_t b = 0; b < F.nb; b++) {
         int64_t i = F.bi[b], j = F.bj[b];
         Site si[2] = {F.site(i, 0), F.site(i, 1)}, sj[2] = {F.site(j, 0), F.site(j, 1)};
         int k = (si[0] == sj[0] || si[0] == sj[1]) ? 0 : (si[1] == sj[0] || si[1] == sj[1]) ? 1 : -1;
         require(k >= 0, SC_BAD_INPUT, "a bond whose ends share no cell");
-        lies[(size_t)b] = cell_of(si[k]);
+        lies[(size_t)b] = between[(size_t)i][k];
     }
     const size_t n = sites.size();
     auto face = [&](size_t a, size_t b) { return sites[a] < sites[b] ? std::make_pair(a, b) : std::make_pair(b, a); };
@@ -523,11 +541,13 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
     // A cell without matter of a known material measures as stone (gather.rs:310); the
     // table's first entry stands for it only where such a cell has beams to measure.
     auto mat_value = [&](int32_t k) -> const Mat& { return table[(size_t)std::max<int32_t>(k, 0)]; };
+    ph.mark("index");
     std::vector<Full> fulls(n, Full{std::make_pair(1.0, 1.0), std::make_pair(1.0, 1.0)});
     if (against_full)
         for (size_t c = 0; c < n; c++)
             if (!held[c] && !at[c].empty()) fulls[c] = full_of(mat_value(cmat[c]));
     // Every cell measured, over the host's threads (cells are independent).
+    ph.mark("full");
     std::vector<std::vector<Beam>> found(n);
     auto work = [&](size_t lo, size_t hi) {
         Scratch scr;
@@ -568,6 +588,7 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
             });
         for (auto& th : pool) th.join();
     }
+    ph.mark("measure");
     // Each cell's weight on its faces, as much as each is joined; its beams (gather.rs:370-392).
     out.bi.clear();
     for (size_t c = 0; c < n; c++) {
@@ -615,6 +636,7 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
             }
         }
     }
+    ph.mark("assemble");
 }
 
 // A full block of `mat` at level 0, 6 cells a side about the origin, all free, as
