@@ -272,10 +272,12 @@ sc_status sc_gather(const sc_lattice* fine, const sc_strength* strength, const i
                     sc_gathered** out, int64_t* n_nodes, int64_t* n_bonds);
 /* Copies a gathered level out; any pointer may be NULL. Per node: x (3), m, held, around
  * (6: the two coarse sites it lies between, lesser first), mat (index in the table). Per
- * bond: ends, p (3), n (3), a, d, E, G and the strengths ft, fc, fs (the cell's material
- * made stronger by the beam's measured factor, Mat::stronger, model.rs:71-73). */
+ * bond: ends, material (its cell's, an index in the table), p (3), n (3), a, d, E, G and
+ * the strengths ft, fc, fs (the cell's material made stronger by the beam's measured
+ * factor, Mat::stronger, model.rs:71-73). */
 sc_status sc_gathered_read(const sc_gathered* g, int32_t* level, double* x, double* m, uint8_t* held,
-                           int64_t* around, int32_t* mat, int64_t* bond_i, int64_t* bond_j, double* bond_p,
+                           int64_t* around, int32_t* mat, int64_t* bond_i, int64_t* bond_j, int32_t* bond_mat,
+                           double* bond_p,
                            double* bond_n, double* bond_a, double* bond_d, double* bond_e, double* bond_g,
                            double* ft, double* fc, double* fs);
 void sc_gathered_free(sc_gathered* g);

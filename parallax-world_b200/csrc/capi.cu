@@ -505,7 +505,8 @@ sc_status sc_gather(const sc_lattice* fine, const sc_strength* strength, const i
 }
 
 sc_status sc_gathered_read(const sc_gathered* gp, int32_t* level, double* x, double* m, uint8_t* held,
-                           int64_t* around, int32_t* mat, int64_t* bond_i, int64_t* bond_j, double* bond_p,
+                           int64_t* around, int32_t* mat, int64_t* bond_i, int64_t* bond_j, int32_t* bond_mat,
+                           double* bond_p,
                            double* bond_n, double* bond_a, double* bond_d, double* bond_e, double* bond_g,
                            double* ft, double* fc, double* fs) {
     if (!gp) return SC_BAD_INPUT;
@@ -521,6 +522,7 @@ sc_status sc_gathered_read(const sc_gathered* gp, int32_t* level, double* x, dou
     put(mat, g.mat);
     put(bond_i, g.bi);
     put(bond_j, g.bj);
+    put(bond_mat, g.bmat);
     put(bond_p, g.p);
     put(bond_n, g.n);
     put(bond_a, g.a);

@@ -622,6 +622,7 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
                 V3 p = add(middle, o);
                 out.bi.push_back((int64_t)ia);
                 out.bj.push_back((int64_t)ib);
+                out.bmat.push_back(std::max<int32_t>(cmat[c], 0));
                 for (int t = 0; t < 3; t++) {
                     out.p.push_back(p[t]);
                     out.n.push_back(nrm[t]);

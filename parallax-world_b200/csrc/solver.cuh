@@ -163,6 +163,7 @@ struct Gathered {
     std::vector<int64_t> around;
     std::vector<int32_t> mat;
     std::vector<int64_t> bi, bj;
+    std::vector<int32_t> bmat;  // each bond's material: its cell's
     std::vector<double> p, n, a, d, e, g, ft, fc, fs;
 };
 void gather_level(const sc_lattice& L, const sc_strength& S, const int32_t* node_mat, const sc_material* materials,

@@ -127,7 +127,7 @@ def lib():
                                            P, P]
         L.sc_gather.argtypes = [C.POINTER(LatticeC), C.POINTER(Strength), P, P, C.c_int32, C.c_int32, C.c_int32,
                                 C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
-        L.sc_gathered_read.argtypes = [P, C.POINTER(C.c_int32)] + [P] * 16
+        L.sc_gathered_read.argtypes = [P, C.POINTER(C.c_int32)] + [P] * 17
         L.sc_gathered_free.argtypes = [P]
         L.sc_gathered_free.restype = None
         L.sc_gather_full.argtypes = [P, P]
@@ -251,7 +251,8 @@ def gather(lattice: dict, materials, against_full: bool = True, threads: int = 0
     with against_full=False: the next level up of `lattice` (a lattice dict with masses m,
     bond strengths ft/fc/fs and each node's material index `mat` into `materials`, a list
     of names of MATERIALS or (E, G, ft, fc, fs) rows). Host code (sc_gather, no device).
-    Returns a lattice dict of the same keys, the gathered level's."""
+    Returns a lattice dict of the same keys, the gathered level's, with each bond's
+    material index as `bmat`."""
     L, keep = _lattice_c(lattice)
     S, keep_s = _strength_c(lattice)
     table = _material_table(materials)
@@ -264,12 +265,13 @@ def gather(lattice: dict, materials, against_full: bool = True, threads: int = 0
     try:
         n, b = nn.value, nb.value
         out = dict(x=np.zeros((n, 3)), m=np.zeros(n), held=np.zeros(n, np.uint8), around=np.zeros((n, 2, 3), np.int64),
-                   mat=np.zeros(n, np.int32), bi=np.zeros(b, np.int64), bj=np.zeros(b, np.int64), p=np.zeros((b, 3)),
+                   mat=np.zeros(n, np.int32), bi=np.zeros(b, np.int64), bj=np.zeros(b, np.int64),
+                   bmat=np.zeros(b, np.int32), p=np.zeros((b, 3)),
                    n=np.zeros((b, 3)), a=np.zeros(b), d=np.zeros(b), e=np.zeros(b), g=np.zeros(b), ft=np.zeros(b),
                    fc=np.zeros(b), fs=np.zeros(b))
         level = C.c_int32()
         lib().sc_gathered_read(h, C.byref(level), *(_ptr(out[k]) for k in
-                                                     ("x", "m", "held", "around", "mat", "bi", "bj", "p", "n", "a",
+                                                     ("x", "m", "held", "around", "mat", "bi", "bj", "bmat", "p", "n", "a",
                                                       "d", "e", "g", "ft", "fc", "fs")))
         out["level"] = level.value
         return out

@@ -15,7 +15,8 @@ KEYS = ("x", "m", "held", "around", "bi", "bj", "p", "n", "a", "d", "e", "g", "f
 def _dict(lat, level):
     d = lat.export()
     d.update(lat.strengths())
-    d["mat"] = lat.materials()["node"]
+    mats = lat.materials()
+    d["mat"], d["bmat"] = mats["node"], mats["bond"]
     d["level"] = level
     return d
 
@@ -38,7 +39,7 @@ def test_library_gather_is_the_oracles(name, against_full):
         lib = sc.gather(lib, NAMES, against_full)
         want = _dict(ora, level)
         assert lib["level"] == level
-        for key in KEYS + ("mat",):
+        for key in KEYS + ("mat", "bmat"):
             assert lib[key].shape == np.asarray(want[key]).shape, (level, key)
             assert np.array_equal(lib[key], want[key]), (level, key)
 
