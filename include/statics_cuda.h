@@ -261,13 +261,17 @@ typedef struct sc_gathered sc_gathered;
  * non-negative least squares with beams between faces, each beam's strength from the
  * finer bonds' use when it is pulled alone) and its weight shared out on its faces.
  * `strength` gives each node's mass and each bond's strengths; node_mat (n_nodes) each
- * node's material in `materials` (n_materials entries). Host arrays; runs on the host's
- * cores (threads: 0 = all). The result is the reference's bit for bit: nodes in the order
- * of their face keys, four bonds a beam. *out receives a handle to read with
+ * node's material in `materials` (n_materials entries). Host arrays. With a context the
+ * cells are measured on its device, one thread block a cell; with ctx NULL on the host's
+ * cores (threads: 0 = all); the indexing around them runs on the host either way. The
+ * result is the reference's bit for bit: nodes in the order of their face keys, four
+ * bonds a beam. *out receives a handle to read with
  * sc_gathered_read and free with sc_gathered_free; *n_nodes, *n_bonds its sizes.
  * SC_BAD_INPUT for a bond whose ends share no cell (the reference panics), indexes out of
- * range, or non-finite or non-positive bond or material values. */
-sc_status sc_gather(const sc_lattice* fine, const sc_strength* strength, const int32_t* node_mat,
+ * range, non-finite or non-positive bond or material values, or (on the device) a coarse
+ * cell with more than 12 finer parts, 6 faces or 480 finer bonds, which no lattice that
+ * build or a gather makes has. */
+sc_status sc_gather(sc_context* ctx, const sc_lattice* fine, const sc_strength* strength, const int32_t* node_mat,
                     const sc_material* materials, int32_t n_materials, int32_t against_full, int32_t threads,
                     sc_gathered** out, int64_t* n_nodes, int64_t* n_bonds);
 /* Copies a gathered level out; any pointer may be NULL. Per node: x (3), m, held, around

@@ -454,7 +454,7 @@ sc_status sc_mech_voxel_system(const uint8_t* state, const float* e, int32_t nx,
     }
 }
 
-sc_status sc_gather(const sc_lattice* fine, const sc_strength* strength, const int32_t* node_mat,
+sc_status sc_gather(sc_context* ctx, const sc_lattice* fine, const sc_strength* strength, const int32_t* node_mat,
                     const sc_material* materials, int32_t n_materials, int32_t against_full, int32_t threads,
                     sc_gathered** out, int64_t* n_nodes, int64_t* n_bonds) {
     if (!fine || !strength || !materials || !out || !n_nodes || !n_bonds || n_materials < 1) return SC_BAD_INPUT;
@@ -485,17 +485,16 @@ sc_status sc_gather(const sc_lattice* fine, const sc_strength* strength, const i
             !positive(S.ft[b]) || !positive(S.fc[b]) || !positive(S.fs[b]))
             return SC_BAD_INPUT;
     }
-    try {
-        auto* g = new sc_gathered;
-        try {
-            sc::gather_level(L, S, node_mat, materials, n_materials, against_full != 0, threads, g->g);
-        } catch (...) {
-            delete g;
-            throw;
-        }
-        *out = g;
+    auto run = [&](sc::Context* dev) {
+        auto g = std::make_unique<sc_gathered>();
+        sc::gather_level(dev, L, S, node_mat, materials, n_materials, against_full != 0, threads, g->g);
         *n_nodes = (int64_t)g->g.m.size();
         *n_bonds = (int64_t)g->g.bi.size();
+        *out = g.release();
+    };
+    if (ctx) return guarded(ctx, [&] { run(&ctx->c); });
+    try {
+        run(nullptr);
         return SC_OK;
     } catch (const sc::Error& e) {
         return e.status;

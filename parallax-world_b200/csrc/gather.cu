@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -366,6 +367,500 @@ std::vector<Beam> measure_cell(const CellProblem& cp, const std::vector<V3>& at,
     return found;
 }
 
+// ---- one cell as the phases of a thread block ---------------------------------------
+// The same measurement as measure_cell, written for a CTA: every phase a loop strided by
+// the thread index, a barrier between phases, each entry still summed in bond order by
+// one thread, and the reductions (the pivot, the most negative beam) taken in a fixed
+// order. The kernel runs it with GF_THREADS threads a cell; the host can run it with one
+// thread (gf_emulate), the same code with no barriers, so the CPU can check it against
+// the reference's order bit for bit. The file is compiled without contraction of
+// multiplies and adds (-fmad=false), so the device rounds each operation as the host
+// does. Sizes: a cell of a lattice that build (lattice.rs:124-163) or a gather made has
+// at most 12 free parts (the inner faces of 2 x 2 x 2 finer cells), 6 handles and 480
+// finer bonds (8 finer cells of 15 beams of 4 bonds).
+constexpr int GF_MAXF = 12, GF_MAXH = 6, GF_MAXB = 480, GF_MAXP = 15;
+constexpr int GF_MAXN = 6 * GF_MAXF, GF_MAXM = 3 * GF_MAXH, GF_MAXW = GF_MAXN + GF_MAXM;
+constexpr int GF_THREADS = 256;
+
+#ifdef __CUDA_ARCH__
+#define GF_TID ((int)threadIdx.x)
+#define GF_NT ((int)blockDim.x)
+#define GF_SYNC() __syncthreads()
+#else
+#define GF_TID 0
+#define GF_NT 1
+#define GF_SYNC() ((void)0)
+#endif
+
+struct D3 {
+    double v[3];
+};
+__host__ __device__ inline D3 d3(double a, double b, double c) { return D3{{a, b, c}}; }
+__host__ __device__ inline D3 d_add(D3 a, D3 b) { return d3(a.v[0] + b.v[0], a.v[1] + b.v[1], a.v[2] + b.v[2]); }
+__host__ __device__ inline D3 d_sub(D3 a, D3 b) { return d3(a.v[0] - b.v[0], a.v[1] - b.v[1], a.v[2] - b.v[2]); }
+__host__ __device__ inline D3 d_mul(D3 a, double s) { return d3(a.v[0] * s, a.v[1] * s, a.v[2] * s); }
+__host__ __device__ inline double d_dot(D3 a, D3 b) { return a.v[0] * b.v[0] + a.v[1] * b.v[1] + a.v[2] * b.v[2]; }
+__host__ __device__ inline D3 d_cross(D3 a, D3 b) {
+    return d3(a.v[1] * b.v[2] - a.v[2] * b.v[1], a.v[2] * b.v[0] - a.v[0] * b.v[2], a.v[0] * b.v[1] - a.v[1] * b.v[0]);
+}
+__host__ __device__ inline double d_norm(D3 a) { return sqrt(d_dot(a, a)); }
+__host__ __device__ inline D3 d_unit(D3 a) { return d_mul(a, 1.0 / d_norm(a)); }
+__host__ __device__ inline int64_t d_total_key(double v) {
+#ifdef __CUDA_ARCH__
+    int64_t i = __double_as_longlong(v);
+#else
+    int64_t i;
+    std::memcpy(&i, &v, 8);
+#endif
+    return i ^ (int64_t)(((uint64_t)(i >> 63)) >> 1);
+}
+
+// A finer bond of a packed cell: its point, direction, section, length, E, G, strengths.
+struct GBond {
+    double p[3], n[3], a, d, e, g, ft, fc, fs;
+};
+
+__host__ __device__ inline D3 gb_force(const GBond& b, D3 delta) {  // model.rs:115-119
+    D3 n = d3(b.n[0], b.n[1], b.n[2]);
+    double along = d_dot(delta, n);
+    double k = b.a / b.d;
+    return d_add(d_mul(n, b.e * k * along), d_mul(d_sub(delta, d_mul(n, along)), b.g * k));
+}
+__host__ __device__ inline double mat_used5(const double* m, double s1, double s3) {  // model.rs:66-68
+    return fmax(fmax(s1 / m[2], -s3 / m[3]), (s1 - s3) / (2.0 * m[4]));
+}
+__host__ __device__ inline double gb_used(const GBond& b, D3 f) {  // model.rs:123-129
+    D3 n = d3(b.n[0], b.n[1], b.n[2]);
+    D3 t = d_mul(f, 1.0 / b.a);
+    double sigma = d_dot(t, n);
+    double tau2 = fmax(d_dot(t, t) - sigma * sigma, 0.0);
+    double r = sqrt(sigma * sigma / 4.0 + tau2);
+    const double m[5] = {b.e, b.g, b.ft, b.fc, b.fs};
+    return mat_used5(m, sigma / 2.0 + r, sigma / 2.0 - r);
+}
+__host__ __device__ inline double gb_energy(const GBond& b, D3 f) {  // model.rs:132-136
+    D3 n = d3(b.n[0], b.n[1], b.n[2]);
+    double k = b.a / b.d;
+    double along = d_dot(f, n);
+    return 0.5 * (along * along / (b.e * k) + (d_dot(f, f) - along * along) / (b.g * k));
+}
+
+// One packed cell: nf free parts, nh handles, nb finer bonds (local ends in ij), the
+// places' positions (free parts', then handles'), the cell's material (E, G, ft, fc, fs),
+// the full cell's calibration (section and strength per class), its centre.
+struct CellArgs {
+    int nf, nh, nb, against_full;
+    const uint8_t* ij;
+    const GBond* bonds;
+    const double* place;
+    const double* mat;
+    const double* full;
+    const double* middle;
+    double s;
+};
+
+struct CellSmem {
+    double a[GF_MAXN * GF_MAXW];
+    double x[GF_MAXN * GF_MAXM];
+    double k[GF_MAXM * GF_MAXM];
+    double target[GF_MAXM * GF_MAXM];
+    double f[GF_MAXN];
+    double g[GF_MAXP * (GF_MAXP + 1)];
+    double sol[GF_MAXP];
+    double hold[GF_MAXB], work[GF_MAXB];
+    double place[3 * (GF_MAXF + GF_MAXH)];
+    double uval[GF_MAXP * 36];
+    double fk[GF_MAXP];
+    double scale;
+    int64_t bestkey[GF_THREADS];
+    int32_t bestpos[GF_THREADS];
+    int32_t row[GF_MAXN];
+    int32_t grow[GF_MAXP];
+    int16_t uidx[GF_MAXP * 36];
+    int32_t pa[GF_MAXP], pb[GF_MAXP], idx[GF_MAXP], fa[GF_MAXP], fb[GF_MAXP];
+    int32_t parent[GF_MAXF + GF_MAXH], piece[GF_MAXH];
+    int32_t npairs, mon, nfound, skip, more;
+    uint8_t on[GF_MAXP];
+    uint8_t ij[2 * GF_MAXB];
+};
+
+// gather.rs:164-184 on a small row-major n x (n + rhs) matrix, by one thread (the beams'
+// normal equations): as eliminate above, with the row permutation in `row`.
+__host__ __device__ inline void gf_eliminate_small(double* a, int n, int rhs, int32_t* row, double* x) {
+    const int w = n + rhs;
+    double scale = 0.0;
+    for (int r = 0; r < n; r++) scale = fmax(scale, fabs(a[r * w + r]));
+    for (int r = 0; r < n; r++) row[r] = r;
+    for (int c = 0; c < n; c++) {
+        int p = c;
+        int64_t best = d_total_key(fabs(a[row[c] * w + c]));
+        for (int q = c + 1; q < n; q++) {
+            int64_t k = d_total_key(fabs(a[row[q] * w + c]));
+            if (k >= best) {
+                best = k;
+                p = q;
+            }
+        }
+        int32_t t = row[c];
+        row[c] = row[p];
+        row[p] = t;
+        const double* piv = &a[row[c] * w];
+        if (fabs(piv[c]) <= 1e-12 * scale) continue;
+        for (int r = 0; r < n; r++) {
+            if (r == c) continue;
+            double* ar = &a[row[r] * w];
+            double f = ar[c] / piv[c];
+            if (f != 0.0)
+                for (int k = c; k < w; k++) ar[k] -= f * piv[k];
+        }
+    }
+    for (int r = 0; r < n; r++) {
+        const double* ar = &a[row[r] * w];
+        for (int k = 0; k < rhs; k++) x[r * rhs + k] = fabs(ar[r]) <= 1e-12 * scale ? 0.0 : ar[n + k] / ar[r];
+    }
+}
+
+__host__ __device__ inline int32_t gf_find(int32_t* p, int32_t a) {  // bodies.rs:628-634
+    while (p[a] != a) {
+        p[a] = p[p[a]];
+        a = p[a];
+    }
+    return a;
+}
+
+// The cell's beams into out_ab (a, b per beam), out_ks (stiffness along it, strength
+// factor per beam) and *out_count. F: the finer bonds' forces, m x nb x 3 doubles.
+__host__ __device__ void gf_measure_cell(const CellArgs& A, CellSmem& S, double* F, int32_t* out_ab, double* out_ks,
+                                         int32_t* out_count) {
+    const int tid = GF_TID, nt = GF_NT;
+    const int nf = A.nf, nh = A.nh, nb = A.nb, n = 6 * nf, m = 3 * nh, w = n + m, np = nf + nh;
+    for (int t = tid; t < 3 * np; t += nt) S.place[t] = A.place[t];
+    for (int t = tid; t < 2 * nb; t += nt) S.ij[t] = A.ij[t];
+    for (int t = tid; t < n * w; t += nt) S.a[t] = 0.0;
+    GF_SYNC();
+    auto pos = [&](int v) { return d3(S.place[3 * v], S.place[3 * v + 1], S.place[3 * v + 2]); };
+    auto column = [&](int v, int d, D3 p) -> D3 {
+        D3 e = d3(0.0, 0.0, 0.0);
+        e.v[d % 3] = 1.0;
+        return d < 3 ? e : d_cross(e, d_sub(p, pos(v)));
+    };
+    // gather.rs:84-101: the free parts' rows, a thread a row, each entry in bond order.
+    for (int r = tid; r < n; r += nt) {
+        const int v = r / 6, d = r % 6;
+        double* ar = &S.a[r * w];
+        for (int q = 0; q < nb; q++) {
+            const int bi = S.ij[2 * q], bj = S.ij[2 * q + 1];
+            if (bi != v && bj != v) continue;
+            const GBond& B = A.bonds[q];
+            const double k = B.a / B.d;
+            D3 srow[3];
+            for (int rr = 0; rr < 3; rr++)
+                for (int cc = 0; cc < 3; cc++) {
+                    double nn = B.n[rr] * B.n[cc];
+                    srow[rr].v[cc] = B.e * k * nn + B.g * k * ((rr == cc ? 1.0 : 0.0) - nn);
+                }
+            const D3 p = d3(B.p[0], B.p[1], B.p[2]);
+            const int ends[2] = {bi, bj};
+            const double sgn[2] = {-1.0, 1.0};
+            for (int s1 = 0; s1 < 2; s1++) {
+                if (ends[s1] != v) continue;
+                const double sv = sgn[s1];
+                D3 cv = column(v, d, p);
+                D3 scv = d3(d_dot(srow[0], cv), d_dot(srow[1], cv), d_dot(srow[2], cv));
+                for (int s2 = 0; s2 < 2; s2++) {
+                    const int u = ends[s2];
+                    const double su = sgn[s2];
+                    for (int e = 0; e < 6; e++) {
+                        int c;
+                        if (u < nf)
+                            c = 6 * u + e;
+                        else if (e < 3)
+                            c = n + 3 * (u - nf) + e;
+                        else
+                            continue;
+                        double sign = c < n ? 1.0 : -1.0;
+                        ar[c] += sign * sv * su * d_dot(scv, column(u, e, p));
+                    }
+                }
+            }
+        }
+    }
+    GF_SYNC();
+    // gather.rs:164-184: Gauss–Jordan over the free parts, every handle axis at once.
+    if (tid == 0) {
+        double sc = 0.0;
+        for (int r = 0; r < n; r++) sc = fmax(sc, fabs(S.a[r * w + r]));
+        S.scale = sc;
+    }
+    for (int r = tid; r < n; r += nt) S.row[r] = r;
+    GF_SYNC();
+    const double small = 1e-12 * S.scale;
+    for (int c = 0; c < n; c++) {
+        // the largest |a| at or below the diagonal, the last of equals: the largest
+        // (key, position), whatever the threads' split
+        int64_t bk = INT64_MIN;
+        int32_t bp = -1;
+        for (int q = c + tid; q < n; q += nt) {
+            int64_t k = d_total_key(fabs(S.a[S.row[q] * w + c]));
+            if (k > bk || (k == bk && q > bp)) {
+                bk = k;
+                bp = q;
+            }
+        }
+        S.bestkey[tid] = bk;
+        S.bestpos[tid] = bp;
+        GF_SYNC();
+        if (tid == 0) {
+            int64_t K = S.bestkey[0];
+            int32_t P = S.bestpos[0];
+            for (int t = 1; t < nt; t++)
+                if (S.bestpos[t] >= 0 && (S.bestkey[t] > K || (S.bestkey[t] == K && S.bestpos[t] > P))) {
+                    K = S.bestkey[t];
+                    P = S.bestpos[t];
+                }
+            int32_t t = S.row[c];
+            S.row[c] = S.row[P];
+            S.row[P] = t;
+            S.skip = fabs(S.a[S.row[c] * w + c]) <= small ? 1 : 0;
+        }
+        GF_SYNC();
+        if (S.skip) continue;
+        const double* piv = &S.a[S.row[c] * w];
+        for (int r = tid; r < n; r += nt) S.f[r] = r == c ? 0.0 : S.a[S.row[r] * w + c] / piv[c];
+        GF_SYNC();
+        const int cols = w - c;
+        for (int t = tid; t < n * cols; t += nt) {
+            const int r = t / cols, k = c + t % cols;
+            const double f = S.f[r];
+            if (r == c || f == 0.0) continue;
+            S.a[S.row[r] * w + k] -= f * piv[k];
+        }
+        GF_SYNC();
+    }
+    for (int t = tid; t < n * m; t += nt) {
+        const int r = t / m, k = t % m;
+        const double* ar = &S.a[S.row[r] * w];
+        S.x[t] = fabs(ar[r]) <= small ? 0.0 : ar[n + k] / ar[r];
+    }
+    GF_SYNC();
+    // Each handle axis moved alone: the finer bonds' forces (bodies.rs:420-423).
+    for (int t = tid; t < m * nb; t += nt) {
+        const int c = t / nb, q = t % nb;
+        const GBond& B = A.bonds[q];
+        const D3 p = d3(B.p[0], B.p[1], B.p[2]);
+        auto motion_at = [&](int v) -> D3 {
+            D3 tr = d3(0.0, 0.0, 0.0), ro = d3(0.0, 0.0, 0.0);
+            if (v < nf) {
+                for (int z = 0; z < 3; z++) {
+                    tr.v[z] = S.x[(6 * v + z) * m + c];
+                    ro.v[z] = S.x[(6 * v + 3 + z) * m + c];
+                }
+            } else if (v - nf == c / 3) {
+                tr.v[c % 3] = 1.0;
+            }
+            return d_add(tr, d_cross(ro, d_sub(p, pos(v))));  // bodies.rs:44-47
+        };
+        D3 f = gb_force(B, d_sub(motion_at(S.ij[2 * q + 1]), motion_at(S.ij[2 * q])));
+        for (int z = 0; z < 3; z++) F[(size_t)(c * nb + q) * 3 + z] = f.v[z];
+    }
+    GF_SYNC();
+    // The stiffness between handles (gather.rs:322-333), each entry in bond order.
+    for (int t = tid; t < m * m; t += nt) {
+        const int r = t / m, c = t % m, h = r / 3, z = r % 3;
+        double acc = 0.0;
+        for (int q = 0; q < nb; q++) {
+            const double fz = F[(size_t)(c * nb + q) * 3 + z];
+            if (S.ij[2 * q + 1] == nf + h) acc += 1.0 * fz;
+            if (S.ij[2 * q] == nf + h) acc += -1.0 * fz;
+        }
+        S.k[r * m + c] = acc;
+    }
+    GF_SYNC();
+    // Which handles the matter joins (gather.rs:43-51); the pairs it joins (gather.rs:121-122).
+    if (tid == 0) {
+        for (int t = 0; t < np; t++) S.parent[t] = t;
+        for (int q = 0; q < nb; q++) {
+            int32_t a = gf_find(S.parent, S.ij[2 * q]), b = gf_find(S.parent, S.ij[2 * q + 1]);
+            S.parent[a] = b;
+        }
+        for (int h = 0; h < nh; h++) S.piece[h] = gf_find(S.parent, nf + h);
+        int np2 = 0;
+        for (int a = 0; a < nh; a++)
+            for (int b = a + 1; b < nh; b++)
+                if (S.piece[a] == S.piece[b]) {
+                    S.pa[np2] = a;
+                    S.pb[np2] = b;
+                    S.on[np2] = 1;
+                    np2++;
+                }
+        S.npairs = np2;
+    }
+    GF_SYNC();
+    auto at = [&](int h) { return pos(nf + h); };
+    // A unit of each beam's stiffness (gather.rs:125-139): four 3x3 blocks, in flat order.
+    for (int q = tid; q < S.npairs; q += nt) {
+        const int a = S.pa[q], b = S.pb[q];
+        D3 e = d_unit(d_sub(at(b), at(a)));
+        int j = 0;
+        for (int half = 0; half < 2; half++) {
+            const int r0 = half == 0 ? 3 * a : 3 * b;
+            for (int r = 0; r < 3; r++)
+                for (int side = 0; side < 2; side++) {
+                    const int c0 = side == 0 ? 3 * a : 3 * b;
+                    for (int c = 0; c < 3; c++) {
+                        double v = e.v[r] * e.v[c];
+                        S.uidx[q * 36 + j] = (int16_t)((r0 + r) * m + c0 + c);
+                        S.uval[q * 36 + j] = side == half ? 0.0 + v : 0.0 - v;
+                        j++;
+                    }
+                }
+        }
+    }
+    for (int t = tid; t < m * m; t += nt) S.target[t] = 0.5 * (S.k[(t / m) * m + t % m] + S.k[(t % m) * m + t / m]);
+    GF_SYNC();
+    // Least squares, dropping the most negative beam till none is (gather.rs:143-160).
+    for (;;) {
+        if (tid == 0) {
+            int c = 0;
+            for (int q = 0; q < S.npairs; q++)
+                if (S.on[q]) S.idx[c++] = q;
+            S.mon = c;
+        }
+        GF_SYNC();
+        const int mo = S.mon;
+        for (int t = tid; t < mo * (mo + 1); t += nt) {
+            const int r = t / (mo + 1), c = t % (mo + 1);
+            const double* pv = &S.uval[S.idx[r] * 36];
+            const int16_t* pi = &S.uidx[S.idx[r] * 36];
+            double acc = 0.0;
+            if (c < mo) {
+                const double* qv = &S.uval[S.idx[c] * 36];
+                const int16_t* qi = &S.uidx[S.idx[c] * 36];
+                int i = 0, j = 0;
+                while (i < 36 && j < 36) {
+                    if (pi[i] < qi[j])
+                        i++;
+                    else if (qi[j] < pi[i])
+                        j++;
+                    else {
+                        acc += pv[i] * qv[j];
+                        i++;
+                        j++;
+                    }
+                }
+            } else {
+                for (int i = 0; i < 36; i++) acc += pv[i] * S.target[pi[i]];
+            }
+            S.g[r * (mo + 1) + c] = acc;
+        }
+        GF_SYNC();
+        if (tid == 0) {
+            gf_eliminate_small(S.g, mo, 1, S.grow, S.sol);
+            int worst = -1;
+            for (int r = 0; r < mo; r++)
+                if (S.sol[r] < 0.0 && (worst < 0 || d_total_key(S.sol[r]) < d_total_key(S.sol[worst]))) worst = r;
+            if (worst >= 0) {
+                S.on[S.idx[worst]] = 0;
+                S.more = 1;
+            } else {
+                int c = 0;
+                for (int r = 0; r < mo; r++)
+                    if (S.sol[r] > 0.0) {
+                        S.fa[c] = S.pa[S.idx[r]];
+                        S.fb[c] = S.pb[S.idx[r]];
+                        S.fk[c] = S.sol[r];
+                        c++;
+                    }
+                S.nfound = c;
+                S.more = 0;
+            }
+        }
+        GF_SYNC();
+        if (!S.more) break;
+    }
+    // Each beam pulled alone, a unit apart (gather.rs:337-361).
+    const int nfound = S.nfound;
+    for (int bm = 0; bm < nfound; bm++) {
+        const int a = S.fa[bm], b = S.fb[bm];
+        const D3 e = d_unit(d_sub(at(b), at(a)));
+        for (int q = tid; q < nb; q += nt) {
+            D3 f = d3(0.0, 0.0, 0.0);
+            for (int z = 0; z < 3; z++) {
+                const double* fb_ = &F[(size_t)((3 * b + z) * nb + q) * 3];
+                const double* fa_ = &F[(size_t)((3 * a + z) * nb + q) * 3];
+                f = d_add(f, d_add(d_mul(d3(fb_[0], fb_[1], fb_[2]), e.v[z] / 2.0),
+                                   d_mul(d3(fa_[0], fa_[1], fa_[2]), -e.v[z] / 2.0)));
+            }
+            const double u = gb_used(A.bonds[q], f);
+            const double wq = gb_energy(A.bonds[q], f);
+            S.hold[q] = wq * u;
+            S.work[q] = wq;
+        }
+        GF_SYNC();
+        if (tid == 0) {
+            double hold = 0.0, work = 0.0;
+            for (int q = 0; q < nb; q++) {
+                hold += S.hold[q];
+                work += S.work[q];
+            }
+            const double fine_used = work > 0.0 ? hold / work : 0.0;
+            const double length = d_norm(d_sub(at(b), at(a)));
+            const double own = mat_used5(A.mat, A.mat[0] / length, 0.0);
+            const double stronger = fine_used > 0.0 ? own / fine_used : 1.0;
+            const D3 mid = d3(A.middle[0], A.middle[1], A.middle[2]);
+            const D3 u1 = d_sub(at(a), mid), u2 = d_sub(at(b), mid);
+            const int cls = (int)round(1.0 + d_dot(u1, u2) / (d_norm(u1) * d_norm(u2)));  // lattice.rs:29-32
+            double section = S.fk[bm] * length / A.mat[0] / (A.s * A.s);
+            if (A.against_full) section = section * 0.336 / A.full[2 * cls];  // SECTION, lattice.rs:25
+            out_ab[2 * bm] = a;
+            out_ab[2 * bm + 1] = b;
+            out_ks[2 * bm] = section * A.s * A.s * A.mat[0] / length;
+            out_ks[2 * bm + 1] = stronger / A.full[2 * cls + 1];
+        }
+        GF_SYNC();
+    }
+    if (tid == 0) *out_count = nfound;
+}
+
+// One CTA a cell at a time over the batch; F: each CTA's own forces scratch.
+struct CellBatchView {
+    int32_t ncells, against_full;
+    double s;
+    const int32_t *nf, *nh;
+    const int64_t *bond_ptr, *place_ptr;
+    const uint8_t* ij;
+    const GBond* bonds;
+    const double *place, *mat, *full, *middle;
+    int32_t *out_ab, *out_count;
+    double* out_ks;
+    __host__ __device__ CellArgs cell(int c) const {
+        CellArgs A;
+        A.nf = nf[c];
+        A.nh = nh[c];
+        A.nb = (int)(bond_ptr[c + 1] - bond_ptr[c]);
+        A.against_full = against_full;
+        A.ij = ij + 2 * bond_ptr[c];
+        A.bonds = bonds + bond_ptr[c];
+        A.place = place + 3 * place_ptr[c];
+        A.mat = mat + 5 * (size_t)c;
+        A.full = full + 4 * (size_t)c;
+        A.middle = middle + 3 * (size_t)c;
+        A.s = s;
+        return A;
+    }
+};
+
+__global__ void __launch_bounds__(GF_THREADS) k_gather_cells(CellBatchView B, double* scratch) {
+    extern __shared__ __align__(16) unsigned char gf_smem[];
+    CellSmem& S = *reinterpret_cast<CellSmem*>(gf_smem);
+    double* F = scratch + (size_t)blockIdx.x * GF_MAXM * GF_MAXB * 3;
+    for (int c = blockIdx.x; c < B.ncells; c += gridDim.x) {
+        gf_measure_cell(B.cell(c), S, F, B.out_ab + 2 * GF_MAXP * (size_t)c, B.out_ks + 2 * GF_MAXP * (size_t)c,
+                        B.out_count + c);
+        __syncthreads();
+    }
+}
+
 struct FineView {
     int level;
     int64_t nn, nb;
@@ -400,8 +895,128 @@ struct HostPhases {
     }
 };
 
-// gather.rs:230-395
-void measured(const FineView& F, const std::vector<Mat>& table, bool against_full, int threads, Gathered& out) {
+// The cells to measure, packed for gf_measure_cell: a cell's finer bonds and places
+// contiguous, its material, calibration and centre beside them.
+struct CellBatch {
+    std::vector<int32_t> which, nf, nh;
+    std::vector<int64_t> bond_ptr{0}, place_ptr{0};
+    std::vector<uint8_t> ij;
+    std::vector<GBond> bonds;
+    std::vector<double> place, mat, full, middle;
+    CellBatchView view(double s, bool against_full) {
+        CellBatchView v{};
+        v.ncells = (int32_t)which.size();
+        v.against_full = against_full ? 1 : 0;
+        v.s = s;
+        v.nf = nf.data();
+        v.nh = nh.data();
+        v.bond_ptr = bond_ptr.data();
+        v.place_ptr = place_ptr.data();
+        v.ij = ij.data();
+        v.bonds = bonds.data();
+        v.place = place.data();
+        v.mat = mat.data();
+        v.full = full.data();
+        v.middle = middle.data();
+        return v;
+    }
+};
+
+// gf_measure_cell over the batch on the device: one CTA a cell at a time, as many CTAs as
+// fit on the GPU at once, each with its own forces scratch.
+void measure_on_device(Context& ctx, CellBatch& cb, double s, bool against_full, std::vector<int32_t>& ab,
+                       std::vector<double>& ks, std::vector<int32_t>& count) {
+    const int ncells = (int)cb.which.size();
+    if (!ncells) return;
+    cudaStream_t st = ctx.stream;
+    auto up = [&](auto& buf, const auto& host) {
+        buf.alloc(std::max<size_t>(host.size(), 1), st, &ctx.mem);
+        buf.upload(host.data(), host.size());
+    };
+    DBuf<int32_t> nf, nh, oab, ocount;
+    DBuf<int64_t> bptr, pptr;
+    DBuf<uint8_t> ij;
+    DBuf<GBond> bonds;
+    DBuf<double> place, mat, full, middle, oks, scratch;
+    up(nf, cb.nf);
+    up(nh, cb.nh);
+    up(bptr, cb.bond_ptr);
+    up(pptr, cb.place_ptr);
+    up(ij, cb.ij);
+    up(bonds, cb.bonds);
+    up(place, cb.place);
+    up(mat, cb.mat);
+    up(full, cb.full);
+    up(middle, cb.middle);
+    oab.alloc((size_t)ncells * 2 * GF_MAXP, st, &ctx.mem);
+    oks.alloc((size_t)ncells * 2 * GF_MAXP, st, &ctx.mem);
+    ocount.alloc((size_t)ncells, st, &ctx.mem);
+    const size_t smem = sizeof(CellSmem);
+    SC_CK(cudaFuncSetAttribute(k_gather_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int sms = 0, per = 0;
+    SC_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+    SC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_gather_cells, GF_THREADS, smem));
+    require(per > 0, SC_CUDA, "the cell measurement does not fit on an SM");
+    const int grid = std::min(ncells, sms * per);
+    scratch.alloc((size_t)grid * GF_MAXM * GF_MAXB * 3, st, &ctx.mem);
+    CellBatchView v{};
+    v.ncells = ncells;
+    v.against_full = against_full ? 1 : 0;
+    v.s = s;
+    v.nf = nf.get();
+    v.nh = nh.get();
+    v.bond_ptr = bptr.get();
+    v.place_ptr = pptr.get();
+    v.ij = ij.get();
+    v.bonds = bonds.get();
+    v.place = place.get();
+    v.mat = mat.get();
+    v.full = full.get();
+    v.middle = middle.get();
+    v.out_ab = oab.get();
+    v.out_ks = oks.get();
+    v.out_count = ocount.get();
+    k_gather_cells<<<grid, GF_THREADS, smem, st>>>(v, scratch.get());
+    SC_LAUNCH_CK();
+    ab.resize((size_t)ncells * 2 * GF_MAXP);
+    ks.resize((size_t)ncells * 2 * GF_MAXP);
+    count.resize((size_t)ncells);
+    oab.download(ab.data(), ab.size());
+    oks.download(ks.data(), ks.size());
+    ocount.download(count.data(), count.size());
+    SC_CK(cudaStreamSynchronize(st));
+}
+
+// gf_measure_cell over the batch on the host's cores, one thread a cell (the kernel's
+// code with one thread and no barriers).
+void measure_emulated(CellBatch& cb, double s, bool against_full, size_t threads, std::vector<int32_t>& ab,
+                      std::vector<double>& ks, std::vector<int32_t>& count) {
+    const size_t ncells = cb.which.size();
+    ab.assign(ncells * 2 * GF_MAXP, 0);
+    ks.assign(ncells * 2 * GF_MAXP, 0.0);
+    count.assign(ncells, 0);
+    CellBatchView v = cb.view(s, against_full);
+    v.out_ab = ab.data();
+    v.out_ks = ks.data();
+    v.out_count = count.data();
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        auto S = std::make_unique<CellSmem>();
+        std::vector<double> F((size_t)GF_MAXM * GF_MAXB * 3);
+        for (size_t c; (c = next.fetch_add(1)) < ncells;)
+            gf_measure_cell(v.cell((int)c), *S, F.data(), v.out_ab + 2 * GF_MAXP * c, v.out_ks + 2 * GF_MAXP * c,
+                            v.out_count + c);
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < threads; t++) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+}
+
+// gather.rs:230-395. `dev`: measure the cells on that context's device; else on the
+// host's cores (SC_GATHER_EMULATE set: with the device's code, one thread a cell).
+void measured(const FineView& F, const std::vector<Mat>& table, bool against_full, int threads, Gathered& out,
+              Context* dev = nullptr) {
     HostPhases ph;
     const int level = F.level + 1;
     std::unordered_map<Site, size_t, SiteHash> index;
@@ -570,7 +1185,54 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
         }
     };
     size_t T = threads > 0 ? (size_t)threads : std::max<size_t>(1, std::thread::hardware_concurrency());
-    if (n < 64 || T == 1) {
+    const bool emulate = !dev && std::getenv("SC_GATHER_EMULATE") != nullptr;
+    if (dev || emulate) {
+        CellBatch cb;
+        for (size_t c = 0; c < n; c++) {
+            if (held[c] || at[c].empty()) continue;
+            const size_t nf = free[c].size(), nh = at[c].size(), nb = cbonds[c].size();
+            require(nf <= GF_MAXF && nh <= GF_MAXH && nb <= GF_MAXB, SC_BAD_INPUT,
+                    "a coarse cell holds more finer parts, faces or bonds than a built lattice's");
+            cb.which.push_back((int32_t)c);
+            cb.nf.push_back((int32_t)nf);
+            cb.nh.push_back((int32_t)nh);
+            for (size_t v : free[c])
+                for (int t = 0; t < 3; t++) cb.place.push_back(F.x[3 * v + t]);
+            for (const V3& h : at[c])
+                for (int t = 0; t < 3; t++) cb.place.push_back(h[t]);
+            cb.place_ptr.push_back(cb.place_ptr.back() + (int64_t)(nf + nh));
+            for (const auto& t : cbonds[c]) {
+                const size_t b = t[2];
+                cb.ij.push_back((uint8_t)t[0]);
+                cb.ij.push_back((uint8_t)t[1]);
+                cb.bonds.push_back(GBond{{F.p[3 * b], F.p[3 * b + 1], F.p[3 * b + 2]},
+                                         {F.n[3 * b], F.n[3 * b + 1], F.n[3 * b + 2]},
+                                         F.a[b], F.d[b], F.e[b], F.g[b], F.ft[b], F.fc[b], F.fs[b]});
+            }
+            cb.bond_ptr.push_back(cb.bond_ptr.back() + (int64_t)nb);
+            const Mat& mt = mat_value(cmat[c]);
+            for (double v : {mt.e, mt.g, mt.ft, mt.fc, mt.fs}) cb.mat.push_back(v);
+            for (int k = 0; k < 2; k++) {
+                cb.full.push_back(fulls[c][k].first);
+                cb.full.push_back(fulls[c][k].second);
+            }
+            V3 mid = centre(sites[c], level);
+            for (int t = 0; t < 3; t++) cb.middle.push_back(mid[t]);
+        }
+        ph.mark("pack");
+        std::vector<int32_t> ab, count;
+        std::vector<double> ks;
+        if (dev)
+            measure_on_device(*dev, cb, s, against_full, ab, ks, count);
+        else
+            measure_emulated(cb, s, against_full, T, ab, ks, count);
+        for (size_t i = 0; i < cb.which.size(); i++) {
+            auto& fc = found[(size_t)cb.which[i]];
+            for (int bm = 0; bm < count[i]; bm++)
+                fc.push_back(Beam{(size_t)ab[2 * GF_MAXP * i + 2 * bm], (size_t)ab[2 * GF_MAXP * i + 2 * bm + 1],
+                                  ks[2 * GF_MAXP * i + 2 * bm], ks[2 * GF_MAXP * i + 2 * bm + 1]});
+        }
+    } else if (n < 64 || T == 1) {
         work(0, n);
     } else {
         // Interleaved blocks of cells: a level's cells with matter cluster by first
@@ -764,15 +1426,16 @@ Full full_of(const Mat& mt) {
 
 }  // namespace gth
 
-void gather_level(const sc_lattice& L, const sc_strength& S, const int32_t* node_mat, const sc_material* materials,
-                  int32_t n_materials, bool against_full, int32_t threads, Gathered& out) {
+void gather_level(Context* dev, const sc_lattice& L, const sc_strength& S, const int32_t* node_mat,
+                  const sc_material* materials, int32_t n_materials, bool against_full, int32_t threads,
+                  Gathered& out) {
     std::vector<gth::Mat> table((size_t)n_materials);
     for (int32_t k = 0; k < n_materials; k++)
         table[(size_t)k] = gth::Mat{materials[k].e, materials[k].g, materials[k].ft, materials[k].fc, materials[k].fs};
     gth::FineView F{L.level,  L.n_nodes,  L.n_bonds,  L.x,        S.m,        L.held,     L.around,
                     node_mat, L.bond_i,   L.bond_j,   L.bond_p,   L.bond_n,   L.bond_a,   L.bond_d,
                     L.bond_e, L.bond_g,   S.ft,       S.fc,       S.fs};
-    gth::measured(F, table, against_full, threads, out);
+    gth::measured(F, table, against_full, threads, out, dev);
 }
 
 void gather_full(const sc_material& m, double* out) {

@@ -166,8 +166,10 @@ struct Gathered {
     std::vector<int32_t> bmat;  // each bond's material: its cell's
     std::vector<double> p, n, a, d, e, g, ft, fc, fs;
 };
-void gather_level(const sc_lattice& L, const sc_strength& S, const int32_t* node_mat, const sc_material* materials,
-                  int32_t n_materials, bool against_full, int32_t threads, Gathered& out);
+// dev: measure the cells on that context's device (NULL: on the host's cores)
+void gather_level(Context* dev, const sc_lattice& L, const sc_strength& S, const int32_t* node_mat,
+                  const sc_material* materials, int32_t n_materials, bool against_full, int32_t threads,
+                  Gathered& out);
 void gather_full(const sc_material& m, double* out);
 
 // --- capi.cu / settle.cu -----------------------------------------------------------------

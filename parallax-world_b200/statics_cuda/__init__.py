@@ -125,7 +125,7 @@ def lib():
         L.sc_mech_voxel_system.argtypes = [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                            C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_int64), P, P, P, P, P,
                                            P, P]
-        L.sc_gather.argtypes = [C.POINTER(LatticeC), C.POINTER(Strength), P, P, C.c_int32, C.c_int32, C.c_int32,
+        L.sc_gather.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), P, P, C.c_int32, C.c_int32, C.c_int32,
                                 C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.sc_gathered_read.argtypes = [P, C.POINTER(C.c_int32)] + [P] * 17
         L.sc_gathered_free.argtypes = [P]
@@ -246,11 +246,12 @@ def _material_table(materials) -> np.ndarray:
     return np.ascontiguousarray(np.array(rows, np.float64).reshape(-1, 5))
 
 
-def gather(lattice: dict, materials, against_full: bool = True, threads: int = 0) -> dict:
+def gather(lattice: dict, materials, against_full: bool = True, threads: int = 0, solver=None) -> dict:
     """statics::gather::gathered (statics/src/gather.rs:193-195), or measured(fine, false)
     with against_full=False: the next level up of `lattice` (a lattice dict with masses m,
     bond strengths ft/fc/fs and each node's material index `mat` into `materials`, a list
-    of names of MATERIALS or (E, G, ft, fc, fs) rows). Host code (sc_gather, no device).
+    of names of MATERIALS or (E, G, ft, fc, fs) rows), by sc_gather: the cells measured on
+    `solver`'s device, or on the host's cores without one.
     Returns a lattice dict of the same keys, the gathered level's, with each bond's
     material index as `bmat`."""
     L, keep = _lattice_c(lattice)
@@ -258,7 +259,7 @@ def gather(lattice: dict, materials, against_full: bool = True, threads: int = 0
     table = _material_table(materials)
     node_mat = np.ascontiguousarray(lattice["mat"], np.int32)
     h, nn, nb = C.c_void_p(), C.c_int64(), C.c_int64()
-    s = lib().sc_gather(C.byref(L), C.byref(S), _ptr(node_mat), _ptr(table), len(table), 1 if against_full else 0,
+    s = lib().sc_gather(solver.h if solver is not None else None, C.byref(L), C.byref(S), _ptr(node_mat), _ptr(table), len(table), 1 if against_full else 0,
                         int(threads), C.byref(h), C.byref(nn), C.byref(nb))
     if s != OK:
         raise StaticsError(s, "sc_gather")
@@ -344,6 +345,10 @@ class Solver:
 
     def __del__(self):
         self.close()
+
+    def gather(self, lattice: dict, materials, against_full: bool = True) -> dict:
+        """statics::gather::gathered with the cells measured on this solver's device."""
+        return gather(lattice, materials, against_full, solver=self)
 
     def _check(self, s: int, what: str, soft=(OK, MAXITER, BREAKDOWN, NOT_SPD)):
         if s not in soft:

@@ -1,7 +1,8 @@
-"""The library's statics::gather (sc_gather: host code, no device) against the CPU
+"""The library's statics::gather (sc_gather on the host's cores, no device) against the CPU
 restatement of statics/src/gather.rs: the same gathered lattice, array for array and bit for
 bit, level after level, on the reference's own bar (gather.rs:403-405) and example scenes
-(statics/examples/statics.rs), measured against a full cell and as it is."""
+(statics/examples/statics.rs), measured against a full cell and as it is; and the same for
+the device kernel's per-cell code run on the host (SC_GATHER_EMULATE)."""
 import numpy as np
 import pytest
 
@@ -29,9 +30,14 @@ def _scene(name):
     return O.Lattice.scene("portico", O.STONE, 1, 0.5)
 
 
+@pytest.mark.parametrize("emulated", [False, True])
 @pytest.mark.parametrize("against_full", [True, False])
 @pytest.mark.parametrize("name", ["bar", "cantilever", "portico"])
-def test_library_gather_is_the_oracles(name, against_full):
+def test_library_gather_is_the_oracles(name, against_full, emulated, monkeypatch):
+    """emulated: the cells measured by the device kernel's own code (gf_measure_cell) run by
+    one host thread a cell, so the CPU checks the kernel's indexing and order of operations."""
+    if emulated:
+        monkeypatch.setenv("SC_GATHER_EMULATE", "1")
     ora = _scene(name)
     lib = _dict(ora, 0)
     for level in (1, 2, 3):
