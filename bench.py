@@ -364,24 +364,38 @@ def run_probe(args):
         # (the library builds level 0 of voxel pieces only, on the device).
         from oracle import oracle as O
         names = list(sc.MATERIALS)
+        keys = ("x", "m", "held", "around", "bi", "bj", "p", "n", "a", "d", "e", "g", "ft", "fc", "fs")
         sc.gather_full("stone"), O.full(O.STONE)  # both full-cell calibrations made once
         ora = O.Lattice.scene("tree", O.STONE, 8.0, 1.0, 0.0)
         lat = dict(ora.export(), **ora.strengths(), mat=ora.materials()["node"], level=0)
+        try:  # the device leg: the cells measured by k_gather_cells, one thread block a cell
+            solver = sc.Solver(0)
+            solver.gather(lat, names)  # warm-up: module load, the other materials' calibrations
+        except Exception:
+            solver = None
         for level in range(1, 5):
             t = time.perf_counter()
             nxt = sc.gather(lat, names)
             lib_s = time.perf_counter() - t
+            dev_s = dev_same = None
+            if solver is not None:
+                t = time.perf_counter()
+                dev = solver.gather(lat, names)
+                dev_s = time.perf_counter() - t
+                dev_same = all(np.array_equal(nxt[k], dev[k]) for k in keys)
             t = time.perf_counter()
             ora = ora.gathered()
             ora_s = time.perf_counter() - t
             want = dict(ora.export(), **ora.strengths())
-            same = all(np.array_equal(nxt[k], want[k]) for k in
-                       ("x", "m", "held", "around", "bi", "bj", "p", "n", "a", "d", "e", "g", "ft", "fc", "fs"))
+            same = all(np.array_equal(nxt[k], want[k]) for k in keys)
             print(json.dumps({"probe": "gather", "scene": "tree(8, 1, 0)", "level": level,
                               "fine_nodes": int(len(lat["m"])), "fine_bonds": int(len(lat["bi"])),
                               "nodes": int(len(nxt["m"])), "bonds": int(len(nxt["bi"])), "library_s": lib_s,
-                              "oracle_s": ora_s, "cores": os.cpu_count(), "identical": bool(same)}), flush=True)
+                              "device_s": dev_s, "oracle_s": ora_s, "cores": os.cpu_count(),
+                              "identical": bool(same), "device_identical": dev_same}), flush=True)
             lat = nxt
+        if solver is not None:
+            solver.close()
         return
     if args.probe == "large":
         # the large configuration: a 256^3 piece, lognormal k (mu 0, sigma 0.5) clipped to

@@ -415,9 +415,28 @@ __host__ __device__ inline int64_t d_total_key(double v) {
     return i ^ (int64_t)(((uint64_t)(i >> 63)) >> 1);
 }
 
-// A finer bond of a packed cell: its point, direction, section, length, E, G, strengths.
+// A finer bond: its point, direction, section, length, E, G, strengths.
 struct GBond {
     double p[3], n[3], a, d, e, g, ft, fc, fs;
+};
+// The finer lattice's bonds as the caller holds them (structure of arrays).
+struct BondsSoA {
+    const double *p, *n, *a, *d, *e, *g, *ft, *fc, *fs;
+    __host__ __device__ GBond at(int64_t b) const {
+        GBond r;
+        for (int k = 0; k < 3; k++) {
+            r.p[k] = p[3 * b + k];
+            r.n[k] = n[3 * b + k];
+        }
+        r.a = a[b];
+        r.d = d[b];
+        r.e = e[b];
+        r.g = g[b];
+        r.ft = ft[b];
+        r.fc = fc[b];
+        r.fs = fs[b];
+        return r;
+    }
 };
 
 __host__ __device__ inline D3 gb_force(const GBond& b, D3 delta) {  // model.rs:115-119
@@ -445,13 +464,15 @@ __host__ __device__ inline double gb_energy(const GBond& b, D3 f) {  // model.rs
     return 0.5 * (along * along / (b.e * k) + (d_dot(f, f) - along * along) / (b.g * k));
 }
 
-// One packed cell: nf free parts, nh handles, nb finer bonds (local ends in ij), the
-// places' positions (free parts', then handles'), the cell's material (E, G, ft, fc, fs),
-// the full cell's calibration (section and strength per class), its centre.
+// One packed cell: nf free parts, nh handles, nb finer bonds (local ends in ij, the bond
+// itself at bix in the finer lattice), the places' positions (free parts', then
+// handles'), the cell's material (E, G, ft, fc, fs), the full cell's calibration (section
+// and strength per class), its centre.
 struct CellArgs {
     int nf, nh, nb, against_full;
     const uint8_t* ij;
-    const GBond* bonds;
+    const int64_t* bix;
+    BondsSoA fine;
     const double* place;
     const double* mat;
     const double* full;
@@ -551,7 +572,7 @@ __host__ __device__ void gf_measure_cell(const CellArgs& A, CellSmem& S, double*
         for (int q = 0; q < nb; q++) {
             const int bi = S.ij[2 * q], bj = S.ij[2 * q + 1];
             if (bi != v && bj != v) continue;
-            const GBond& B = A.bonds[q];
+            const GBond B = A.fine.at(A.bix[q]);
             const double k = B.a / B.d;
             D3 srow[3];
             for (int rr = 0; rr < 3; rr++)
@@ -646,7 +667,7 @@ __host__ __device__ void gf_measure_cell(const CellArgs& A, CellSmem& S, double*
     // Each handle axis moved alone: the finer bonds' forces (bodies.rs:420-423).
     for (int t = tid; t < m * nb; t += nt) {
         const int c = t / nb, q = t % nb;
-        const GBond& B = A.bonds[q];
+        const GBond B = A.fine.at(A.bix[q]);
         const D3 p = d3(B.p[0], B.p[1], B.p[2]);
         auto motion_at = [&](int v) -> D3 {
             D3 tr = d3(0.0, 0.0, 0.0), ro = d3(0.0, 0.0, 0.0);
@@ -791,8 +812,9 @@ __host__ __device__ void gf_measure_cell(const CellArgs& A, CellSmem& S, double*
                 f = d_add(f, d_add(d_mul(d3(fb_[0], fb_[1], fb_[2]), e.v[z] / 2.0),
                                    d_mul(d3(fa_[0], fa_[1], fa_[2]), -e.v[z] / 2.0)));
             }
-            const double u = gb_used(A.bonds[q], f);
-            const double wq = gb_energy(A.bonds[q], f);
+            const GBond B = A.fine.at(A.bix[q]);
+            const double u = gb_used(B, f);
+            const double wq = gb_energy(B, f);
             S.hold[q] = wq * u;
             S.work[q] = wq;
         }
@@ -829,7 +851,8 @@ struct CellBatchView {
     const int32_t *nf, *nh;
     const int64_t *bond_ptr, *place_ptr;
     const uint8_t* ij;
-    const GBond* bonds;
+    const int64_t* bix;
+    BondsSoA fine;
     const double *place, *mat, *full, *middle;
     int32_t *out_ab, *out_count;
     double* out_ks;
@@ -840,7 +863,8 @@ struct CellBatchView {
         A.nb = (int)(bond_ptr[c + 1] - bond_ptr[c]);
         A.against_full = against_full;
         A.ij = ij + 2 * bond_ptr[c];
-        A.bonds = bonds + bond_ptr[c];
+        A.bix = bix + bond_ptr[c];
+        A.fine = fine;
         A.place = place + 3 * place_ptr[c];
         A.mat = mat + 5 * (size_t)c;
         A.full = full + 4 * (size_t)c;
@@ -901,7 +925,8 @@ struct CellBatch {
     std::vector<int32_t> which, nf, nh;
     std::vector<int64_t> bond_ptr{0}, place_ptr{0};
     std::vector<uint8_t> ij;
-    std::vector<GBond> bonds;
+    std::vector<int64_t> bix;
+    BondsSoA fine{};
     std::vector<double> place, mat, full, middle;
     CellBatchView view(double s, bool against_full) {
         CellBatchView v{};
@@ -913,7 +938,8 @@ struct CellBatch {
         v.bond_ptr = bond_ptr.data();
         v.place_ptr = place_ptr.data();
         v.ij = ij.data();
-        v.bonds = bonds.data();
+        v.bix = bix.data();
+        v.fine = fine;
         v.place = place.data();
         v.mat = mat.data();
         v.full = full.data();
@@ -924,8 +950,8 @@ struct CellBatch {
 
 // gf_measure_cell over the batch on the device: one CTA a cell at a time, as many CTAs as
 // fit on the GPU at once, each with its own forces scratch.
-void measure_on_device(Context& ctx, CellBatch& cb, double s, bool against_full, std::vector<int32_t>& ab,
-                       std::vector<double>& ks, std::vector<int32_t>& count) {
+void measure_on_device(Context& ctx, CellBatch& cb, int64_t fine_bonds, double s, bool against_full,
+                       std::vector<int32_t>& ab, std::vector<double>& ks, std::vector<int32_t>& count) {
     const int ncells = (int)cb.which.size();
     if (!ncells) return;
     cudaStream_t st = ctx.stream;
@@ -934,16 +960,24 @@ void measure_on_device(Context& ctx, CellBatch& cb, double s, bool against_full,
         buf.upload(host.data(), host.size());
     };
     DBuf<int32_t> nf, nh, oab, ocount;
-    DBuf<int64_t> bptr, pptr;
+    DBuf<int64_t> bptr, pptr, bix;
     DBuf<uint8_t> ij;
-    DBuf<GBond> bonds;
     DBuf<double> place, mat, full, middle, oks, scratch;
     up(nf, cb.nf);
     up(nh, cb.nh);
     up(bptr, cb.bond_ptr);
     up(pptr, cb.place_ptr);
     up(ij, cb.ij);
-    up(bonds, cb.bonds);
+    up(bix, cb.bix);
+    // the finer bonds straight from the caller's arrays
+    DBuf<double> fb[9];
+    const double* src[9] = {cb.fine.p, cb.fine.n, cb.fine.a, cb.fine.d, cb.fine.e,
+                            cb.fine.g, cb.fine.ft, cb.fine.fc, cb.fine.fs};
+    for (int k = 0; k < 9; k++) {
+        const size_t count = (k < 2 ? 3 : 1) * (size_t)fine_bonds;
+        fb[k].alloc(std::max<size_t>(count, 1), st, &ctx.mem);
+        fb[k].upload(src[k], count);
+    }
     up(place, cb.place);
     up(mat, cb.mat);
     up(full, cb.full);
@@ -968,7 +1002,9 @@ void measure_on_device(Context& ctx, CellBatch& cb, double s, bool against_full,
     v.bond_ptr = bptr.get();
     v.place_ptr = pptr.get();
     v.ij = ij.get();
-    v.bonds = bonds.get();
+    v.bix = bix.get();
+    v.fine = BondsSoA{fb[0].get(), fb[1].get(), fb[2].get(), fb[3].get(), fb[4].get(),
+                      fb[5].get(), fb[6].get(), fb[7].get(), fb[8].get()};
     v.place = place.get();
     v.mat = mat.get();
     v.full = full.get();
@@ -1188,6 +1224,9 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
     const bool emulate = !dev && std::getenv("SC_GATHER_EMULATE") != nullptr;
     if (dev || emulate) {
         CellBatch cb;
+        cb.fine = BondsSoA{F.p, F.n, F.a, F.d, F.e, F.g, F.ft, F.fc, F.fs};
+        cb.ij.reserve(2 * (size_t)F.nb);
+        cb.bix.reserve((size_t)F.nb);
         for (size_t c = 0; c < n; c++) {
             if (held[c] || at[c].empty()) continue;
             const size_t nf = free[c].size(), nh = at[c].size(), nb = cbonds[c].size();
@@ -1202,12 +1241,9 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
                 for (int t = 0; t < 3; t++) cb.place.push_back(h[t]);
             cb.place_ptr.push_back(cb.place_ptr.back() + (int64_t)(nf + nh));
             for (const auto& t : cbonds[c]) {
-                const size_t b = t[2];
                 cb.ij.push_back((uint8_t)t[0]);
                 cb.ij.push_back((uint8_t)t[1]);
-                cb.bonds.push_back(GBond{{F.p[3 * b], F.p[3 * b + 1], F.p[3 * b + 2]},
-                                         {F.n[3 * b], F.n[3 * b + 1], F.n[3 * b + 2]},
-                                         F.a[b], F.d[b], F.e[b], F.g[b], F.ft[b], F.fc[b], F.fs[b]});
+                cb.bix.push_back((int64_t)t[2]);
             }
             cb.bond_ptr.push_back(cb.bond_ptr.back() + (int64_t)nb);
             const Mat& mt = mat_value(cmat[c]);
@@ -1223,7 +1259,7 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
         std::vector<int32_t> ab, count;
         std::vector<double> ks;
         if (dev)
-            measure_on_device(*dev, cb, s, against_full, ab, ks, count);
+            measure_on_device(*dev, cb, F.nb, s, against_full, ab, ks, count);
         else
             measure_emulated(cb, s, against_full, T, ab, ks, count);
         for (size_t i = 0; i < cb.which.size(); i++) {
