@@ -919,6 +919,20 @@ struct HostPhases {
     }
 };
 
+// f(lo, hi) over [0, n) in T contiguous ranges on T threads (f must not throw); one
+// range below `least` items.
+template <class Fn>
+void split(size_t n, size_t T, Fn f, size_t least = 4096) {
+    if (T <= 1 || n < least) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < T; t++) pool.emplace_back(f, n * t / T, n * (t + 1) / T);
+    f(0, n / T);
+    for (auto& th : pool) th.join();
+}
+
 // The cells to measure, packed for gf_measure_cell: a cell's finer bonds and places
 // contiguous, its material, calibration and centre beside them.
 struct CellBatch {
@@ -1012,8 +1026,25 @@ void measure_on_device(Context& ctx, CellBatch& cb, int64_t fine_bonds, double s
     v.out_ab = oab.get();
     v.out_ks = oks.get();
     v.out_count = ocount.get();
+    const bool timing = std::getenv("SC_TIMING") != nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing) {
+        SC_CK(cudaEventCreate(&e0));
+        SC_CK(cudaEventCreate(&e1));
+        SC_CK(cudaEventRecord(e0, st));
+    }
     k_gather_cells<<<grid, GF_THREADS, smem, st>>>(v, scratch.get());
     SC_LAUNCH_CK();
+    if (timing) {
+        SC_CK(cudaEventRecord(e1, st));
+        SC_CK(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        SC_CK(cudaEventElapsedTime(&ms, e0, e1));
+        std::fprintf(stderr, "[gather] kernel     %8.3f ms (%d cells, %d blocks of %d threads, %zu B shared)\n", ms,
+                     ncells, grid, GF_THREADS, smem);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
     ab.resize((size_t)ncells * 2 * GF_MAXP);
     ks.resize((size_t)ncells * 2 * GF_MAXP);
     count.resize((size_t)ncells);
@@ -1071,16 +1102,26 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
         size_t y = cell_of(F.site(v, 1));
         between[(size_t)v] = {x, y};
     }
+    ph.mark("cells");
+    const size_t T = threads > 0 ? (size_t)threads : std::max<size_t>(1, std::thread::hardware_concurrency());
     // The site a bond's ends share is one of its first end's, whose coarse cell the node
-    // pass above has numbered already: no bond adds a cell.
+    // pass above has numbered already: no bond adds a cell. Bond by bond, over the threads.
     std::vector<size_t> lies((size_t)F.nb);
-    for (int64_t b = 0; b < F.nb; b++) {
-        int64_t i = F.bi[b], j = F.bj[b];
-        Site si[2] = {F.site(i, 0), F.site(i, 1)}, sj[2] = {F.site(j, 0), F.site(j, 1)};
-        int k = (si[0] == sj[0] || si[0] == sj[1]) ? 0 : (si[1] == sj[0] || si[1] == sj[1]) ? 1 : -1;
-        require(k >= 0, SC_BAD_INPUT, "a bond whose ends share no cell");
-        lies[(size_t)b] = between[(size_t)i][k];
-    }
+    std::atomic<bool> apart{false};
+    split((size_t)F.nb, T, [&](size_t lo, size_t hi) {
+        for (size_t b = lo; b < hi; b++) {
+            int64_t i = F.bi[b], j = F.bj[b];
+            Site si[2] = {F.site(i, 0), F.site(i, 1)}, sj[2] = {F.site(j, 0), F.site(j, 1)};
+            int k = (si[0] == sj[0] || si[0] == sj[1]) ? 0 : (si[1] == sj[0] || si[1] == sj[1]) ? 1 : -1;
+            if (k < 0) {
+                apart = true;
+                return;
+            }
+            lies[b] = between[(size_t)i][k];
+        }
+    });
+    require(!apart, SC_BAD_INPUT, "a bond whose ends share no cell");
+    ph.mark("lies");
     const size_t n = sites.size();
     auto face = [&](size_t a, size_t b) { return sites[a] < sites[b] ? std::make_pair(a, b) : std::make_pair(b, a); };
     // Faces: every (cell, cell across) a node lies between or a bond reaches, in key order.
@@ -1109,23 +1150,62 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
     for (size_t c = 0; c < n; c++)
         for (size_t k = 0; k < free[c].size(); k++) place[free[c][k]] = k;
     // Each bond into its cell's problem; handles numbered by first use (gather.rs:285-294).
-    std::vector<std::vector<size_t>> across(n);
-    std::vector<std::vector<std::array<size_t, 3>>> cbonds(n);
-    for (int64_t b = 0; b < F.nb; b++) {
-        size_t c = lies[(size_t)b];
-        auto at = [&](int64_t v) {
-            size_t x = between[(size_t)v][0], y = between[(size_t)v][1];
-            if (x == c && y == c) return place[(size_t)v];
-            size_t other = x == c ? y : x;
-            auto& ac = across[c];
-            size_t k = (size_t)(std::find(ac.begin(), ac.end(), other) - ac.begin());
-            if (k == ac.size()) ac.push_back(other);
-            return free[c].size() + k;
+    // The bonds grouped by cell in bond order (a stable counting sort), then each cell's
+    // walked in that order on its own thread: the same handles as one pass over all bonds.
+    // Each thread counts its own range of bonds; within a cell, a thread's bonds go after
+    // the threads' before it, so the grouping keeps bond order.
+    std::vector<int64_t> bptr(n + 1, 0), bord((size_t)F.nb);
+    {
+        const size_t nb = (size_t)F.nb, TT = nb < 65536 ? 1 : T;
+        std::vector<std::vector<int64_t>> cnt(TT, std::vector<int64_t>(n, 0));
+        auto range = [&](size_t t) { return std::make_pair(nb * t / TT, nb * (t + 1) / TT); };
+        auto each_thread = [&](auto fn) {
+            std::vector<std::thread> pool;
+            for (size_t t = 1; t < TT; t++) pool.emplace_back(fn, t);
+            fn(0);
+            for (auto& th : pool) th.join();
         };
-        size_t i = at(F.bi[b]);
-        size_t j = at(F.bj[b]);
-        cbonds[c].push_back({i, j, (size_t)b});
+        each_thread([&](size_t t) {
+            auto [lo, hi] = range(t);
+            for (size_t b = lo; b < hi; b++) cnt[t][lies[b]]++;
+        });
+        int64_t at = 0;  // each (cell, thread)'s first slot, cells in order, threads in order
+        for (size_t c = 0; c < n; c++) {
+            bptr[c] = at;
+            for (size_t t = 0; t < TT; t++) {
+                int64_t k = cnt[t][c];
+                cnt[t][c] = at;
+                at += k;
+            }
+        }
+        bptr[n] = at;
+        each_thread([&](size_t t) {
+            auto [lo, hi] = range(t);
+            for (size_t b = lo; b < hi; b++) bord[(size_t)cnt[t][lies[b]]++] = (int64_t)b;
+        });
     }
+    ph.mark("group");
+    std::vector<uint32_t> bli((size_t)F.nb), blj((size_t)F.nb);  // each grouped bond's local ends
+    std::vector<std::vector<size_t>> across(n);
+    split(n, T, [&](size_t lo, size_t hi) {
+        for (size_t c = lo; c < hi; c++) {
+            auto at = [&](int64_t v) {
+                size_t x = between[(size_t)v][0], y = between[(size_t)v][1];
+                if (x == c && y == c) return place[(size_t)v];
+                size_t other = x == c ? y : x;
+                auto& ac = across[c];
+                size_t k = (size_t)(std::find(ac.begin(), ac.end(), other) - ac.begin());
+                if (k == ac.size()) ac.push_back(other);
+                return free[c].size() + k;
+            };
+            for (int64_t q = bptr[c]; q < bptr[c + 1]; q++) {
+                const int64_t b = bord[(size_t)q];
+                bli[(size_t)q] = (uint32_t)at(F.bi[b]);
+                blj[(size_t)q] = (uint32_t)at(F.bj[b]);
+            }
+        }
+    }, 64);
+    ph.mark("handles");
     std::vector<uint8_t> held(n);
     for (size_t c = 0; c < n; c++) {
         bool all = !free[c].empty();
@@ -1210,9 +1290,9 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
             for (size_t v : free[c]) cp.place.push_back({F.x[3 * v], F.x[3 * v + 1], F.x[3 * v + 2]});
             for (const V3& h : at[c]) cp.place.push_back(h);
             cp.bonds.clear();
-            for (const auto& t : cbonds[c]) {
-                size_t b = t[2];
-                cp.bonds.push_back(LBond{t[0], t[1], {F.p[3 * b], F.p[3 * b + 1], F.p[3 * b + 2]},
+            for (int64_t q = bptr[c]; q < bptr[c + 1]; q++) {
+                const size_t b = (size_t)bord[(size_t)q];
+                cp.bonds.push_back(LBond{bli[(size_t)q], blj[(size_t)q], {F.p[3 * b], F.p[3 * b + 1], F.p[3 * b + 2]},
                                          {F.n[3 * b], F.n[3 * b + 1], F.n[3 * b + 2]}, F.a[b], F.d[b], F.e[b], F.g[b],
                                          F.ft[b], F.fc[b], F.fs[b]});
             }
@@ -1220,7 +1300,6 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
                                     scr);
         }
     };
-    size_t T = threads > 0 ? (size_t)threads : std::max<size_t>(1, std::thread::hardware_concurrency());
     const bool emulate = !dev && std::getenv("SC_GATHER_EMULATE") != nullptr;
     if (dev || emulate) {
         CellBatch cb;
@@ -1229,7 +1308,7 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
         cb.bix.reserve((size_t)F.nb);
         for (size_t c = 0; c < n; c++) {
             if (held[c] || at[c].empty()) continue;
-            const size_t nf = free[c].size(), nh = at[c].size(), nb = cbonds[c].size();
+            const size_t nf = free[c].size(), nh = at[c].size(), nb = (size_t)(bptr[c + 1] - bptr[c]);
             require(nf <= GF_MAXF && nh <= GF_MAXH && nb <= GF_MAXB, SC_BAD_INPUT,
                     "a coarse cell holds more finer parts, faces or bonds than a built lattice's");
             cb.which.push_back((int32_t)c);
@@ -1240,10 +1319,10 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
             for (const V3& h : at[c])
                 for (int t = 0; t < 3; t++) cb.place.push_back(h[t]);
             cb.place_ptr.push_back(cb.place_ptr.back() + (int64_t)(nf + nh));
-            for (const auto& t : cbonds[c]) {
-                cb.ij.push_back((uint8_t)t[0]);
-                cb.ij.push_back((uint8_t)t[1]);
-                cb.bix.push_back((int64_t)t[2]);
+            for (int64_t q = bptr[c]; q < bptr[c + 1]; q++) {
+                cb.ij.push_back((uint8_t)bli[(size_t)q]);
+                cb.ij.push_back((uint8_t)blj[(size_t)q]);
+                cb.bix.push_back(bord[(size_t)q]);
             }
             cb.bond_ptr.push_back(cb.bond_ptr.back() + (int64_t)nb);
             const Mat& mt = mat_value(cmat[c]);
