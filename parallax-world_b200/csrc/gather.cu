@@ -385,10 +385,12 @@ constexpr int GF_THREADS = 256;
 #ifdef __CUDA_ARCH__
 #define GF_TID ((int)threadIdx.x)
 #define GF_NT ((int)blockDim.x)
+#define GF_LANES 32
 #define GF_SYNC() __syncthreads()
 #else
 #define GF_TID 0
 #define GF_NT 1
+#define GF_LANES 1
 #define GF_SYNC() ((void)0)
 #endif
 
@@ -493,8 +495,6 @@ struct CellSmem {
     double uval[GF_MAXP * 36];
     double fk[GF_MAXP];
     double scale;
-    int64_t bestkey[GF_THREADS];
-    int32_t bestpos[GF_THREADS];
     int32_t row[GF_MAXN];
     int32_t grow[GF_MAXP];
     int16_t uidx[GF_MAXP * 36];
@@ -618,31 +618,33 @@ __host__ __device__ void gf_measure_cell(const CellArgs& A, CellSmem& S, double*
     const double small = 1e-12 * S.scale;
     for (int c = 0; c < n; c++) {
         // the largest |a| at or below the diagonal, the last of equals: the largest
-        // (key, position), whatever the threads' split
-        int64_t bk = INT64_MIN;
-        int32_t bp = -1;
-        for (int q = c + tid; q < n; q += nt) {
-            int64_t k = d_total_key(fabs(S.a[S.row[q] * w + c]));
-            if (k > bk || (k == bk && q > bp)) {
-                bk = k;
-                bp = q;
-            }
-        }
-        S.bestkey[tid] = bk;
-        S.bestpos[tid] = bp;
-        GF_SYNC();
-        if (tid == 0) {
-            int64_t K = S.bestkey[0];
-            int32_t P = S.bestpos[0];
-            for (int t = 1; t < nt; t++)
-                if (S.bestpos[t] >= 0 && (S.bestkey[t] > K || (S.bestkey[t] == K && S.bestpos[t] > P))) {
-                    K = S.bestkey[t];
-                    P = S.bestpos[t];
+        // (key, position), by the first warp (one lane on the host)
+        if (tid < GF_LANES) {
+            int64_t bk = INT64_MIN;
+            int32_t bp = -1;
+            for (int q = c + tid; q < n; q += GF_LANES) {
+                int64_t k = d_total_key(fabs(S.a[S.row[q] * w + c]));
+                if (k > bk || (k == bk && q > bp)) {
+                    bk = k;
+                    bp = q;
                 }
-            int32_t t = S.row[c];
-            S.row[c] = S.row[P];
-            S.row[P] = t;
-            S.skip = fabs(S.a[S.row[c] * w + c]) <= small ? 1 : 0;
+            }
+#ifdef __CUDA_ARCH__
+            for (int off = 16; off > 0; off >>= 1) {
+                const int64_t ok = __shfl_down_sync(0xffffffffu, bk, off);
+                const int32_t op = __shfl_down_sync(0xffffffffu, bp, off);
+                if (op >= 0 && (ok > bk || (ok == bk && op > bp))) {
+                    bk = ok;
+                    bp = op;
+                }
+            }
+#endif
+            if (tid == 0) {
+                int32_t t = S.row[c];
+                S.row[c] = S.row[bp];
+                S.row[bp] = t;
+                S.skip = fabs(S.a[S.row[c] * w + c]) <= small ? 1 : 0;
+            }
         }
         GF_SYNC();
         if (S.skip) continue;
