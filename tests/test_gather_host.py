@@ -27,12 +27,16 @@ def _scene(name):
         return O.Lattice.block(O.STEEL, [-4.5, -1.0, -1.0], [4.5, 1.0, 1.0], [4.0, 0.2, 0.2])
     if name == "cantilever":
         return O.Lattice.scene("cantilever", O.STONE, 0.5, 3.0)
+    if name.startswith("pendant"):
+        # statics.rs:285-303: a held wall; let go, a layer gone, so a cell's matter no longer
+        # joins all its faces and beams go only between the faces it joins
+        return O.Lattice.scene("pendant", O.STONE, 1 if name.endswith("apart") else 0)
     return O.Lattice.scene("portico", O.STONE, 1, 0.5)
 
 
 @pytest.mark.parametrize("emulated", [False, True])
 @pytest.mark.parametrize("against_full", [True, False])
-@pytest.mark.parametrize("name", ["bar", "cantilever", "portico"])
+@pytest.mark.parametrize("name", ["bar", "cantilever", "portico", "pendant", "pendant_apart"])
 def test_library_gather_is_the_oracles(name, against_full, emulated, monkeypatch):
     """emulated: the cells measured by the device kernel's own code (gf_measure_cell) run by
     one host thread a cell, so the CPU checks the kernel's indexing and order of operations."""
@@ -95,3 +99,13 @@ def test_library_gather_rejects_bad_input():
     bad["bi"][0] = len(around)  # out of range
     with pytest.raises(sc.StaticsError):
         sc.gather(bad, NAMES)
+
+
+def test_library_gather_of_nothing():
+    """An empty lattice gathers to an empty level one up."""
+    z = np.zeros
+    lat = dict(x=z((0, 3)), held=z(0, np.uint8), around=z((0, 2, 3), np.int64), bi=z(0, np.int64),
+               bj=z(0, np.int64), p=z((0, 3)), n=z((0, 3)), a=z(0), d=z(0), e=z(0), g=z(0), m=z(0), ft=z(0),
+               fc=z(0), fs=z(0), mat=z(0, np.int32), level=2)
+    out = sc.gather(lat, NAMES)
+    assert out["level"] == 3 and out["x"].shape == (0, 3) and out["bi"].shape == (0,)
