@@ -1368,8 +1368,9 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
         for (auto& th : pool) th.join();
     }
     ph.mark("measure");
-    // Each cell's weight on its faces, as much as each is joined; its beams (gather.rs:370-392).
-    out.bi.clear();
+    // Each cell's weight on its faces, as much as each is joined (gather.rs:370-381): a
+    // face takes from its two cells in cell order, so this stays one pass.
+    std::vector<int64_t> first(n + 1, 0);  // each cell's first bond of the level
     for (size_t c = 0; c < n; c++) {
         double mass = 0.0;
         for (size_t v : free[c]) mass += F.m[v];
@@ -1382,40 +1383,57 @@ void measured(const FineView& F, const std::vector<Mat>& table, bool against_ful
         double total = 0.0;
         for (double j : joined) total += j;
         for (size_t h = 0; h < nh; h++) out.m[ends[c][h]] += mass * (total > 0.0 ? joined[h] / total : 1.0 / (double)nh);
-        const Mat& mt = mat_value(cmat[c]);
-        for (const Beam& bm : found[c]) {
-            size_t ia = ends[c][bm.a], ib = ends[c][bm.b];
-            if (out.held[ia] && out.held[ib]) continue;
-            V3 pa = at[c][bm.a], pb = at[c][bm.b];
-            double length = norm(sub(pb, pa));
-            double area = bm.k * length / mt.e;
-            // lattice.rs:76-84: four bonds at radius sqrt(A / 2 pi) about the middle
-            V3 nrm = unit(sub(pb, pa));
-            V3 e1 = unit(cross(nrm, std::fabs(nrm[0]) < 0.9 ? V3{1.0, 0.0, 0.0} : V3{0.0, 1.0, 0.0}));
-            V3 e2 = cross(nrm, e1);
-            double r = std::sqrt(area / (2.0 * PI));
-            V3 middle = mul(add(pa, pb), 0.5);
-            double d = norm(sub(pb, pa));
-            const V3 offs[4] = {mul(e1, r), mul(e1, -r), mul(e2, r), mul(e2, -r)};
-            for (const V3& o : offs) {
-                V3 p = add(middle, o);
-                out.bi.push_back((int64_t)ia);
-                out.bj.push_back((int64_t)ib);
-                out.bmat.push_back(std::max<int32_t>(cmat[c], 0));
-                for (int t = 0; t < 3; t++) {
-                    out.p.push_back(p[t]);
-                    out.n.push_back(nrm[t]);
+        int64_t kept = 0;
+        for (const Beam& bm : found[c]) kept += (out.held[ends[c][bm.a]] && out.held[ends[c][bm.b]]) ? 0 : 4;
+        first[c + 1] = first[c] + kept;
+    }
+    // Its beams (gather.rs:382-391), every cell's into its own slots, over the threads.
+    const size_t nbo = (size_t)first[n];
+    out.bi.resize(nbo);
+    out.bj.resize(nbo);
+    out.bmat.resize(nbo);
+    out.p.resize(3 * nbo);
+    out.n.resize(3 * nbo);
+    for (auto* v : {&out.a, &out.d, &out.e, &out.g, &out.ft, &out.fc, &out.fs}) v->resize(nbo);
+    split(n, T, [&](size_t lo, size_t hi) {
+        for (size_t c = lo; c < hi; c++) {
+            size_t q = (size_t)first[c];
+            const Mat& mt = mat_value(cmat[c]);
+            for (const Beam& bm : found[c]) {
+                size_t ia = ends[c][bm.a], ib = ends[c][bm.b];
+                if (out.held[ia] && out.held[ib]) continue;
+                V3 pa = at[c][bm.a], pb = at[c][bm.b];
+                double length = norm(sub(pb, pa));
+                double area = bm.k * length / mt.e;
+                // lattice.rs:76-84: four bonds at radius sqrt(A / 2 pi) about the middle
+                V3 nrm = unit(sub(pb, pa));
+                V3 e1 = unit(cross(nrm, std::fabs(nrm[0]) < 0.9 ? V3{1.0, 0.0, 0.0} : V3{0.0, 1.0, 0.0}));
+                V3 e2 = cross(nrm, e1);
+                double r = std::sqrt(area / (2.0 * PI));
+                V3 middle = mul(add(pa, pb), 0.5);
+                double d = norm(sub(pb, pa));
+                const V3 offs[4] = {mul(e1, r), mul(e1, -r), mul(e2, r), mul(e2, -r)};
+                for (const V3& o : offs) {
+                    V3 p = add(middle, o);
+                    out.bi[q] = (int64_t)ia;
+                    out.bj[q] = (int64_t)ib;
+                    out.bmat[q] = std::max<int32_t>(cmat[c], 0);
+                    for (int t = 0; t < 3; t++) {
+                        out.p[3 * q + t] = p[t];
+                        out.n[3 * q + t] = nrm[t];
+                    }
+                    out.a[q] = area / 4.0;
+                    out.d[q] = d;
+                    out.e[q] = mt.e;
+                    out.g[q] = mt.g;
+                    out.ft[q] = mt.ft * bm.stronger;  // Mat::stronger, model.rs:71-73
+                    out.fc[q] = mt.fc * bm.stronger;
+                    out.fs[q] = mt.fs * bm.stronger;
+                    q++;
                 }
-                out.a.push_back(area / 4.0);
-                out.d.push_back(d);
-                out.e.push_back(mt.e);
-                out.g.push_back(mt.g);
-                out.ft.push_back(mt.ft * bm.stronger);  // Mat::stronger, model.rs:71-73
-                out.fc.push_back(mt.fc * bm.stronger);
-                out.fs.push_back(mt.fs * bm.stronger);
             }
         }
-    }
+    }, 64);
     ph.mark("assemble");
 }
 
