@@ -262,6 +262,8 @@ def gather(lattice: dict, materials, against_full: bool = True, threads: int = 0
     s = lib().sc_gather(solver.h if solver is not None else None, C.byref(L), C.byref(S), _ptr(node_mat), _ptr(table), len(table), 1 if against_full else 0,
                         int(threads), C.byref(h), C.byref(nn), C.byref(nb))
     if s != OK:
+        if solver is not None:
+            solver._check(s, "sc_gather", soft=())
         raise StaticsError(s, "sc_gather")
     try:
         n, b = nn.value, nb.value
