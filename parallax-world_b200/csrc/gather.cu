@@ -1,5 +1,5 @@
 // statics::gather (statics/src/gather.rs:193-395): a coarser level measured from a finer
-// one, on the host's cores.
+// one.
 //
 // Each coarse cell of 2^l Z^3 becomes a small problem of its own: its free parts (finer
 // nodes inside it, 6 unknowns each), one rigid handle per face (3 unknowns each) and the
@@ -9,7 +9,13 @@
 // when the beam is pulled alone. In a full lattice a cell has at most 12 free parts and 6
 // handles (a 72 x 90 elimination, 480 bonds), so the cells form a batch of fixed-shape
 // dense problems. The indexing around them (coarse cells by first appearance, faces in
-// key order, handles by first use) is sequential, as the reference's is.
+// key order, handles by first use) runs on the host, as orderly as the reference's.
+//
+// The cells are measured in one of two forms. measure_cell is the host's: any size, one
+// host thread a cell. gf_measure_cell is the device's (k_gather_cells, one thread block a
+// cell, bounded sizes); the host can also run it with one thread a cell
+// (SC_GATHER_EMULATE), which is how the CPU tests check the kernel's own code. Each form is
+// checked against the CPU restatement of gather.rs.
 //
 // Every floating-point operation is the reference's, in its order, so the gathered
 // lattice is the reference's bit for bit (the CPU restatement checks it). Two places
