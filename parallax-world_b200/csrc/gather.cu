@@ -9,7 +9,7 @@
 // when the beam is pulled alone. In a full lattice a cell has at most 12 free parts and 6
 // handles (a 72 x 90 elimination, 480 bonds), so the cells form a batch of fixed-shape
 // dense problems. The indexing around them (coarse cells by first appearance, faces in
-// key order, handles by first use) runs on the host, as orderly as the reference's.
+// key order, handles by first use) runs on the host, in the reference's orders.
 //
 // The cells are measured in one of two forms. measure_cell is the host's: any size, one
 // host thread a cell. gf_measure_cell is the device's (k_gather_cells, one thread block a
