@@ -109,3 +109,19 @@ def test_library_gather_of_nothing():
                fc=z(0), fs=z(0), mat=z(0, np.int32), level=2)
     out = sc.gather(lat, NAMES)
     assert out["level"] == 3 and out["x"].shape == (0, 3) and out["bi"].shape == (0,)
+
+
+def test_library_gather_matches_committed_levels():
+    """The library's gathered levels are the oracle's committed ones
+    (tests/golden/oracle_gather.json), hashed array by array."""
+    from test_gather_oracle import GOLDEN_SCENES, _digest, _golden
+    rows = _golden()
+    for name, make in GOLDEN_SCENES.items():
+        for against in (True, False):
+            lat = _dict(make(), 0)
+            for level in (1, 2, 3):
+                lat = sc.gather(lat, NAMES, against)
+                want = next(r for r in rows if r["scene"] == name and r["against_full"] == against
+                            and r["level"] == level)
+                got = _digest(lat, len(lat["m"]), len(lat["bi"]))
+                assert got == {k: want[k] for k in got}, (name, against, level)

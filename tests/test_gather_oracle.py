@@ -103,3 +103,44 @@ def test_gather_is_the_same_twice_and_on_any_threads():
     for other in outs[1:]:
         for key in outs[0]:
             assert np.array_equal(outs[0][key], other[key]), key
+
+
+def _digest(d: dict, nodes: int, bonds: int) -> dict:
+    """tests/golden/make_gather_golden.py's digest of a gathered level."""
+    import hashlib
+    h = hashlib.sha256()
+    for k in ("x", "m", "held", "around", "bi", "bj", "p", "n", "a", "d", "e", "g", "ft", "fc", "fs"):
+        h.update(np.ascontiguousarray(d[k]).tobytes())
+    return {"nodes": nodes, "bonds": bonds, "weight": float(d["m"].sum()), "sha256": h.hexdigest()[:32]}
+
+
+GOLDEN_SCENES = {
+    "bar": lambda: O.Lattice.block(O.STEEL, [-4.5, -1.0, -1.0], [4.5, 1.0, 1.0], [4.0, 0.2, 0.2]),
+    "cantilever": lambda: O.Lattice.scene("cantilever", O.STONE, 0.5, 3.0),
+    "pendant_apart": lambda: O.Lattice.scene("pendant", O.STONE, 1),
+}
+
+
+def _golden():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_gather.json")
+    return json.load(open(path))
+
+
+def test_oracle_gather_matches_committed_levels():
+    """The oracle's gathered levels are the committed ones (tests/golden/oracle_gather.json),
+    bit for bit: any change to the restatement shows here."""
+    rows = _golden()
+    assert len(rows) == 18
+    for name, make in GOLDEN_SCENES.items():
+        for against in (True, False):
+            lat = make()
+            for level in (1, 2, 3):
+                lat = lat.gathered(against)
+                e = lat.export()
+                e.update(lat.strengths())
+                want = next(r for r in rows if r["scene"] == name and r["against_full"] == against
+                            and r["level"] == level)
+                got = _digest(e, lat.n_nodes, lat.n_bonds)
+                assert got == {k: want[k] for k in got}, (name, against, level)
