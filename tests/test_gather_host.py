@@ -27,6 +27,8 @@ def _scene(name):
         return O.Lattice.block(O.STEEL, [-4.5, -1.0, -1.0], [4.5, 1.0, 1.0], [4.0, 0.2, 0.2])
     if name == "cantilever":
         return O.Lattice.scene("cantilever", O.STONE, 0.5, 3.0)
+    if name == "rock":  # statics.rs:114-133: stone over soil, two materials a cell may mix
+        return O.Lattice.scene("rock", O.STONE, 1.0, 0.5)
     if name.startswith("pendant"):
         # statics.rs:285-303: a held wall; let go, a layer gone, so a cell's matter no longer
         # joins all its faces and beams go only between the faces it joins
@@ -36,7 +38,7 @@ def _scene(name):
 
 @pytest.mark.parametrize("emulated", [False, True])
 @pytest.mark.parametrize("against_full", [True, False])
-@pytest.mark.parametrize("name", ["bar", "cantilever", "portico", "pendant", "pendant_apart"])
+@pytest.mark.parametrize("name", ["bar", "cantilever", "portico", "pendant", "pendant_apart", "rock"])
 def test_library_gather_is_the_oracles(name, against_full, emulated, monkeypatch):
     """emulated: the cells measured by the device kernel's own code (gf_measure_cell) run by
     one host thread a cell, so the CPU checks the kernel's indexing and order of operations."""
