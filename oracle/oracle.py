@@ -1,7 +1,8 @@
 """ORACLE — test infrastructure only.
 
 ctypes front end of the CPU restatement of the reference's `statics` solve
-(statics/src/{model,lattice,bodies}.rs, built from oracle/*.cpp into
+(statics/src/{model,lattice,bodies}.rs) and its coarse-level gather
+(statics/src/gather.rs), built from oracle/*.cpp into
 oracle/_build/liboracle.so by oracle/Makefile). Only tests/, the smoke check and
 bench.py's CPU-baseline leg import this module; the product never does.
 """

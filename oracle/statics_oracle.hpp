@@ -2,7 +2,8 @@
 //
 // A CPU restatement of the reference's `statics` crate (SupraSummus/parallax-world,
 // Rust): statics/src/model.rs, statics/src/lattice.rs and statics/src/bodies.rs,
-// plus the face order of lattice/src/lib.rs:64 (VOXEL_FACES). Loop orders, merge
+// plus the face order of lattice/src/lib.rs:64 (VOXEL_FACES), and statics/src/gather.rs
+// (gather_oracle.cpp). Loop orders, merge
 // orders and floating-point operation orders follow the Rust source line by line so
 // that node numbering, part numbering and body ids are bit-exact, and FP64 values are
 // the reference's up to the sign of zero (Rust's float `sum()` folds from -0.0).
