@@ -4,7 +4,8 @@ ctypes front end of the CPU restatement of the reference's `statics` solve
 (statics/src/{model,lattice,bodies}.rs) and its coarse-level gather
 (statics/src/gather.rs), built from oracle/*.cpp into
 oracle/_build/liboracle.so by oracle/Makefile). Only tests/, the smoke check and
-bench.py's CPU-baseline leg import this module; the product never does.
+bench.py's CPU legs (the CPU baseline and reference arm; the probes' CPU timings, and the
+reference's scenes the gather probe measures) import this module; the product never does.
 """
 from __future__ import annotations
 
