@@ -117,64 +117,90 @@ def barrier(world):
 
 
 # ---- the CPU legs (the oracle: a restatement of the reference's Rust) ------------------------
-def cpu_sample():
-    """One oracle solve of the bounded sample on all host threads."""
+# Their inputs come from the oracle's own generator (oracle/generate_oracle.cpp, byte-equal
+# to the library's, tests/test_oracle_generator.py): the CPU legs load no product library.
+def oracle_solve(n, seed, threads=None):
+    """One oracle `motions` (setup + PCG, timed by std::chrono inside the oracle) of the
+    seeded n^3 piece under -1 along z per unit mass, to TOL, on `threads` host threads
+    (all of them by default)."""
     import numpy as np
 
-    import statics_cuda as sc
     from oracle import oracle as O
-    st, k = sc.generate_piece(SAMPLE_N, SAMPLE_N, SAMPLE_N, SAMPLE_SEED, sc.K_UNIFORM)
+    st, k = O.generate_piece(n, n, n, seed, O.K_UNIFORM)
     lat = O.Lattice.grid(st, k, g_over_e=0.4, rho=512.0)
     ex = lat.export()
     loads = np.zeros((lat.n_nodes, 6))
     loads[:, 2] = -ex["m"]
-    t = time.perf_counter()
-    _, info = lat.motions(loads, tol=TOL)
-    secs = time.perf_counter() - t
-    dof = 6 * info["counts"][0]
-    return dict(seconds=secs, dof=dof, iterations=info["iterations"], threads=O.threads())
+    before = O.threads()
+    if threads:
+        O.set_threads(threads)
+    try:
+        _, info = lat.motions(loads, tol=TOL)
+        used = O.threads()
+    finally:
+        O.set_threads(before)
+    return dict(seconds=info["seconds"], setup_seconds=info["setup_seconds"], solve_seconds=info["solve_seconds"],
+                dof=6 * info["counts"][0], iterations=info["iterations"], threads=used, n=n, seed=seed)
+
+
+def cpu_sample():
+    """The bounded sample of our arm's CPU baseline: one oracle solve of a 48^3 piece on
+    all host threads (about 5 s on 16 threads)."""
+    return oracle_solve(SAMPLE_N, SAMPLE_SEED)
 
 
 def cpu_baseline_obj(s, dof_iters_target):
     rate = s["dof"] * s["iterations"] / s["seconds"]
     return {"value": rate / dof_iters_target, "unit": "solves/s", "cores": s["threads"], "kind": "port",
-            "dof_iters_per_s": rate,
+            "dof_iters_per_s": rate, "sample_solves_per_s": 1.0 / s["seconds"],
             "sample": f"oracle (C++ restatement of statics/src/bodies.rs) solving a {SAMPLE_N}^3 piece "
                       f"(seed {SAMPLE_SEED}, {s['dof']} DOF, {s['iterations']} iterations) to {TOL:g} in "
-                      f"{s['seconds']:.2f} s on {s['threads']} threads; the {N}^3 rate is that DOF*iters/s "
-                      f"over the {N}^3 solve's DOF*iters (optimistic for the CPU: deeper hierarchies cost more "
-                      f"per DOF*iter)"}
+                      f"{s['seconds']:.2f} s on {s['threads']} threads (sample_solves_per_s); value is that "
+                      f"DOF*iters/s over the {N}^3 solve's DOF*iters. The reference arm "
+                      f"(bench.py --impl reference) times whole {N}^3 solves instead"}
 
 
 def run_reference(args):
+    """The reference's algorithm on the host's cores: the oracle's `motions` (setup + PCG)
+    of the same 128^3 piece, timed whole. Warm-up: W solves of a 24^3 piece. Timed: whole
+    128^3 solves, at least one and at most K, no new one started once --ref-budget
+    seconds have passed. Beside it, one 48^3 solve on one thread."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import statics_cuda as sc  # the generator only (host code)
-    st, _ = sc.generate_piece(N, N, N, args.seed, sc.K_UNIFORM)
-    _, parts = sc.grid_count(st)
-    # the 128^3 solve's iterations are the GPU's, equal to the oracle's (parity tests);
-    # without a GPU here use the committed oracle figure when present
-    iters = 60
-    try:
-        for c in json.load(open(os.path.join(ROOT, "tests", "golden", "oracle_pieces.json"))):
-            if c["n"] == N and c["seed"] == args.seed and c["tol"] == TOL:
-                iters = c["iterations"]
-    except Exception:
-        pass
-    target = 6 * parts * iters
-    for _ in range(args.warmup):
-        cpu_sample()
-    samples = [cpu_sample() for _ in range(args.steps)]
-    secs = sum(s["seconds"] for s in samples)
-    agg = dict(seconds=secs / len(samples), dof=samples[0]["dof"], iterations=samples[0]["iterations"],
-               threads=samples[0]["threads"])
-    cb = cpu_baseline_obj(agg, target)
-    line = {"metric": METRIC, "value": cb["value"], "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
+    for w in range(args.warmup):
+        oracle_solve(24, 100 + w)
+    solves = []
+    t_start = time.perf_counter()
+    while len(solves) < max(1, args.steps):
+        solves.append(oracle_solve(N, args.seed))
+        spent = time.perf_counter() - t_start
+        if spent + solves[-1]["seconds"] > args.ref_budget:
+            break
+    one = oracle_solve(SAMPLE_N, SAMPLE_SEED, threads=1)
+    secs = statistics.mean(s["seconds"] for s in solves)
+    s0 = solves[0]
+    value = 1.0 / secs
+    cores = s0["threads"]
+    sample = (f"{len(solves)} whole oracle motions (setup + PCG) of the {N}^3 piece (seed {args.seed}, "
+              f"{s0['dof']} DOF, {s0['iterations']} iterations to {TOL:g}) on {cores} host threads, "
+              f"std::chrono inside the oracle: mean {secs:.1f} s")
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": len(solves),
+            "warmup": args.warmup, "ms_per_step": 1000.0 * secs, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(args.seed),
-            "impl": "reference", "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "impl": "reference",
+            "steps_note": f"--steps {args.steps} asked; {len(solves)} whole {N}^3 solves timed within "
+                          f"--ref-budget {args.ref_budget:g} s (warm-up: {args.warmup} solves of a 24^3 piece)",
+            "dof_iters_per_s": s0["dof"] * s0["iterations"] / secs,
+            "setup_s": statistics.mean(s["setup_seconds"] for s in solves),
+            "solve_s": statistics.mean(s["solve_seconds"] for s in solves),
+            "seconds_each": [round(s["seconds"], 3) for s in solves],
+            "one_core": {"grid": [SAMPLE_N] * 3, "seed": SAMPLE_SEED, "seconds": one["seconds"],
+                         "dof": one["dof"], "iterations": one["iterations"], "threads": one["threads"],
+                         "solves_per_s": 1.0 / one["seconds"],
+                         "dof_iters_per_s": one["dof"] * one["iterations"] / one["seconds"]},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -557,6 +583,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=600.0,
+                    help="--impl reference: seconds after which no further whole solve is started")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-pieces section")
     ap.add_argument("--batch", type=int, default=512, help="pieces in the batched section")
     ap.add_argument("--batch-sample", type=int, default=64, help="pieces the one-at-a-time FP64 leg solves")

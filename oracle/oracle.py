@@ -66,6 +66,8 @@ def lib():
         L.or_materials.argtypes = [P, pi32, pi32, pd]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_threads.restype = C.c_int
+        L.or_generate_piece.restype = C.c_int
+        L.or_generate_piece.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, pu8, pf]
         _lib = L
     return _lib
 
@@ -80,6 +82,21 @@ def set_threads(n: int) -> None:
 
 def threads() -> int:
     return int(lib().or_threads())
+
+
+K_UNIFORM, K_LOGNORMAL = 0, 1
+CELL_EMPTY, CELL_FREE, CELL_HELD = 0, 1, 2
+
+
+def generate_piece(nx: int, ny: int, nz: int, seed: int, k_dist: int = K_UNIFORM):
+    """The benchmark's seeded synthetic piece (generate_oracle.cpp): state (nx, ny, nz)
+    uint8 of CELL_* and k float32, made without the product library."""
+    state = np.zeros((nx, ny, nz), np.uint8)
+    k = np.zeros((nx, ny, nz), np.float32)
+    rc = lib().or_generate_piece(nx, ny, nz, seed, k_dist, _p(state, C.c_uint8), _p(k, C.c_float))
+    if rc != 0:
+        raise ValueError(f"bad piece dimensions {nx} x {ny} x {nz}")
+    return state, k
 
 
 class Lattice:
