@@ -72,7 +72,9 @@ const char* sc_status_string(sc_status s);
 #define SC_MAX_LEVELS 24
 typedef struct sc_solve_info {
     int64_t iterations;      /* CG iterations */
-    int64_t refinements;     /* SC_MIXED_FP32_KRYLOV: FP64 true-residual replacements */
+    int64_t refinements;     /* FP64 true-residual replacements: SC_MIXED_FP32_KRYLOV's reliable
+                                updates; under SC_FP64 and SC_MIXED, the times the recursive residual
+                                met tol while the true one |b - K x| did not, and was replaced by it */
     int32_t levels;          /* levels of the hierarchy, level 0 included */
     int32_t status;          /* sc_status of the solve (batched solves: of this piece) */
     int64_t parts[SC_MAX_LEVELS];   /* parts per level */
@@ -297,14 +299,18 @@ sc_status sc_gather_full(const sc_material* m, double* out);
  * owns the GPU's memory through its own arena, or a per-frame loop that cannot afford
  * cudaMalloc's implicit device synchronisation. It computes C = f . u (n_values doubles each, device pointers; e.g.
  * the loads and the motions of sc_solve_grid, node order) into *compliance (a device
- * pointer), on `stream` (a cudaStream_t; NULL = the legacy default stream), with the
- * solver's deterministic chunked sum, and allocates nothing: its partial sums live in
- * one 512 KB array inside the library, reserved on every GPU that loads it until the
- * process exits. At most SC_NOALLOC_MAX_VALUES values (SC_BAD_INPUT beyond).
- * The first call on a device looks that array up for the device. Every call shares
- * the array: calls whose kernels may overlap on the
- * GPU race and can return wrong sums, so order them on one stream. Asynchronous:
- * *compliance is ready when `stream` reaches this point.
+ * pointer), on `stream` (a cudaStream_t; NULL = the legacy default stream), with a
+ * deterministic two-stage sum (fixed 8192-value chunks, a tree in each chunk, the chunks
+ * in a fixed order; equal to the solver's dot products up to rounding), and allocates
+ * nothing: its partial sums live in one 512 KB array inside the library, reserved on
+ * every GPU that loads it until the process exits. At most SC_NOALLOC_MAX_VALUES values
+ * (SC_BAD_INPUT beyond). Every call looks that array's address up in the CUDA context
+ * current on the calling thread (the address follows the context, not the device
+ * number), so call it with the device of the pointers current. Every call shares the
+ * array: calls whose kernels may overlap on the GPU race and can return wrong sums, so
+ * order them on one stream. Asynchronous: *compliance is ready when `stream` reaches
+ * this point. SC_CUDA when the lookup or a launch fails (an error the caller left
+ * pending is neither consumed nor reported).
  * ------------------------------------------------------------------------- */
 #define SC_NOALLOC_MAX_VALUES (8192LL * 65536LL)
 sc_status sc_compliance_noalloc(const double* loads, const double* motions, int64_t n_values, double* compliance,
@@ -334,7 +340,8 @@ sc_status sc_mech_voxel_system(const uint8_t* state, const float* e, int32_t nx,
                                double* diag, uint32_t* pi, uint32_t* pj, double* pb, double* b);
 /* Only the levels (Solver::new, host code, no device): *nlevels coarse levels, the parts
  * of each (sizes, up to max_levels), and the smoother steps: steps[0] the nodes', steps[l
- * + 1] coarse level l's (0 for the direct top); steps holds max_levels + 1 values. */
+ * + 1] coarse level l's (0 for the direct top); steps holds max_levels + 1 values.
+ * SC_BAD_INPUT when steps is NULL, or sizes is NULL with max_levels > 0. */
 sc_status sc_mech_levels(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
                          const uint32_t* pi, const uint32_t* pj, const double* pb, double size, int32_t max_levels,
                          int64_t* sizes, double* steps, int32_t* nlevels);

@@ -553,6 +553,7 @@ sc_status sc_mech_levels(int64_t n, const int64_t* sites, const double* at, cons
                          const uint32_t* pi, const uint32_t* pj, const double* pb, double size, int32_t max_levels,
                          int64_t* sizes, double* steps, int32_t* nlevels) {
     if (n <= 0 || npairs < 0 || !sites || !at || !diag || !nlevels || !(size > 0.0) || max_levels < 0) return SC_BAD_INPUT;
+    if (!steps || (max_levels > 0 && !sizes)) return SC_BAD_INPUT;
     if (npairs > 0 && (!pi || !pj || !pb)) return SC_BAD_INPUT;
     for (int64_t p = 0; p < npairs; p++)
         if ((int64_t)pi[p] >= n || (int64_t)pj[p] >= n || pi[p] == pj[p]) return SC_BAD_INPUT;

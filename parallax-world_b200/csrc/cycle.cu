@@ -218,6 +218,7 @@ struct CgScalars {
     int32_t* done;
     int64_t* iters;
     int32_t* status;
+    int64_t* replaced;  // per piece: residual replacements (k_cg_verify)
 };
 
 __global__ void k_cg_init(int np, double tol, CgScalars s, const int32_t* __restrict__ start_done) {
@@ -277,6 +278,22 @@ __global__ void k_cg_beta_flex(int np, CgScalars s, const double* __restrict__ z
     beta[p] = -s.alpha[p] * zap[p] / s.rz[p];
     s.rz[p] = s.next[p];
     s.iters[p] += 1;
+}
+
+// A piece whose recursive residual said converged is held to its true residual
+// rr_true = |b - K x|^2, recomputed in FP64: where that misses the goal the piece goes on
+// (the recursion drifted from b - K x by more than the tolerance) and is counted, so its
+// residual can be replaced by the true one. Pieces stopped by a breakdown or the cap keep
+// their status.
+__global__ void k_cg_verify(int np, CgScalars s, const double* __restrict__ rr_true, int32_t* __restrict__ count) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    if (!s.done[p] || s.status[p] != (int)SC_OK) return;
+    if (!(sqrt(rr_true[p]) <= s.goal[p])) {
+        s.done[p] = 0;
+        s.replaced[p] += 1;
+        atomicAdd(count, 1);
+    }
 }
 
 // The condition of the device-side iteration loop: go on while a piece is not done and
@@ -405,6 +422,7 @@ struct CgState {
     DBuf<double> scal;  // 9 arrays of np
     DBuf<int32_t> flags;
     DBuf<int64_t> iters;
+    DBuf<int64_t> replaced;
     DBuf<int32_t> ndone;
     DBuf<uint32_t> loop_count;  // iterations since the device-side loop's launch
     CgScalars s{};
@@ -419,6 +437,8 @@ struct CgState {
         flags.zero();
         iters.alloc(np, ctx.stream, &ctx.mem);
         iters.zero();
+        replaced.alloc(np, ctx.stream, &ctx.mem);
+        replaced.zero();
         ndone.alloc(1, ctx.stream, &ctx.mem);
         loop_count.alloc(1, ctx.stream, &ctx.mem);
         double* q = scal.get();
@@ -434,6 +454,7 @@ struct CgState {
         s.done = flags.get();
         s.iters = iters.get();
         s.status = status;
+        s.replaced = replaced.get();
     }
 };
 
@@ -513,6 +534,9 @@ static cudaGraphExec_t capture_loop(cudaStream_t st, F&& fill, Context& ctx) {
     cudaGraphDestroy(g);
     return exec;
 }
+
+// Times a solve may replace the residuals of pieces whose true residual missed the goal.
+constexpr int MAX_REPLACEMENTS = 8;
 
 // PCG with per-piece scalars on level 0. V is the vector type of p, r, z, Ap; S the
 // type of x; P the precision of the V-cycle preconditioner (with rp, zp its vectors when
@@ -596,7 +620,53 @@ static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p,
         k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
         SC_LAUNCH_CK();
     };
+    // Residual replacement: r = b - K x in FP64 for the pieces whose true residual misses
+    // the goal (k_cg_verify sets them going again), then z = M r, p = z (a restart from
+    // the current x), and the dots of the next check. Returns whether any piece goes on.
+    static_assert(std::is_same<V, double>::value && std::is_same<S, double>::value,
+                  "the conjugate gradients' vectors and x are FP64");
+    const double* rhs64 = rhs;
     int32_t* ndone_h = ctx.pinned_i32();
+    DBuf<double> res, rr_true;
+    DBuf<int32_t> nrep;
+    res.alloc(n6, st, &ctx.mem);
+    rr_true.alloc(np, st, &ctx.mem);
+    nrep.alloc(1, st, &ctx.mem);
+    auto replace_residuals = [&]() -> bool {
+        if (L.matrix_free)
+            stencil_residual<double>(ctx, b, x, rhs64, res.get(), nullptr, nullptr);
+        else
+            spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), x, rhs64, res.get(), nullptr,
+                         nullptr, L.piece.get(), nullptr, nullptr, L.nnzb);
+        dot2<double>(ctx, L, nullptr, res.get(), res.get(), rr_true.get(), nullptr);
+        SC_CK(cudaMemsetAsync(nrep.get(), 0, sizeof(int32_t), st));
+        k_cg_verify<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, rr_true.get(), nrep.get());
+        SC_LAUNCH_CK();
+        SC_CK(cudaMemcpyAsync(ndone_h, nrep.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SC_CK(cudaStreamSynchronize(st));
+        if (*ndone_h == 0) return false;
+        if (L.nchunks > 0) {
+            k_cast_chunks<double, V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(),
+                                                                          cg.s.done, res.get(), r);
+            SC_LAUNCH_CK();
+            if constexpr (!same) {
+                k_cast_chunks<V, P><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(),
+                                                                          cg.s.done, r, rp);
+                SC_LAUNCH_CK();
+            }
+        }
+        precondition();
+        if (L.nchunks > 0) {
+            k_cast_chunks<P, V><<<(unsigned)L.nchunks, 256, 0, st>>>(L.chunk_lo.get(), L.chunk_piece.get(), cg.s.done,
+                                                                      zs, p);
+            SC_LAUNCH_CK();
+        }
+        dot2<V, P>(ctx, L, cg.s.done, r, zs, cg.s.rz, cg.s.rr);
+        SC_CK(cudaMemsetAsync(cg.ndone.get(), 0, sizeof(int32_t), st));
+        k_cg_check<<<grid_for(np, 128), 128, 0, st>>>(np, max_iter, cg.s, cg.ndone.get());
+        SC_LAUNCH_CK();
+        return true;
+    };
     cudaGraphExec_t exec = nullptr, loop = nullptr;
     int64_t per_iteration = 0, graph_kernels = 0;
     // iterations one launch of the device-side loop runs at most between looks at the
@@ -642,10 +712,16 @@ static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p,
         SC_LAUNCH_CK();
         // iterations run between looks at the done count (finished pieces' kernels return at once)
         const int per_look = 4;
+        int replacements = 0;
         for (;;) {
             SC_CK(cudaMemcpyAsync(ndone_h, cg.ndone.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             SC_CK(cudaStreamSynchronize(st));
-            if (*ndone_h >= np) break;
+            if (*ndone_h >= np) {
+                // every piece stopped: those whose true residual misses the goal take it as
+                // their residual and go on (residual replacement), a bounded number of times
+                if (replacements++ >= MAX_REPLACEMENTS || !replace_residuals()) break;
+                continue;
+            }
             if (timeout_ms > 0 &&
                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count() >
                     timeout_ms)
@@ -722,7 +798,7 @@ void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, So
     SC_CK(cudaStreamSynchronize(ctx.stream));
     count_loop_launches(per_it, it);
     stats.iterations = it;
-    stats.refinements.assign(b.npieces, 0);
+    stats.refinements = cg.replaced.to_host();
     true_residual(ctx, b, x.get(), stats.residual);
 }
 
@@ -847,7 +923,7 @@ void pcg_fp32_cycle(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>&
     SC_CK(cudaStreamSynchronize(ctx.stream));
     count_loop_launches(per_it, it);
     stats.iterations = it;
-    stats.refinements.assign(b.npieces, 0);
+    stats.refinements = cg.replaced.to_host();
     true_residual(ctx, b, x.get(), stats.residual);
 }
 

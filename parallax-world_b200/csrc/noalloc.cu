@@ -8,8 +8,10 @@
 // so every other entry point, which takes its work memory from the device pool, is
 // closed to them.
 //
-// The reduction is the same deterministic two-stage sum the solver uses for its dot
-// products (fixed chunks, fixed-order tree in each chunk, chunks summed in order); its
+// The reduction is a deterministic two-stage sum of its own: fixed 8192-value chunks,
+// a fixed-order tree inside each chunk, and the chunks' partial sums added by one block
+// in a fixed order (strided runs, then a tree). It is not the solver's dot-product sum
+// (whose chunks follow the pieces), so the two agree to rounding, not bit for bit. Its
 // per-chunk partial sums live in one file-scope device array instead of allocated
 // scratch. That array is process-wide: every GPU that loads this library holds its
 // 512 KB until the process exits, every call shares it, and it keeps the last call's
@@ -17,9 +19,12 @@
 // has to start at zero). Two calls whose kernels overlap on the GPU (different streams,
 // no ordering between them) race on it and may return wrong sums: order such calls on
 // one stream, or wait for one before starting the other.
+//
+// The array's device address belongs to the CUDA context that is current, not to the
+// device number: an engine may make its own context current or reset the device between
+// calls. So each call looks the address up again (cudaGetSymbolAddress, which allocates
+// nothing) in the caller's current context, with the caller's device current.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/statics_cuda.h"
 #include "common.cuh"
@@ -50,38 +55,20 @@ __global__ void __launch_bounds__(NOALLOC_BLOCK) k_noalloc_chunks(const double* 
     if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
 }
 
-// The chunks' partial sums added in chunk order by one thread (deterministic).
-__global__ void k_noalloc_total(const double* __restrict__ partial, int64_t chunks, double* __restrict__ out) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// The chunks' partial sums, by one block: thread t adds chunks t, t + 256, ... in order,
+// then a fixed-order tree (deterministic).
+__global__ void __launch_bounds__(NOALLOC_BLOCK) k_noalloc_total(const double* __restrict__ partial, int64_t chunks,
+                                                                 double* __restrict__ out) {
     double s = 0.0;
-    for (int64_t c = 0; c < chunks; c++) s += partial[c];
-    *out = s;
-}
-
-// The array's device address, looked up once per device with that device current. On
-// the host, `g_noalloc_partials` names a host-side stand-in, not device memory, so it is
-// never handed to a kernel.
-constexpr int MAX_DEVICES = 64;
-std::mutex g_lookup;
-double* g_partials_of[MAX_DEVICES] = {};
-
-sc_status partials_for_current_device(double** out) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
-        cudaGetLastError();
-        return SC_NO_DEVICE;
+    for (int64_t c = threadIdx.x; c < chunks; c += NOALLOC_BLOCK) s += partial[c];
+    __shared__ double red[NOALLOC_BLOCK];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = NOALLOC_BLOCK / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
     }
-    std::lock_guard<std::mutex> lock(g_lookup);
-    if (!g_partials_of[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) {
-            cudaGetLastError();
-            return SC_CUDA;
-        }
-        g_partials_of[dev] = static_cast<double*>(p);
-    }
-    *out = g_partials_of[dev];
-    return SC_OK;
+    if (threadIdx.x == 0) *out = red[0];
 }
 
 }  // namespace
@@ -92,18 +79,26 @@ extern "C" sc_status sc_compliance_noalloc(const double* loads, const double* mo
     using namespace sc;
     if (!loads || !motions || !compliance || n_values < 0) return SC_BAD_INPUT;
     if (n_values > SC_NOALLOC_MAX_VALUES) return SC_BAD_INPUT;
-    double* partial = nullptr;
-    sc_status s = partials_for_current_device(&partial);
-    if (s != SC_OK) return s;
+    // the array's address in the current context (on the host, g_noalloc_partials names
+    // a host-side stand-in, never handed to a kernel)
+    void* addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_noalloc_partials) != cudaSuccess || !addr) return SC_CUDA;
+    double* partial = static_cast<double*>(addr);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int64_t chunks = (n_values + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK;
+    // launched through cudaLaunchKernel, whose return value is this launch's own result:
+    // an error the caller left pending is neither consumed nor reported here
     if (chunks > 0) {
-        k_noalloc_chunks<<<(unsigned)chunks, NOALLOC_BLOCK, 0, st>>>(loads, motions, n_values, partial);
+        void* args[] = {(void*)&loads, (void*)&motions, (void*)&n_values, (void*)&partial};
+        if (cudaLaunchKernel((const void*)k_noalloc_chunks, dim3((unsigned)chunks), dim3(NOALLOC_BLOCK), args, 0, st) !=
+            cudaSuccess)
+            return SC_CUDA;
         g_launches.fetch_add(1, std::memory_order_relaxed);
     }
-    k_noalloc_total<<<1, 1, 0, st>>>(partial, chunks, compliance);
+    void* targs[] = {(void*)&partial, (void*)&chunks, (void*)&compliance};
+    if (cudaLaunchKernel((const void*)k_noalloc_total, dim3(1), dim3(NOALLOC_BLOCK), targs, 0, st) != cudaSuccess)
+        return SC_CUDA;
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    if (cudaGetLastError() != cudaSuccess) return SC_CUDA;
     return SC_OK;
 }
 

@@ -93,3 +93,24 @@ def test_status_strings():
     lib = sc.lib()
     for s in range(8):
         assert lib.sc_status_string(s)
+
+
+def test_mech_levels_rejects_missing_outputs():
+    """sc_mech_levels writes steps (and sizes when max_levels > 0): NULL there is
+    SC_BAD_INPUT, never a write through a null pointer."""
+    st, k = piece(8, 1)
+    s = sc.mech_voxel_system(st, k * 1e9, h=0.125, dt=1 / 60, mass=2000 * 0.125 ** 3)
+    arrs = [np.ascontiguousarray(s[name], dt) for name, dt in
+            (("sites", np.int64), ("at", np.float64), ("diag", np.float64), ("pi", np.uint32), ("pj", np.uint32),
+             ("pb", np.float64))]
+    ptr = [a.ctypes.data_as(ctypes.c_void_p) for a in arrs]
+    n, npairs = len(arrs[0]), len(arrs[3])
+    lib = sc.lib()
+    nl = ctypes.c_int32()
+    sizes, steps = np.zeros(4, np.int64), np.zeros(5)
+    args = (n, ptr[0], ptr[1], ptr[2], npairs, ptr[3], ptr[4], ptr[5], ctypes.c_double(0.125))
+    assert lib.sc_mech_levels(*args, 4, sizes.ctypes.data_as(ctypes.c_void_p), None, ctypes.byref(nl)) == sc.BAD_INPUT
+    assert lib.sc_mech_levels(*args, 4, None, steps.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nl)) == sc.BAD_INPUT
+    # a count-only query: no sizes, steps[0] only
+    assert lib.sc_mech_levels(*args, 0, None, steps.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nl)) == sc.OK
+    assert nl.value >= 1
