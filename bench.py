@@ -492,7 +492,7 @@ def run_probe(args):
         solver.close()
         return
     if args.probe == "batch":
-        pieces = batch_pieces(sc, args.batch, 0)
+        pieces = batch_pieces(sc, args.batch)
         solver = sc.Solver(0)
         names = {sc.FP64: "fp64", sc.MIXED: "mixed", sc.MIXED_FP32_KRYLOV: "mixed_fp32_krylov"}
         slow = None
@@ -547,41 +547,77 @@ def run_probe(args):
     solver.close()
 
 
-def batch_pieces(sc, count, rank):
-    """`count` pieces with edges drawn from EDGES per axis, seeded per rank."""
+def batch_pieces(sc, count, seed0=10_000):
+    """`count` pieces with edges drawn from EDGES per axis, seeds seed0 + i. Every rank
+    makes the same batch; batch_share picks its part."""
     import numpy as np
-    rng = np.random.default_rng(777 + rank)
+    rng = np.random.default_rng(777)
     pieces = []
     for i in range(count):
         nx, ny, nz = (int(v) for v in rng.choice(EDGES, 3))
-        pieces.append(sc.generate_piece(nx, ny, nz, 10_000 + count * rank + i, sc.K_UNIFORM))
+        pieces.append(sc.generate_piece(nx, ny, nz, seed0 + i, sc.K_UNIFORM))
     return pieces
 
 
+def batch_share(sc, pieces, rank, world):
+    """This rank's indices into `pieces`: one batch split across the ranks, longest
+    pieces (by unknowns) first (statics_cuda.shard.lpt_split)."""
+    from statics_cuda import shard
+    dof = [6 * sc.grid_count(st)[1] for st, _ in pieces]
+    return shard.lpt_split(dof, world)[rank], dof
+
+
+def batch_stats(infos, tol, world):
+    """Counts and extremes of this rank's solves, summed / maxed over the ranks (one
+    all-reduce each, the same on every rank)."""
+    import torch
+    import torch.distributed as dist
+
+    from statics_cuda import autotune
+    sums = [len(infos), sum(1 for i in infos if i["status"] != 0),
+            sum(1 for i in infos if i["status"] == 0 and not autotune.converged(i, tol)),
+            sum(1 for i in infos if i["refinements"] > 0), sum(1 for i in infos if i.get("retried")),
+            sum(i["iterations"] for i in infos)]
+    worst = max([i["residual"] for i in infos] or [0.0])
+    if world > 1:
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor(sums, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        sums = [float(v) for v in t.tolist()]
+        worst = max_over_ranks(worst, world)
+    return {"pieces": int(sums[0]), "failed": int(sums[1]), "above_tol": int(sums[2]), "replaced": int(sums[3]),
+            "retried": int(sums[4]), "iterations_mean": sums[5] / max(sums[0], 1), "max_true_residual": worst}
+
+
 def batch_section(solver, sc, rank, world, args):
-    """Many pieces of uneven size: BATCH pieces whose edges are drawn from EDGES per axis
-    (seeded per rank), solved by the autotuned mixed-precision batched solve; against the
-    plain FP64 drop-in solving them one call at a time (a seeded sample of them)."""
-    import numpy as np
+    """One batch of BATCH pieces whose edges are drawn from EDGES per axis, split across
+    the ranks (longest first by unknowns) and solved by the autotuned mixed-precision
+    batched solve on each; against the plain FP64 drop-in solving a sample of them one
+    call at a time (the sample split the same way). Time: the max over ranks."""
     import torch
 
     from statics_cuda import autotune
-    pieces = batch_pieces(sc, args.batch, rank)
-    dof = sum(6 * sc.grid_count(p[0])[1] for p in pieces)
+    pieces = batch_pieces(sc, args.batch)
+    mine, dof_all = batch_share(sc, pieces, rank, world)
+    mine_p = [pieces[i] for i in mine]
     t = time.perf_counter()
-    setting = autotune.choose(solver, pieces, sc.MIXED, TOL)
+    setting = autotune.choose(solver, mine_p, sc.MIXED, TOL)
     tune_s = time.perf_counter() - t
     stream = torch.cuda.ExternalStream(solver.stream())
-    autotune.solve_batch(solver, pieces[: min(8, len(pieces))], sc.MIXED, TOL, setting=setting)  # warm-up
+    autotune.solve_batch(solver, mine_p[: min(8, len(mine_p))], sc.MIXED, TOL, setting=setting)  # warm-up
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = sc.launches()
     e0.record(stream)
-    _, infos = autotune.solve_batch(solver, pieces, sc.MIXED, TOL, setting=setting)
+    _, infos = autotune.solve_batch(solver, mine_p, sc.MIXED, TOL, setting=setting)
     e1.record(stream)
     torch.cuda.synchronize()
+    launches = sc.launches() - l0
     ms_b = max_over_ranks(e0.elapsed_time(e1), world)
-    sample = pieces[: min(args.batch_sample, len(pieces))]
+    stats = batch_stats(infos, TOL, world)
+    sample_all = pieces[: min(args.batch_sample, len(pieces))]
+    sample = [sample_all[i] for i in batch_share(sc, sample_all, rank, world)[0]]
     opt64 = sc.options(tol=TOL, precision=sc.FP64)
     solver.solve_grid(*sample[0], opt64)  # warm-up
     barrier(world)
@@ -592,21 +628,21 @@ def batch_section(solver, sc, rank, world, args):
     e1.record(stream)
     torch.cuda.synchronize()
     ms_1 = max_over_ranks(e0.elapsed_time(e1), world)
-    batched = world * len(pieces) / (ms_b / 1000.0)
-    single = world * len(sample) / (ms_1 / 1000.0)
-    failed = sum(1 for i in infos if i["status"] != 0)
-    above = sum(1 for i in infos if i["status"] == 0 and not autotune.converged(i, TOL))
-    replaced = sum(1 for i in infos if i["refinements"] > 0)
-    retried = sum(1 for i in infos if i.get("retried"))
-    return {"workload": f"{len(pieces)} pieces per rank, edges from {list(EDGES)} per axis, seeds 10000+; "
-                        f"value noise period 8 thr 0.5, k U[0.5,2], tol {TOL:g}",
-            "pieces": len(pieces), "dof": dof, "mixed_batched_solves_per_s": batched,
-            "fp64_single_solves_per_s": single, "fp64_single_sample": len(sample),
+    batched = len(pieces) / (ms_b / 1000.0)
+    single = len(sample_all) / (ms_1 / 1000.0)
+    groups = len({(i["setup_ms"], i["solve_ms"]) for i in infos})
+    return {"workload": f"one batch of {len(pieces)} pieces split across {world} rank(s) (longest first by "
+                        f"unknowns), edges from {list(EDGES)} per axis, seeds 10000+; value noise period 8 "
+                        f"thr 0.5, k U[0.5,2], tol {TOL:g}",
+            "scaling": "strong", "pieces": len(pieces), "dof": int(sum(dof_all)),
+            "pieces_this_rank": len(mine_p), "dof_this_rank": int(sum(dof_all[i] for i in mine)),
+            "mixed_batched_solves_per_s": batched,
+            "fp64_single_solves_per_s": single, "fp64_single_sample": len(sample_all),
             "speedup_batched_mixed_vs_fp64_single": batched / single,
-            "mixed_batched_ms": ms_b, "iterations_mean": float(np.mean([i["iterations"] for i in infos])),
-            "pieces_failed": failed, "pieces_true_residual_above_tol": above,
-            "pieces_residual_replaced": replaced,
-            "max_true_residual": max(i["residual"] for i in infos), "pieces_retried": retried,
+            "mixed_batched_ms": ms_b, "iterations_mean": stats["iterations_mean"],
+            "pieces_failed": stats["failed"], "pieces_true_residual_above_tol": stats["above_tol"],
+            "pieces_residual_replaced": stats["replaced"], "max_true_residual": stats["max_true_residual"],
+            "pieces_retried": stats["retried"], "groups_this_rank": groups, "gpu_launches_this_rank": launches,
             "autotune": {"sweeps": setting["sweeps"], "tile": setting["tile"]}, "autotune_seconds": tune_s}
 
 
