@@ -50,9 +50,12 @@ typedef struct sc_options {
                           reference does 1 (bodies.rs:386, 397-401) */
     double inner_tol;  /* unused (kept for layout) */
     int64_t timeout_ms;/* wall-clock bound of one call; 0 = none */
-    int32_t tile;      /* voxel pieces, level-0 stencil: a power of two >= 32 is the window of
-                          parts grouped by axis for the per-part stencil; 0 = that stencil with
-                          1024; 1 = the plane-pencil stencil (cells staged in shared memory) */
+    int32_t tile;      /* voxel pieces, the level-0 stencil of the iterations: 0 = the brick
+                          stencil (the iterations run in brick order: bricks of 4 x 8 x 8 cells,
+                          each brick's faces and halo staged in shared memory); a power of two
+                          >= 32 = the per-part stencil in the reference's part order, with that
+                          window of parts grouped by axis; 1 = the plane-pencil stencil; 2 = the
+                          two-pass stencil. The setup always uses the per-part stencil. */
     int32_t reserved;
 } sc_options;
 
@@ -87,6 +90,11 @@ typedef struct sc_solve_info {
     int64_t n_nodes;         /* nodes of the lattice */
     int64_t n_parts;         /* free nodes: level-0 unknowns / 6 */
     int64_t peak_bytes;      /* device memory held by the solve at its peak */
+    double residual_floor;   /* |K d| / |b| for d = x moved by one unit in the last place of each
+                                value (random signs): about the least relative residual any FP64
+                                vector of motions has for this piece. Where it is above tol (slender
+                                pieces with large motions) the solve stops at it instead: `residual`
+                                is then at most about this, and the status SC_OK. */
 } sc_solve_info;
 
 /* ---------------------------------------------------------------------------
@@ -145,8 +153,14 @@ sc_status sc_compliance_grad(sc_context* ctx, const sc_grid* g, const sc_options
 
 /* Level 0's operator on a piece: y = K x over the free nodes (n_parts x 6, part order),
  * the reference's Level::new + Level::apply (statics/src/bodies.rs:126-206), in FP64
- * (SC_FP64) or FP32 arithmetic (SC_MIXED). Host arrays. For parity checks. */
+ * (SC_FP64) or FP32 arithmetic (SC_MIXED), by the stencil the solve's iterations use
+ * (brick order; x and y are permuted in and out). Host arrays. For parity checks. */
 sc_status sc_grid_apply(sc_context* ctx, const sc_grid* g, int32_t precision, const double* x, double* y);
+/* The same by the stencil `tile` selects (sc_options.tile): 0 the brick-ordered one
+ * above, a power of two >= 32 the per-part stencil in part order (the setup's), 1 the
+ * plane-pencil stencil, 2 the two-pass stencil. */
+sc_status sc_grid_apply_tile(sc_context* ctx, const sc_grid* g, int32_t precision, int32_t tile, const double* x,
+                             double* y);
 
 /* After a solve: the body of each part at level `level` (the reference's `up` from
  * bodies_of, statics/src/bodies.rs:472-496), parts[level] entries; and piece-level
@@ -242,6 +256,19 @@ typedef struct sc_settle_info {
  * until a round breaks nothing. gone: n_nodes bytes (host), 1 for a fallen node. */
 sc_status sc_settle(sc_context* ctx, const sc_lattice* lattice, const sc_strength* strength, const sc_options* opt,
                     uint8_t* gone, sc_settle_info* out);
+
+/* Replaces statics::bodies::as_generated (statics/src/bodies.rs:611-625): the strength a
+ * lattice needs to stand as its world was generated, MARGIN = 2 times (bodies.rs:605).
+ * Every beam of `generated` (bonds keyed by the cells their two end nodes lie between,
+ * `around`, the lesser pair first) needs the most of its strength any of its bonds uses
+ * standing (sc_used_standing of `generated`, solved on the device); each bond of
+ * `lattice` on such a beam becomes max(2 * that, 1) times as strong (Mat::stronger,
+ * statics/src/model.rs:71-73), the others keep theirs. The reference changes the
+ * lattice's materials in place; here the new strengths go to ft, fc, fs (n_bonds of
+ * `lattice`, host) and the inputs stay as they are. */
+sc_status sc_as_generated(sc_context* ctx, const sc_lattice* lattice, const sc_strength* strength,
+                          const sc_lattice* generated, const sc_strength* generated_strength,
+                          const sc_options* opt, double* ft, double* fc, double* fs);
 
 /* ---------------------------------------------------------------------------
  * Coarser levels measured from finer ones: statics::gather (statics/src/gather.rs).

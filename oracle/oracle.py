@@ -54,6 +54,8 @@ def lib():
         L.or_settle.argtypes = [P, pd, pi64, pu8]
         L.or_strengths.argtypes = [P, pd, pd, pd]
         L.or_as_generated.argtypes = [P, P]
+        L.or_clone.restype = P
+        L.or_clone.argtypes = [P]
         L.or_level0_apply.argtypes = [P, I64, pd, pd]
         L.or_invert.argtypes = [pd, pd]
         L.or_coarse_site.argtypes = [pi64, C.c_uint32, pi64]
@@ -217,7 +219,14 @@ class Lattice:
         return fallen.value, rounds.value, gone
 
     def as_generated(self, generated: "Lattice") -> None:
+        """bodies.rs:611-625: each bond's strength no less than MARGIN times what the same
+        beam of `generated` uses standing (in place)."""
         lib().or_as_generated(self.h, generated.h)
+
+    def copy(self) -> "Lattice":
+        lat = Lattice(lib().or_clone(self.h))
+        lat.level = getattr(self, "level", 0)
+        return lat
 
     def gathered(self, against_full: bool = True) -> "Lattice":
         """gather.rs:193-195 (or measured(fine, false), gather.rs:230-395): the next

@@ -211,6 +211,13 @@ void or_settle(void* p, double* fallen, int64_t* rounds, uint8_t* gone) {
         for (size_t v = 0; v < o.gone.size(); v++) gone[v] = o.gone[v] ? 1 : 0;
 }
 
+// A copy of a lattice (Lattice::clone), as a new handle.
+void* or_clone(void* p) {
+    auto* h = new Handle;
+    *h = *static_cast<Handle*>(p);
+    return h;
+}
+
 void or_as_generated(void* lattice, void* generated) {
     as_generated(static_cast<Handle*>(lattice)->lat, static_cast<Handle*>(generated)->lat);
 }

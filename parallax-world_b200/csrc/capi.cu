@@ -239,6 +239,7 @@ void fill_info(const Batch& b, int piece, const SolveStats& st, sc_solve_info* i
         info->blocks[l] = b.npieces == 1 ? L.nnzb : 0;
     }
     info->residual = st.residual.empty() ? 0 : st.residual[piece];
+    info->residual_floor = st.floor.empty() ? 0 : st.floor[piece];
     info->work = work_of(b, piece, info->iterations);
     info->setup_ms = b.setup_ms;
     info->solve_ms = solve_ms;
@@ -263,6 +264,15 @@ sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double
     b.sweeps = opt.sweeps;
     build_hierarchy(ctx, b, opt);
     PhaseTimer pt(ctx);
+    if (b.levels[0].matrix_free && b.grid.use_bricks) {
+        // the iterations run in brick order (brick.cu); its layout counts as setup
+        auto tb = std::chrono::steady_clock::now();
+        bricks_build(ctx, b);
+        bricks_enter(ctx, b);
+        SC_CK(cudaStreamSynchronize(ctx.stream));
+        b.setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+        pt.mark("brick layout");
+    }
     auto t0 = std::chrono::steady_clock::now();
     if (opt.precision == SC_MIXED)
         pcg_fp32_cycle(ctx, b, opt, x, st);
@@ -270,6 +280,7 @@ sc_status solve_batch(Context& ctx, Batch& b, const sc_options& opt, DBuf<double
         pcg_mixed(ctx, b, opt, x, st);
     else
         pcg_fp64(ctx, b, opt, x, st);
+    bricks_leave(ctx, b, &x);  // x back in the reference's part order
     SC_CK(cudaStreamSynchronize(ctx.stream));
     solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     pt.mark("conjugate gradients");
@@ -302,6 +313,20 @@ sc_status lattice_motions(Context& c, const sc_lattice& lat, const uint8_t* aliv
                           const double* loads, const sc_options& opt, double* out, sc_solve_info* info) {
     auto b = std::make_unique<Batch>();
     c.last.reset();  // the previous solve's hierarchy is not kept through this one
+    // Every node held or gone: nothing to solve, every motion zero (the reference's CG
+    // stops at once on an empty right-hand side, bodies.rs:350-352).
+    bool any_part = false;
+    for (int64_t v = 0; v < lat.n_nodes && !any_part; v++) any_part = !lat.held[v] && !(gone && gone[v]);
+    if (!any_part) {
+        SC_CK(cudaMemsetAsync(out, 0, 6 * lat.n_nodes * sizeof(double), c.stream));
+        SC_CK(cudaStreamSynchronize(c.stream));
+        if (info) {
+            std::memset(info, 0, sizeof(*info));
+            info->levels = 0;
+            info->n_nodes = lat.n_nodes;
+        }
+        return SC_OK;
+    }
     SC_CK(cudaStreamSynchronize(c.stream));
     c.mem.peak = c.mem.now;
     lattice_level0(c, *b, lat, alive, gone, loads);
@@ -750,29 +775,56 @@ sc_status sc_compliance_grad(sc_context* ctx, const sc_grid* g, const sc_options
 }
 
 sc_status sc_grid_apply(sc_context* ctx, const sc_grid* g, int32_t precision, const double* xin, double* yout) {
+    return sc_grid_apply_tile(ctx, g, precision, 0, xin, yout);
+}
+
+sc_status sc_grid_apply_tile(sc_context* ctx, const sc_grid* g, int32_t precision, int32_t tile, const double* xin,
+                             double* yout) {
     if (!g || !xin || !yout) return SC_BAD_INPUT;
     return guarded(ctx, [&] {
         Context& c = ctx->c;
         check_grid(*g);
+        sc_options o;
+        sc_default_options(&o);
+        o.tile = tile;
+        check_options(o);
         Batch b;
-        grid_level0(c, b, {*g}, false, 0);
+        grid_level0(c, b, {*g}, false, tile);
         const Level& L = b.levels[0];
         int64_t n6 = 6 * L.n;
         DBuf<double> x, y;
         x.alloc(n6, c.stream, &c.mem);
         y.alloc(n6, c.stream, &c.mem);
         x.upload(xin, n6);
+        if (b.grid.use_bricks) {  // the iterations' stencil: x into brick order, y back
+            bricks_build(c, b);
+            bricks_enter(c, b);
+            DBuf<double> xb;
+            xb.alloc(n6, c.stream, &c.mem);
+            brick_permute<double>(c, b, x.get(), xb.get(), true);
+            x = std::move(xb);
+        }
+        auto to_ref = [&](auto& v) {  // y from brick order into the reference's
+            if (!b.grid.use_bricks) return;
+            using V = typename std::remove_reference<decltype(*v.get())>::type;
+            DBuf<V> o;
+            o.alloc(n6, c.stream, &c.mem);
+            brick_permute<V>(c, b, v.get(), o.get(), false);
+            v = std::move(o);
+        };
         if (precision == SC_MIXED) {
             DBuf<float> xf, yf;
             to_float(c, x, xf);
             yf.alloc(n6, c.stream, &c.mem);
             stencil_apply<float>(c, b, xf.get(), yf.get(), nullptr, nullptr);
+            to_ref(yf);
             std::vector<float> h(n6);
             yf.download(h.data(), n6);
             SC_CK(cudaStreamSynchronize(c.stream));
             for (int64_t i = 0; i < n6; i++) yout[i] = h[i];
         } else {
             stencil_apply<double>(c, b, x.get(), y.get(), nullptr, nullptr);
+            to_ref(y);
             y.download(yout, n6);
             SC_CK(cudaStreamSynchronize(c.stream));
         }
@@ -834,6 +886,22 @@ sc_status sc_settle(sc_context* ctx, const sc_lattice* lat, const sc_strength* s
         require(str->m && (lat->n_bonds == 0 || (str->ft && str->fc && str->fs)), SC_BAD_INPUT,
                 "masses and strengths are required");
         solve_status = settle(ctx->c, *lat, *str, *opt, gone, out);
+    });
+    return s != SC_OK ? s : solve_status;
+}
+
+sc_status sc_as_generated(sc_context* ctx, const sc_lattice* lat, const sc_strength* str, const sc_lattice* gen,
+                          const sc_strength* gen_str, const sc_options* opt, double* ft, double* fc, double* fs) {
+    if (!lat || !str || !gen || !gen_str || !opt || (lat->n_bonds > 0 && (!ft || !fc || !fs))) return SC_BAD_INPUT;
+    sc_status solve_status = SC_OK;
+    sc_status s = guarded(ctx, [&] {
+        check_options(*opt);
+        check_lattice(*lat);
+        check_lattice(*gen);
+        require(lat->n_bonds == 0 || (str->ft && str->fc && str->fs), SC_BAD_INPUT, "strengths are required");
+        require(gen_str->m && (gen->n_bonds == 0 || (gen_str->ft && gen_str->fc && gen_str->fs)), SC_BAD_INPUT,
+                "the generated lattice's masses and strengths are required");
+        solve_status = as_generated(ctx->c, *lat, *str, *gen, *gen_str, *opt, ft, fc, fs);
     });
     return s != SC_OK ? s : solve_status;
 }

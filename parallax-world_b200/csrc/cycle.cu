@@ -285,15 +285,33 @@ __global__ void k_cg_beta_flex(int np, CgScalars s, const double* __restrict__ z
 // (the recursion drifted from b - K x by more than the tolerance) and is counted, so its
 // residual can be replaced by the true one. Pieces stopped by a breakdown or the cap keep
 // their status.
-__global__ void k_cg_verify(int np, CgScalars s, const double* __restrict__ rr_true, int32_t* __restrict__ count) {
+__global__ void k_cg_verify(int np, CgScalars s, const double* __restrict__ rr_true, const double* __restrict__ ff,
+                            int32_t* __restrict__ count) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np) return;
     if (!s.done[p] || s.status[p] != (int)SC_OK) return;
-    if (!(sqrt(rr_true[p]) <= s.goal[p])) {
+    // a piece at its FP64 floor (no FP64 x does better: see k_floor_delta) has met it too
+    if (!(sqrt(rr_true[p]) <= fmax(s.goal[p], sqrt(ff[p])))) {
         s.done[p] = 0;
         s.replaced[p] += 1;
         atomicAdd(count, 1);
     }
+}
+
+// delta = eps |x| sigma, sigma = +-1 from a hash of the index: x moved by one unit in the
+// last place of each value, in random directions. |K delta| is the residual that rounding
+// x to FP64 alone leaves, the floor no FP64 vector of motions gets under: on slender
+// pieces with large motions it is above 1e-8 |b| (the reference's own FP64 solve stops
+// there too), and the solve takes a piece that reached it as converged.
+__global__ void k_floor_delta(int64_t n, const double* __restrict__ x, double* __restrict__ delta) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    const double sgn = (h >> 63) ? -1.0 : 1.0;
+    delta[i] = sgn * 0x1.0p-52 * fabs(x[i]);
 }
 
 // The condition of the device-side iteration loop: go on while a piece is not done and
@@ -535,6 +553,24 @@ static cudaGraphExec_t capture_loop(cudaStream_t st, F&& fill, Context& ctx) {
     return exec;
 }
 
+// Per piece |K delta|^2 with delta = eps |x| sigma (k_floor_delta): the squared residual
+// that rounding x to FP64 leaves.
+static void residual_floor(Context& ctx, Batch& b, const double* x, double* ff) {
+    Level& L = b.levels[0];
+    const int64_t n6 = 6 * L.n;
+    DBuf<double> delta, kd;
+    delta.alloc(n6, ctx.stream, &ctx.mem);
+    kd.alloc(n6, ctx.stream, &ctx.mem);
+    k_floor_delta<<<grid_for(n6, 256), 256, 0, ctx.stream>>>(n6, x, delta.get());
+    SC_LAUNCH_CK();
+    if (L.matrix_free)
+        stencil_apply<double>(ctx, b, delta.get(), kd.get(), nullptr, nullptr);
+    else
+        spmv<double>(ctx, SPMV_Y, L.n, L.rowptr.get(), L.col.get(), L.val.get(), delta.get(), nullptr, kd.get(),
+                     nullptr, nullptr, L.piece.get(), nullptr, nullptr, L.nnzb);
+    dot2<double>(ctx, L, nullptr, kd.get(), kd.get(), ff, nullptr);
+}
+
 // Times a solve may replace the residuals of pieces whose true residual missed the goal.
 constexpr int MAX_REPLACEMENTS = 8;
 
@@ -627,10 +663,11 @@ static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p,
                   "the conjugate gradients' vectors and x are FP64");
     const double* rhs64 = rhs;
     int32_t* ndone_h = ctx.pinned_i32();
-    DBuf<double> res, rr_true;
+    DBuf<double> res, rr_true, ff;
     DBuf<int32_t> nrep;
     res.alloc(n6, st, &ctx.mem);
     rr_true.alloc(np, st, &ctx.mem);
+    ff.alloc(np, st, &ctx.mem);
     nrep.alloc(1, st, &ctx.mem);
     auto replace_residuals = [&]() -> bool {
         if (L.matrix_free)
@@ -639,8 +676,9 @@ static int64_t pcg(Context& ctx, Batch& b, const V* rhs, S* x, V* r, V* z, V* p,
             spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), x, rhs64, res.get(), nullptr,
                          nullptr, L.piece.get(), nullptr, nullptr, L.nnzb);
         dot2<double>(ctx, L, nullptr, res.get(), res.get(), rr_true.get(), nullptr);
+        residual_floor(ctx, b, x, ff.get());
         SC_CK(cudaMemsetAsync(nrep.get(), 0, sizeof(int32_t), st));
-        k_cg_verify<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, rr_true.get(), nrep.get());
+        k_cg_verify<<<grid_for(np, 128), 128, 0, st>>>(np, cg.s, rr_true.get(), ff.get(), nrep.get());
         SC_LAUNCH_CK();
         SC_CK(cudaMemcpyAsync(ndone_h, nrep.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         SC_CK(cudaStreamSynchronize(st));
@@ -759,13 +797,14 @@ static void count_loop_launches(int64_t per_iteration, const std::vector<int64_t
     g_launches.fetch_add(per_iteration * (most + 1));
 }
 
-// |b - K x| / |b| per piece, in FP64
-static void true_residual(Context& ctx, Batch& b, const double* x, std::vector<double>& out) {
+// |b - K x| / |b| per piece, in FP64, and the floor of that ratio rounding x to FP64
+// leaves (residual_floor)
+static void true_residual(Context& ctx, Batch& b, const double* x, SolveStats& st) {
     Level& L = b.levels[0];
     int np = b.npieces;
     DBuf<double> res, nr;
     res.alloc(6 * L.n, ctx.stream, &ctx.mem);
-    nr.alloc(2 * np, ctx.stream, &ctx.mem);
+    nr.alloc(3 * np, ctx.stream, &ctx.mem);
     if (L.matrix_free)
         stencil_residual<double>(ctx, b, x, b.loads.get(), res.get(), nullptr, nullptr);
     else
@@ -773,9 +812,14 @@ static void true_residual(Context& ctx, Batch& b, const double* x, std::vector<d
                      nullptr, nullptr, L.piece.get(), nullptr, nullptr, L.nnzb);
     dot2<double>(ctx, L, nullptr, res.get(), res.get(), nr.get(), nullptr);
     dot2<double>(ctx, L, nullptr, b.loads.get(), b.loads.get(), nr.get() + np, nullptr);
+    residual_floor(ctx, b, x, nr.get() + 2 * np);
     std::vector<double> h = nr.to_host();
-    out.resize(np);
-    for (int p = 0; p < np; p++) out[p] = h[np + p] > 0 ? std::sqrt(h[p] / h[np + p]) : 0.0;
+    st.residual.resize(np);
+    st.floor.resize(np);
+    for (int p = 0; p < np; p++) {
+        st.residual[p] = h[np + p] > 0 ? std::sqrt(h[p] / h[np + p]) : 0.0;
+        st.floor[p] = h[np + p] > 0 ? std::sqrt(h[2 * np + p] / h[np + p]) : 0.0;
+    }
 }
 
 void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& stats) {
@@ -799,7 +843,7 @@ void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, So
     count_loop_launches(per_it, it);
     stats.iterations = it;
     stats.refinements = cg.replaced.to_host();
-    true_residual(ctx, b, x.get(), stats.residual);
+    true_residual(ctx, b, x.get(), stats);
 }
 
 // ---- mixed precision --------------------------------------------------------------
@@ -924,7 +968,7 @@ void pcg_fp32_cycle(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>&
     count_loop_launches(per_it, it);
     stats.iterations = it;
     stats.refinements = cg.replaced.to_host();
-    true_residual(ctx, b, x.get(), stats.residual);
+    true_residual(ctx, b, x.get(), stats);
 }
 
 void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& stats) {
@@ -1093,7 +1137,7 @@ void pcg_mixed(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, S
     SC_CK(cudaStreamSynchronize(st));
     stats.iterations = it;
     stats.refinements = up;
-    true_residual(ctx, b, x.get(), stats.residual);
+    true_residual(ctx, b, x.get(), stats);
 }
 
 }  // namespace sc

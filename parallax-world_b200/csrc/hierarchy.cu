@@ -1362,6 +1362,25 @@ void to_float(Context& ctx, const DBuf<double>& a, DBuf<float>& b) {
 
 // Levels for every piece: while a piece has more than FEW parts and its bodies are fewer
 // than its parts, coarsen it (bodies.rs:444-461); then factor each piece's top.
+// A matrix-free level 0 keeps only what the solve reads: the assembled blocks, their
+// inverses and the explicit prolongator serve the setup alone.
+static void release_level0_setup(Batch& b) {
+    if (!b.levels[0].matrix_free || b.levels.size() < 2) return;
+    Level& L0 = b.levels[0];
+    L0.val.release();
+    L0.desc.release();
+    b.grid.tpl_s.release();
+    L0.col.release();
+    L0.rowptr.release();
+    L0.inv.release();
+    L0.pval.release();
+    L0.pcol.release();
+    L0.prow.release();
+    L0.tptr.release();
+    L0.tent.release();
+    L0.trow.release();
+}
+
 void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
     auto t0 = std::chrono::steady_clock::now();
     PhaseTimer pt(ctx);
@@ -1397,26 +1416,26 @@ void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
         }
         build_top(ctx, b, l, tops);
         pt.mark("tops");
+        // Level l is finished: the levels above it are made from their own operators. Its
+        // setup-only arrays go now rather than at the end, so the next products run with
+        // less memory held. Under SC_MIXED the V-cycle reads a coarse level's operator,
+        // inverses and transfers in FP32 only (the FP64 conjugate gradients read level 0
+        // alone), so a coarse level keeps just those.
+        if (l == 0) release_level0_setup(b);
+        if (l >= 1 && opt.precision == SC_MIXED) {
+            Level& D = b.levels[l];
+            to_float(ctx, D.val, D.val32);
+            to_float(ctx, D.inv, D.inv32);
+            if (D.pval.size()) to_float(ctx, D.pval, D.pval32);
+            if (D.ptval.size()) to_float(ctx, D.ptval, D.ptval32);
+            D.val.release();
+            D.inv.release();
+            D.pval.release();
+            D.ptval.release();
+        }
+        pt.mark("release");
         if (!more) break;
     }
-    // a matrix-free level 0 keeps only what the solve reads: the assembled blocks, their
-    // inverses and the explicit prolongator served the setup alone
-    if (b.levels[0].matrix_free && b.levels.size() > 1) {
-        Level& L0 = b.levels[0];
-        L0.val.release();
-        L0.desc.release();
-        b.grid.tpl_s.release();
-        L0.col.release();
-        L0.rowptr.release();
-        L0.inv.release();
-        L0.pval.release();
-        L0.pcol.release();
-        L0.prow.release();
-        L0.tptr.release();
-        L0.tent.release();
-        L0.trow.release();
-    }
-    pt.mark("release level 0");
     b.piece_levels.assign(np, 0);
     for (size_t l = 0; l < b.levels.size(); l++)
         for (int p = 0; p < np; p++)

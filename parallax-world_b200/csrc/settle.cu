@@ -7,6 +7,9 @@
 // forces of the motions (moved, bodies.rs:420-423, Bond::force, model.rs:115-119), their
 // use of the bond's strength (Bond::used / Mat::used, model.rs:66-68, 123-129) and the
 // breaking of whole beams -- runs in the kernels below.
+#include <algorithm>
+#include <array>
+#include <cmath>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -265,6 +268,54 @@ sc_status settle(Context& c, const sc_lattice& L, const sc_strength& S, const sc
         out->status = worst;
     }
     return worst;
+}
+
+
+// statics::bodies::as_generated (bodies.rs:611-625): for every beam of `generated` (its
+// bonds keyed by the cells their two ends lie between, the lesser end first), the most
+// of its strength any of its bonds uses standing; each bond of `lattice` on the same beam
+// made max(MARGIN * that, 1) times as strong (Mat::stronger, model.rs:71-73), the others
+// unchanged. The used fractions are the device's (used_standing); the matching is host
+// work, as the reference's is: both bond lists keyed and sorted, then merged.
+sc_status as_generated(Context& c, const sc_lattice& L, const sc_strength& S, const sc_lattice& G,
+                       const sc_strength& GS, const sc_options& opt, double* ft, double* fc, double* fs) {
+    constexpr double MARGIN = 2.0;  // bodies.rs:605
+    std::vector<double> used((size_t)std::max<int64_t>(G.n_bonds, 1));
+    sc_solve_info info;
+    sc_status s = used_standing(c, G, GS, opt, used.data(), &info);
+    using Key = std::array<int64_t, 12>;
+    auto key_of = [](const sc_lattice& l, int64_t b) {
+        const int64_t* i = l.around + 6 * l.bond_i[b];
+        const int64_t* j = l.around + 6 * l.bond_j[b];
+        Key k;
+        const bool swap = !std::lexicographical_compare(i, i + 6, j, j + 6);  // i < j keeps the order
+        const int64_t* a = swap ? j : i;
+        const int64_t* z = swap ? i : j;
+        std::copy(a, a + 6, k.begin());
+        std::copy(z, z + 6, k.begin() + 6);
+        return k;
+    };
+    // the generated beams' need: the most any of their bonds uses (f64::max, NaN ignored)
+    std::vector<std::pair<Key, double>> need((size_t)G.n_bonds);
+    for (int64_t b = 0; b < G.n_bonds; b++) need[b] = {key_of(G, b), used[b]};
+    std::stable_sort(need.begin(), need.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    std::vector<std::pair<Key, double>> beams;
+    for (auto& kv : need) {
+        if (beams.empty() || beams.back().first != kv.first)
+            beams.push_back({kv.first, std::fmax(0.0, kv.second)});
+        else
+            beams.back().second = std::fmax(beams.back().second, kv.second);
+    }
+    for (int64_t b = 0; b < L.n_bonds; b++) {
+        const Key k = key_of(L, b);
+        auto it = std::lower_bound(beams.begin(), beams.end(), k,
+                                   [](const auto& x, const Key& y) { return x.first < y; });
+        const double by = (it != beams.end() && it->first == k) ? std::fmax(it->second * MARGIN, 1.0) : 1.0;
+        ft[b] = S.ft[b] * by;
+        fc[b] = S.fc[b] * by;
+        fs[b] = S.fs[b] * by;
+    }
+    return s;
 }
 
 }  // namespace sc

@@ -20,6 +20,23 @@ namespace sc {
 
 constexpr int CHUNK = 4096;  // parts per reduction chunk (chunks never cross pieces)
 
+// Level 0 of voxel pieces in brick order (brick.cu): the layout of the iterations.
+struct Bricks {
+    int32_t n_bricks = 0;
+    bool active = false;        // the batch's level-0 vectors and transfer arrays are in brick order
+    DBuf<int32_t> start;        // n_bricks + 1: each brick's first part (brick order)
+    DBuf<uint32_t> mask;        // per brick: one bit per slot, set where the slot holds a part
+    DBuf<uint16_t> pre;         // per brick and mask word: parts in the words before it
+    DBuf<int4> info;            // per brick: piece, brick coordinates
+    DBuf<int32_t> nbr;          // per brick: the 13 bricks its stencil reads from (-1 none)
+    DBuf<float> kd;             // per brick: each cell's k (0 where not free)
+    DBuf<uint8_t> geo;          // per piece: dimensions, brick grid, first cell and brick
+    DBuf<uint8_t> box;          // where each entry of a brick's shared-memory box comes from
+    DBuf<int32_t> ref_of_bo;    // brick-ordered part -> the reference's part index
+    DBuf<int32_t> bo_of_ref;    // and back
+    DBuf<float2> kk;            // per brick-ordered part: its cells' k, its axis in their signs
+};
+
 // Level 0 of voxel pieces: the cells, and for each part its two cells.
 struct Grid0 {
     int64_t ncells = 0;
@@ -42,6 +59,9 @@ struct Grid0 {
     DBuf<int64_t> cell_flat;    // per free cell: its flat index in the batch's concatenated grids
     DBuf<double> tpl_s;         // the cell template at spacing s, 36 x 36 (setup only)
     std::vector<int64_t> grid_off;  // per piece: first flat cell index; npieces + 1
+    std::vector<int32_t> dims_h;    // per piece: nx, ny, nz
+    bool use_bricks = false;        // the iterations run in brick order (sc_options.tile 0)
+    Bricks bricks;
 };
 
 struct Level {
@@ -139,6 +159,19 @@ void level0_up(Context& ctx, const Batch& b, const T* r, T* x, T* e, const T* zc
 template <class T>
 void level0_smooth(Context& ctx, const Batch& b, const T* r, const T* x, T* z, const int32_t* done);
 
+// --- brick.cu -------------------------------------------------------------------------
+void bricks_build(Context& ctx, Batch& b);
+void bricks_enter(Context& ctx, Batch& b);
+void bricks_leave(Context& ctx, Batch& b, DBuf<double>* x);
+template <class T>
+void brick_permute(Context& ctx, const Batch& b, const T* in, T* out, bool to_bricks);
+template <class T, int MODE>
+void brick_stencil(Context& ctx, const Batch& b, const T* x, const T* r, T* y, T* y2, const double* step,
+                   const int32_t* skip_row, const int32_t* done);
+template <class T>
+void brick_jacobi(Context& ctx, const Batch& b, const T* r, T* x, const double* step, const int32_t* skip_row,
+                  const int32_t* done);
+
 // --- lattice.cu -----------------------------------------------------------------------
 void lattice_level0(Context& ctx, Batch& b, const sc_lattice& L, const uint8_t* alive, const uint8_t* gone,
                     const double* loads);
@@ -180,6 +213,8 @@ sc_status used_standing(Context& ctx, const sc_lattice& L, const sc_strength& S,
                         double* used, sc_solve_info* info);
 sc_status settle(Context& ctx, const sc_lattice& L, const sc_strength& S, const sc_options& opt, uint8_t* gone,
                  sc_settle_info* out);
+sc_status as_generated(Context& ctx, const sc_lattice& L, const sc_strength& S, const sc_lattice& G,
+                       const sc_strength& GS, const sc_options& opt, double* ft, double* fc, double* fs);
 
 // --- hierarchy.cu ---------------------------------------------------------------------
 void setup_chunks(Context& ctx, Level& L, int32_t npieces);
@@ -192,6 +227,7 @@ struct SolveStats {
     std::vector<int64_t> iterations;
     std::vector<int64_t> refinements;
     std::vector<double> residual;
+    std::vector<double> floor;  // per piece: the relative residual rounding x to FP64 leaves
     double work = 0;
 };
 void pcg_fp64(Context& ctx, Batch& b, const sc_options& opt, DBuf<double>& x, SolveStats& st);

@@ -55,14 +55,15 @@ class SolveInfo(C.Structure):
                 ("status", C.c_int32), ("parts", C.c_int64 * MAX_LEVELS), ("blocks", C.c_int64 * MAX_LEVELS),
                 ("steps", C.c_double * MAX_LEVELS), ("residual", C.c_double), ("work", C.c_double),
                 ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("n_nodes", C.c_int64),
-                ("n_parts", C.c_int64), ("peak_bytes", C.c_int64)]
+                ("n_parts", C.c_int64), ("peak_bytes", C.c_int64), ("residual_floor", C.c_double)]
 
     def as_dict(self) -> dict:
         nl = self.levels
         return dict(iterations=self.iterations, refinements=self.refinements, levels=nl, status=self.status,
                     parts=list(self.parts[:nl]), blocks=list(self.blocks[:nl]), steps=list(self.steps[:nl]),
                     residual=self.residual, work=self.work, setup_ms=self.setup_ms, solve_ms=self.solve_ms,
-                    n_nodes=self.n_nodes, n_parts=self.n_parts, peak_bytes=self.peak_bytes)
+                    n_nodes=self.n_nodes, n_parts=self.n_parts, peak_bytes=self.peak_bytes,
+                    residual_floor=self.residual_floor)
 
 
 class Grid(C.Structure):
@@ -114,6 +115,7 @@ def lib():
         L.sc_compliance_grad.argtypes = [P, C.POINTER(Grid), C.POINTER(Options), C.POINTER(C.c_double), P, P,
                                          C.c_int64, C.POINTER(SolveInfo)]
         L.sc_grid_apply.argtypes = [P, C.POINTER(Grid), C.c_int32, P, P]
+        L.sc_grid_apply_tile.argtypes = [P, C.POINTER(Grid), C.c_int32, C.c_int32, P, P]
         L.sc_last_up.argtypes = [P, C.c_int32, P, C.c_int64]
         L.sc_motions.argtypes = [P, C.POINTER(LatticeC), P, P, P, C.POINTER(Options), P, C.POINTER(SolveInfo)]
         L.sc_profile.argtypes = [P, C.c_uint32]
@@ -139,12 +141,16 @@ def lib():
                                        C.POINTER(SolveInfo)]
         L.sc_settle.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
                                 C.POINTER(SettleInfo)]
+        L.sc_as_generated.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(LatticeC),
+                                      C.POINTER(Strength), C.POINTER(Options), P, P, P]
+        L.sc_as_generated.restype = C.c_int
         L.sc_compliance_noalloc.argtypes = [P, P, C.c_int64, P, P]
         L.sc_compliance_noalloc.restype = C.c_int
         for name in ("sc_profile", "sc_profile_read", "sc_context_stream"):
             getattr(L, name).restype = C.c_int
         for name in ("sc_create", "sc_generate_piece", "sc_grid_count", "sc_solve_grid", "sc_solve_grid_batch",
-                     "sc_compliance_grad", "sc_grid_apply", "sc_last_up", "sc_motions", "sc_used_standing",
+                     "sc_compliance_grad", "sc_grid_apply", "sc_grid_apply_tile", "sc_last_up", "sc_motions",
+                     "sc_used_standing",
                      "sc_settle"):
             getattr(L, name).restype = C.c_int
         _lib = L
@@ -466,15 +472,16 @@ class Solver:
         self._check(s, "sc_compliance_grad")
         return comp.value, grad, mot[:n_nodes], info.as_dict()
 
-    def grid_apply(self, state, k, x_parts: np.ndarray, precision=FP64) -> np.ndarray:
-        """Level 0's operator y = K x over the free nodes (n_parts x 6)."""
+    def grid_apply(self, state, k, x_parts: np.ndarray, precision=FP64, tile: int = 0) -> np.ndarray:
+        """Level 0's operator y = K x over the free nodes (n_parts x 6, part order), by the
+        stencil `tile` selects (0: the brick stencil the iterations use)."""
         state = np.ascontiguousarray(state, np.uint8)
         k = np.ascontiguousarray(k, np.float32)
         g = make_grid(state, k)
         x = np.ascontiguousarray(x_parts, np.float64)
         y = np.zeros_like(x)
-        s = lib().sc_grid_apply(self.h, C.byref(g), precision, _ptr(x), _ptr(y))
-        self._check(s, "sc_grid_apply", soft=(OK,))
+        s = lib().sc_grid_apply_tile(self.h, C.byref(g), precision, tile, _ptr(x), _ptr(y))
+        self._check(s, "sc_grid_apply_tile", soft=(OK,))
         return y
 
     def last_up(self, level: int, n_parts: int) -> np.ndarray:
@@ -520,6 +527,23 @@ class Solver:
                                    C.byref(info))
         self._check(s, "sc_used_standing", soft=(OK, MAXITER))
         return used[:L.n_bonds], info.as_dict()
+
+    def as_generated(self, lattice: dict, generated: dict, opt: Options | None = None) -> dict:
+        """statics::bodies::as_generated (bodies.rs:611-625): `lattice` with each bond's
+        strengths (ft, fc, fs) made what its world as generated (`generated`, a lattice
+        dict with m, ft, fc, fs) needs, twice. Returns a new dict; the inputs are kept."""
+        L, arr = _lattice_c(lattice)
+        S, keep = _strength_c(lattice)
+        G, garr = _lattice_c(generated)
+        GS, gkeep = _strength_c(generated)
+        nb = max(L.n_bonds, 1)
+        ft, fc, fs = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+        s = lib().sc_as_generated(self.h, C.byref(L), C.byref(S), C.byref(G), C.byref(GS),
+                                  C.byref(opt or options()), _ptr(ft), _ptr(fc), _ptr(fs))
+        self._check(s, "sc_as_generated", soft=(OK, MAXITER))
+        out = dict(lattice)
+        out.update(ft=ft[:L.n_bonds], fc=fc[:L.n_bonds], fs=fs[:L.n_bonds])
+        return out
 
     def settle(self, lattice: dict, opt: Options | None = None):
         """statics::bodies::settle (bodies.rs:511-541): (fallen fraction of the free mass,

@@ -7,8 +7,9 @@ setting, each as slow as its worst member. So the tuner times a batched solve (s
 PCG to the requested tolerance, as the batch will run) of a sample of the batch -- up to
 SAMPLES pieces spread evenly over its size range -- under every candidate setting:
 block-Jacobi sweeps before and after each coarse correction (the reference does one,
-statics/src/bodies.rs:386, 396-401) and the stencil tile (the window of parts grouped by
-axis). It keeps the fastest setting that solved every sample: two sweeps per level cut
+statics/src/bodies.rs:386, 396-401) and the level-0 stencil (sc_options.tile: 0 the
+brick stencil, whose iterations run in brick order, or the per-part stencil in the
+reference's part order with a window of 1024 parts grouped by axis). It keeps the fastest setting that solved every sample: two sweeps per level cut
 the mean iteration count but can leave a straggler (the damped-Jacobi step 4/(3
 lambda_max) is the reference's choice for one sweep; on some pieces two sweeps lose
 definiteness and CG stalls), so a setting counts only if all its samples converge within
@@ -27,7 +28,7 @@ import time
 from . import FP64, MIXED, Solver, options
 
 SWEEPS = (1, 2)
-TILES = (256, 1024, 4096)
+TILES = (0, 1024)  # the brick stencil (brick order), the per-part stencil (the reference's order)
 SAMPLES = 32
 TRIAL_MAX_ITER = 2000
 MAX_ITER = 20000
@@ -37,9 +38,16 @@ DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotu
 
 def converged(info: dict, tol: float) -> bool:
     """The solve met its criterion: status OK and its true residual |b - K x| / |b|,
-    recomputed in FP64, at most tol (up to the rounding of that ratio). The solver holds
-    every piece to this, replacing a drifted recursive residual by the true one."""
-    return info["status"] == 0 and info["residual"] <= tol * (1.0 + 1e-9)
+    recomputed in FP64, at most tol (up to the rounding of that ratio), or at most the
+    piece's FP64 floor (info["residual_floor"]: the residual rounding x to FP64 leaves,
+    which no FP64 vector of motions gets under). The solver holds every piece to this,
+    replacing a drifted recursive residual by the true one."""
+    return info["status"] == 0 and info["residual"] <= max(tol, info.get("residual_floor", 0.0)) * (1.0 + 1e-9)
+
+
+def above_tol_at_floor(info: dict, tol: float) -> bool:
+    """Converged at its FP64 floor, which lies above tol."""
+    return converged(info, tol) and info["residual"] > tol * (1.0 + 1e-9)
 
 
 def size_class(state) -> int:

@@ -139,3 +139,37 @@ def test_golden_fixtures():
         assert np.linalg.norm(u) == pytest.approx(c["u_norm"], rel=1e-12)
         idx = np.asarray(c["sample_idx"])
         assert np.allclose(u.ravel()[idx], c["sample_u"], rtol=1e-10, atol=1e-14 * c["u_norm"])
+
+
+def _edits_golden():
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_edits.json")
+    return json.load(open(path))
+
+
+def _verdict(fallen):
+    if fallen == 0.0:
+        return "stands"
+    if 0.35 <= fallen <= 0.45:
+        return "two fifths fall"
+    return "falls"
+
+
+def test_edits_verdicts_match_the_docs():
+    """The reference's per-level verdicts of its edits experiment (docs/statics.md:236-247,
+    made by exp_edits, statics/examples/statics.rs:310-344), from the oracle's recorded run
+    of the same chain (gather, as_generated, settle) at levels 0-4."""
+    for case in _edits_golden():
+        got = [_verdict(lv["fallen"][1]) for lv in case["levels"]]
+        assert got == case["docs"], case["name"]
+
+
+@pytest.mark.parametrize("name", ["cantilever 6 m", "block hanging let go"])
+def test_edits_golden_is_the_oracles(name):
+    """The recorded chain is the oracle's: the cheap cases run again here."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_edits_golden as M
+    want = next(c for c in _edits_golden() if c["name"] == name)
+    got = M.run(name)
+    for a, b in zip(got["levels"], want["levels"]):
+        assert a["fallen"] == b["fallen"] and a["rounds"] == b["rounds"] and a["gone_hash"] == b["gone_hash"]
