@@ -12,15 +12,17 @@
 // order (z fastest), pieces in order, so every piece keeps its range of part indices and
 // the chunked dot products and axpys are unchanged.
 //
-// The stencil gives each brick one thread block. The block reads the x of every face
-// its parts' two cells touch -- its own parts, a contiguous run, and the halo faces of
-// twelve neighbour bricks -- into a dense box in shared memory, together with the k of
-// its cells and of the one-cell layers on its -x, -y and -z sides; then each thread
-// takes a part (in storage order, so its epilogue's loads and stores are contiguous)
-// and adds the strips of its lesser and greater cell's 36x36 template rows (the same
-// per-cell matrix k s D Kt D as grid.cu's stencil) from the box. Which faces are parts
-// and where a brick's part sits in its run come from a bit mask per brick (one bit a
-// slot) and popcounts; no per-part record is read.
+// The stencil gives each brick one thread block. The block copies into a dense box in
+// shared memory the x of every face its parts' two cells touch, with asynchronous copies
+// (cp.async, global to shared memory without registers, all issued, then awaited once):
+// its own parts, a contiguous run read in order and placed by each part's 16-bit code
+// (axis and brick-local position), and its halo, a list of (box entry, part) pairs
+// resolved once per solve from the twelve neighbour bricks' slot masks (bricks_build).
+// The k of its cells and of the one-cell layers on its -x, -y and -z sides come the same
+// way. Then each thread takes a part (in storage order, so its epilogue's loads and
+// stores are contiguous) and adds the strips of its lesser and greater cell's rows of
+// the level-0 cell matrix k s D T D (the template with the spacing folded into its
+// constants, BlkS, so the box holds the motions as they are).
 //
 // The reference's order stays the order of everything else: the hierarchy is built in
 // it (so the bit-exact parity holds), the caller's loads come in and the motions go out
@@ -50,8 +52,10 @@ constexpr int XB0 = (BX + 2) * (BY + 1) * (BZ + 1), XB1 = (BX + 1) * (BY + 2) * 
 constexpr int NBOX = XB0 + XB1 + XB2;
 constexpr int KB = (BX + 1) * (BY + 1) * (BZ + 1);  // cells lo-1 .. hi-1
 constexpr int NNB = 13;                             // the brick and the twelve it reads from
+constexpr int HKX = BY * BZ, HKY = BX * BZ, HKZ = BX * BY, HK = HKX + HKY + HKZ;  // halo cells
 constexpr int BRICK_THREADS = 256;
-static_assert(NSLOT < 4096, "slot indices take 12 bits (box_table)");
+static_assert(NSLOT < 4096, "slot indices take 12 bits (halo_table)");
+static_assert(BRICK_THREADS == BCELLS, "the k box is filled a cell a thread");
 
 // The bricks a brick reads from, as offsets in brick units: itself, its six face
 // neighbours, and the six edge neighbours one step back along one axis and one step
@@ -108,7 +112,11 @@ struct BrickView {
     const int32_t* nbr;    // NNB a brick: the bricks of NB_OFF_H, -1 where none
     const float* kd;       // BCELLS a brick: each cell's k, 0 where not free
     const BrickGeo* geo;   // per piece
-    const uint4* box;      // NBOX: where each box entry comes from (box_table)
+    const uint16_t* code;  // per part (brick order): its part_code
+    const int32_t* hstart; // n_bricks + 1: each brick's halo list
+    const uint16_t* hent;  // per halo item: the box entry it fills
+    const int32_t* hsrc;   // per halo item: the part (brick order) it comes from
+    const float* hk;       // per brick, HK values: the k of the cells of its -x, -y, -z layers
 };
 
 // A part's slot as the part phase reads it: axis (bits 12-13), brick-local face position
@@ -118,15 +126,17 @@ __host__ __device__ constexpr uint32_t part_code(int a, int l0, int l1, int l2) 
 }
 static_assert(BX + 1 < 8 && BY + 1 < 16 && BZ + 1 < 16, "part_code fields");
 
-// Where each entry of a brick's box comes from, the same for every brick: entry i is the
-// face of axis a at brick-local position c. x: bit 31 the entry is read by some part;
-// bits 27-30 the brick (index into NB_OFF) holding it and bits 0-11 its slot there;
-// bits 25-26 the axis a; bit 24 the entry lies on the + plane of axis a, where it belongs
-// to the next brick along a, or, for a brick at the piece's + end along a, to the brick's
-// own plane of extra slots: y then holds that brick index (bits 27-30) and slot (0-11).
-// z and w: the part_code of the entry as the brick's own part (x's and y's case).
-std::vector<uint4> box_table() {
-    std::vector<uint4> t(NBOX);
+// The entries of a brick's box that other bricks hold, the same for every brick (the
+// brick's own parts go to the box straight from their run, by their part_code). Entry i
+// is the face of axis a at brick-local position c, read by some part. x: bits 27-30 the
+// brick (index into NB_OFF) holding it and bits 0-11 its slot there; bits 25-26 the
+// axis a; bits 12-23 the entry i; bit 24 the entry lies on the + plane of axis a, where
+// it belongs to the next brick along a -- or, for bricks at the piece's + end along a,
+// to the plane of extra slots of the brick one step back from there (y: that brick,
+// bits 27-30, and slot, bits 0-11; brick 0 is the brick itself, whose own parts are
+// filled as those are).
+std::vector<uint2> halo_table() {
+    std::vector<uint2> t;
     constexpr CodeTable code = make_code_table();
     const int B[3] = {BX, BY, BZ};
     for (int i = 0; i < NBOX; i++) {
@@ -134,32 +144,29 @@ std::vector<uint4> box_table() {
         const int rem = i - box_off(a);
         const int e2 = box_ext(a, 2), e1 = box_ext(a, 1);
         const int c[3] = {rem / (e2 * e1) - 1, rem / e2 % e1 - 1, rem % e2 - 1};
-        uint32_t x = 0, y = 0, z = 0, w = 0;
-        if ((c[0] < 0) + (c[1] < 0) + (c[2] < 0) <= 1) {
-            int o[3], l[3], oa[3], la[3];
-            for (int d = 0; d < 3; d++) {
-                if (c[d] < 0) {
-                    o[d] = oa[d] = -1;
-                    l[d] = la[d] = B[d] - 1;
-                } else if (c[d] >= B[d]) {  // only along a
-                    o[d] = 1;
-                    l[d] = 0;
-                    oa[d] = 0;
-                    la[d] = B[d];
-                } else {
-                    o[d] = oa[d] = 0;
-                    l[d] = la[d] = c[d];
-                }
+        if ((c[0] < 0) + (c[1] < 0) + (c[2] < 0) > 1) continue;  // read by no part
+        int o[3], l[3], oa[3], la[3];
+        for (int d = 0; d < 3; d++) {
+            if (c[d] < 0) {
+                o[d] = oa[d] = -1;
+                l[d] = la[d] = B[d] - 1;
+            } else if (c[d] >= B[d]) {  // only along a
+                o[d] = 1;
+                l[d] = 0;
+                oa[d] = 0;
+                la[d] = B[d];
+            } else {
+                o[d] = oa[d] = 0;
+                l[d] = la[d] = c[d];
             }
-            const int q = code.v[(o[0] + 1) * 9 + (o[1] + 1) * 3 + (o[2] + 1)];
-            const int qa = code.v[(oa[0] + 1) * 9 + (oa[1] + 1) * 3 + (oa[2] + 1)];
-            x = (1u << 31) | ((uint32_t)q << 27) | ((uint32_t)a << 25) | ((c[a] >= B[a] ? 1u : 0u) << 24) |
-                (uint32_t)slot_of(a, l[0], l[1], l[2]);
-            y = ((uint32_t)qa << 27) | (uint32_t)slot_of(a, la[0], la[1], la[2]);
-            z = part_code(a, l[0], l[1], l[2]);
-            w = part_code(a, la[0], la[1], la[2]);
         }
-        t[i] = make_uint4(x, y, z, w);
+        const int q = code.v[(o[0] + 1) * 9 + (o[1] + 1) * 3 + (o[2] + 1)];
+        const int qa = code.v[(oa[0] + 1) * 9 + (oa[1] + 1) * 3 + (oa[2] + 1)];
+        if (q == 0) continue;  // an own slot
+        const bool plane = c[a] >= B[a];
+        t.push_back(make_uint2(((uint32_t)q << 27) | ((uint32_t)a << 25) | ((plane ? 1u : 0u) << 24) |
+                                   ((uint32_t)i << 12) | (uint32_t)slot_of(a, l[0], l[1], l[2]),
+                               ((uint32_t)qa << 27) | (uint32_t)slot_of(a, la[0], la[1], la[2])));
     }
     return t;
 }
@@ -360,8 +367,17 @@ __device__ __forceinline__ void sts6(T* __restrict__ box, int e, const T (&o)[6]
     }
 }
 
-// acc += kc * (row strip SLOT of the cell template) * (the six faces of cell c, from the
-// box, which holds each face's rotations already times the spacing)
+// t += (row strip SLOT of the level-0 cell template k s D T D, spacing baked in: BlkS) *
+// (the six faces of cell c, from the box)
+template <int SLOT, int F, class T>
+__device__ __forceinline__ void face_macs_s(const T (&xs)[6][6], T (&t)[6]) {
+    if constexpr (F < 6) {
+        BlkS<SLOT, F>::mac(xs[F], t);
+        face_macs_s<SLOT, F + 1, T>(xs, t);
+    }
+}
+
+// acc += kc * (row strip SLOT of the cell matrix) * (the six faces of cell c)
 template <int SLOT, class T>
 __device__ __forceinline__ void box_term(const T* __restrict__ box, int c0, int c1, int c2, T kc, T (&acc)[6]) {
     T xs[6][6];
@@ -372,20 +388,9 @@ __device__ __forceinline__ void box_term(const T* __restrict__ box, int c0, int 
     lds6<T>(box, box_index(2, c0, c1, c2), xs[4]);
     lds6<T>(box, box_index(2, c0, c1, c2 + 1), xs[5]);
     T t[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    face_macs<SLOT, 0, T>(xs, t);
+    face_macs_s<SLOT, 0, T>(xs, t);
 #pragma unroll
     for (int i = 0; i < 6; i++) acc[i] = fma(kc, t[i], acc[i]);
-}
-
-// a part's own x from the box (its rotations back over the spacing, a power of two, so
-// exactly)
-template <class T>
-__device__ __forceinline__ void own_x(const T* __restrict__ box, int e, T s, T (&o)[6]) {
-    lds6<T>(box, e, o);
-    const T is = T(1) / s;
-    o[3] *= is;
-    o[4] *= is;
-    o[5] *= is;
 }
 
 // one part on axis AX at brick-local face position l: Kx from its lesser cell (l - e_AX,
@@ -401,7 +406,7 @@ __device__ __forceinline__ void brick_part(const T* __restrict__ box, const floa
     T acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
     if (kL != T(0)) box_term<2 * AX + 1, T>(box, l0 - (AX == 0), l1 - (AX == 1), l2 - (AX == 2), kL, acc);
     if (kG != T(0)) box_term<2 * AX, T>(box, l0, l1, l2, kG, acc);
-    const T kx[6] = {acc[0] * s, acc[1] * s, acc[2] * s, acc[3] * s * s, acc[4] * s * s, acc[5] * s * s};
+    const T(&kx)[6] = acc;
     T o[6];
     if constexpr (MODE == ST_Y) {
         store6<T>(y, q, kx);
@@ -426,7 +431,7 @@ __device__ __forceinline__ void brick_part(const T* __restrict__ box, const floa
     } else if constexpr (MODE == ST_PROLONG) {
         T d[6], xv[6], acc2[6];
         dinv<AX, T>(kL, kG, s, kx, d);
-        own_x<T>(box, box_index(AX, l0, l1, l2), s, xv);
+        lds6<T>(box, box_index(AX, l0, l1, l2), xv);
         load6<T>(y, q, acc2);
 #pragma unroll
         for (int j = 0; j < 6; j++) o[j] = acc2[j] + fma(-w, d[j], xv[j]);
@@ -437,25 +442,64 @@ __device__ __forceinline__ void brick_part(const T* __restrict__ box, const floa
 #pragma unroll
         for (int j = 0; j < 6; j++) rv[j] -= kx[j];
         dinv<AX, T>(kL, kG, s, rv, d);
-        own_x<T>(box, box_index(AX, l0, l1, l2), s, xv);
+        lds6<T>(box, box_index(AX, l0, l1, l2), xv);
 #pragma unroll
         for (int j = 0; j < 6; j++) o[j] = fma(w, d[j], xv[j]);
         store6<T>(y, q, o);
     }
 }
 
-// Shared memory of one brick: the x box (NBOX faces, 6 values each), the k box, the
-// brick's parts' part_codes in storage order, the 13 bricks' masks and prefix counts.
+// cp.async: an asynchronous copy of 8 or 16 bytes from global to shared memory
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// one part's six values into the box: 16-byte copies for FP64 where x is 16-byte aligned
+// (a part is 48 bytes), else 8-byte ones (FP32 parts are 24 bytes)
+template <class T>
+__device__ __forceinline__ void copy_part(T* dst, const T* src, bool vec16) {
+    if (sizeof(T) == 8 && vec16) {
+        cp_async16(dst, src);
+        cp_async16(dst + 2, src + 2);
+        cp_async16(dst + 4, src + 4);
+    } else {
+        constexpr int STEP = 8 / sizeof(T);
+#pragma unroll
+        for (int j = 0; j < 6; j += STEP) cp_async8(dst + j, src + j);
+    }
+}
+
+// Shared memory of one brick: the x box (NBOX faces, 6 values each), the k box and the
+// brick's parts' part_codes in storage order.
 template <class T>
 constexpr size_t brick_smem() {
-    return sizeof(T) * 6 * NBOX + sizeof(float) * KB + sizeof(uint32_t) * NSLOT + sizeof(uint32_t) * NNB * MW +
-           sizeof(uint16_t) * NNB * MW;
+    return sizeof(T) * 6 * NBOX + sizeof(float) * KB + sizeof(uint16_t) * (NSLOT + 8);
+}
+
+// the box entry of an own part's face, from its part_code
+__device__ __forceinline__ int own_entry(uint32_t c) {
+    const int a = (c >> 12) & 3, l0 = (c >> 8) & 7, l1 = (c >> 4) & 15, l2 = c & 15;
+    return a == 0 ? box_index(0, l0, l1, l2) : a == 1 ? box_index(1, l0, l1, l2) : box_index(2, l0, l1, l2);
+}
+
+// Resident blocks an SM the register cap aims at: five in FP32 (shared memory allows
+// five), four where the epilogue applies the block-Jacobi factor (more registers, which
+// five blocks would spill), three in FP64 (shared memory allows three).
+template <class T, int MODE>
+constexpr int brick_min_blocks() {
+    return sizeof(T) == 8 ? 3 : (MODE == ST_RES_JAC || MODE == ST_PROLONG || MODE == ST_SMOOTH) ? 4 : 5;
 }
 
 // Level 0 applied over bricks, one thread block a brick (see the file's head). The same
 // epilogues as grid.cu's k_stencil: y = Kx, r - Kx, ... (ST_* in level0.cuh).
 template <class T, int MODE>
-__global__ void __launch_bounds__(BRICK_THREADS, sizeof(T) == 4 ? 4 : 3) k_brick_stencil(BrickView v, const T* __restrict__ x,
+__global__ void __launch_bounds__(BRICK_THREADS, brick_min_blocks<T, MODE>()) k_brick_stencil(BrickView v, const T* __restrict__ x,
                                                                  const T* __restrict__ r, T* __restrict__ y,
                                                                  T* __restrict__ y2, T s,
                                                                  const double* __restrict__ step,
@@ -464,87 +508,53 @@ __global__ void __launch_bounds__(BRICK_THREADS, sizeof(T) == 4 ? 4 : 3) k_brick
     extern __shared__ __align__(16) unsigned char brick_sm[];
     T* box = reinterpret_cast<T*>(brick_sm);
     float* kbox = reinterpret_cast<float*>(box + 6 * NBOX);
-    uint32_t* codes = reinterpret_cast<uint32_t*>(kbox + KB);
-    uint32_t* nmask = codes + NSLOT;
-    uint16_t* npre = reinterpret_cast<uint16_t*>(nmask + NNB * MW);
-    __shared__ int32_t nid[NNB], nstart[NNB];
+    uint16_t* codes = reinterpret_cast<uint16_t*>(kbox + KB);
     const int b = blockIdx.x;
     const int4 inf = v.info[b];
     if (done && done[inf.x]) return;
     const int32_t start = v.start[b], cnt = v.start[b + 1] - start;
     if (cnt == 0) return;                            // only cells: nothing of its own to write
     if (skip_row && skip_row[start]) return;         // the piece is solved at level 0
-    const BrickGeo g = v.geo[inf.x];
     const T w = step ? (T)step[inf.x] : T(0);
-    if (threadIdx.x < NNB) {
-        const int32_t id = v.nbr[(int64_t)b * NNB + threadIdx.x];
-        nid[threadIdx.x] = id;
-        nstart[threadIdx.x] = id >= 0 ? v.start[id] : 0;
+    // the box starts at zero: faces that are no part stay so
+    {
+        constexpr int N16 = (int)(sizeof(T) * 6 * NBOX / 16);
+        float4* z = reinterpret_cast<float4*>(box);
+        for (int i = threadIdx.x; i < N16; i += BRICK_THREADS) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < NNB * MW; i += BRICK_THREADS) {
-        const int32_t id = nid[i / MW];
-        nmask[i] = id >= 0 ? __ldg(v.mask + (int64_t)id * MW + i % MW) : 0u;
-        npre[i] = id >= 0 ? __ldg(v.pre + (int64_t)id * MW + i % MW) : (uint16_t)0;
+    // The box is filled by asynchronous copies (cp.async: global memory straight to shared
+    // memory, no registers in between) issued together and awaited once: the brick's own
+    // parts, their run read in order, each to its face's entry (by its part_code, kept for
+    // the part phase), and the halo parts of its resolved list (bricks_build).
+    const bool vec16 = sizeof(T) == 8 && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    for (int t = threadIdx.x; t < cnt; t += BRICK_THREADS) {
+        const uint32_t c = __ldg(v.code + start + t);
+        codes[t] = (uint16_t)c;
+        copy_part<T>(box + 6 * own_entry(c), x + 6 * ((int64_t)start + t), vec16);
+    }
+    {
+        const int32_t h0 = __ldg(v.hstart + b), h1 = __ldg(v.hstart + b + 1);
+        for (int32_t h = h0 + threadIdx.x; h < h1; h += BRICK_THREADS)
+            copy_part<T>(box + 6 * (int)__ldg(v.hent + h), x + 6 * (int64_t)__ldg(v.hsrc + h), vec16);
     }
     // k of the brick's cells and of the single layers before it (-x, -y, -z)
-    for (int i = threadIdx.x; i < KB; i += BRICK_THREADS) {
-        const int c2 = i % (BZ + 1) - 1, c1 = i / (BZ + 1) % (BY + 1) - 1, c0 = i / ((BZ + 1) * (BY + 1)) - 1;
-        float kv = 0.0f;
-        if ((c0 < 0) + (c1 < 0) + (c2 < 0) <= 1) {
-            const int q = c0 < 0 ? 1 : c1 < 0 ? 2 : c2 < 0 ? 3 : 0;
-            const int32_t id = nid[q];
-            if (id >= 0)
-                kv = __ldg(v.kd + (int64_t)id * BCELLS +
-                           ((c0 < 0 ? BX - 1 : c0) * BY + (c1 < 0 ? BY - 1 : c1)) * BZ + (c2 < 0 ? BZ - 1 : c2));
-        }
-        kbox[i] = kv;
-    }
-    __syncthreads();
-    // the x box: every face the parts' cells touch, zero where the face is no part, its
-    // rotations times the spacing. A thread's entries (i = tid + j * BRICK_THREADS) are
-    // located first (box_table), then all their loads issued, then stored, so the loads
-    // of one thread are in flight together.
-    constexpr int PER_THREAD = (NBOX + BRICK_THREADS - 1) / BRICK_THREADS;
-    const bool last0 = inf.y == g.nbx - 1, last1 = inf.z == g.nby - 1, last2 = inf.w == g.nbz - 1;
-    int32_t src[PER_THREAD];  // 6 * (index of the part in x), or -1: a zero; -2: not stored
-#pragma unroll
-    for (int j = 0; j < PER_THREAD; j++) {
-        const int i = threadIdx.x + j * BRICK_THREADS;
-        src[j] = -2;
-        if (i >= NBOX) continue;
-        const uint4 e = __ldg(v.box + i);
-        if (!(e.x >> 31)) continue;  // read by no part
-        src[j] = -1;
-        const int a = (e.x >> 25) & 3;
-        const bool own_plane = ((e.x >> 24) & 1u) && (a == 0 ? last0 : a == 1 ? last1 : last2);
-        const uint32_t w = own_plane ? e.y : e.x;
-        const int q = (w >> 27) & 15, slot = w & 0xFFF;
-        if (nid[q] < 0) continue;
-        const uint32_t m = nmask[q * MW + slot / 32];
-        if (!((m >> (slot & 31)) & 1u)) continue;
-        const int rank = npre[q * MW + slot / 32] + __popc(m & ((1u << (slot & 31)) - 1u));
-        src[j] = 6 * (nstart[q] + rank);
-        if (q == 0) codes[rank] = own_plane ? e.w : e.z;
-    }
-    T val[PER_THREAD][6];
-#pragma unroll
-    for (int j = 0; j < PER_THREAD; j++) {
-        if (src[j] >= 0) {
-            load6<T>(x + src[j], 0, val[j]);
-        } else {
-#pragma unroll
-            for (int e = 0; e < 6; e++) val[j][e] = T(0);
+    {
+        const int t = threadIdx.x;  // BRICK_THREADS == BCELLS: one cell of the brick a thread
+        kbox[kbox_index(t / (BY * BZ), t / BZ % BY, t % BZ)] = __ldg(v.kd + (int64_t)b * BCELLS + t);
+        if (t < HK) {
+            int h0, h1, h2;
+            if (t < HKX) {
+                h0 = -1, h1 = t / BZ, h2 = t % BZ;
+            } else if (t < HKX + HKY) {
+                h0 = (t - HKX) / BZ, h1 = -1, h2 = (t - HKX) % BZ;
+            } else {
+                h0 = (t - HKX - HKY) / BY, h1 = (t - HKX - HKY) % BY, h2 = -1;
+            }
+            kbox[kbox_index(h0, h1, h2)] = __ldg(v.hk + (int64_t)b * HK + t);
         }
     }
-#pragma unroll
-    for (int j = 0; j < PER_THREAD; j++) {
-        if (src[j] == -2) continue;
-        val[j][3] *= s;
-        val[j][4] *= s;
-        val[j][5] *= s;
-        sts6<T>(box, threadIdx.x + j * BRICK_THREADS, val[j]);
-    }
+    cp_async_wait_all();
     __syncthreads();
     // the brick's parts, in storage order (their vectors from the brick's first part on)
     const T* rb = r ? r + 6 * (int64_t)start : nullptr;
@@ -591,15 +601,99 @@ __global__ void __launch_bounds__(256) k_brick_jacobi(int64_t n, const float2* _
     store6<T>(x, i, d);
 }
 
+// A brick's halo, resolved once for the solve: for each entry of the halo table, the
+// part (brick order) that fills it, where the neighbour brick holds one there. Pass 0
+// counts a brick's items, pass 1 writes them at the brick's offset.
+template <int PASS>
+__global__ void k_halo_lists(int32_t nb, const int4* __restrict__ info, const BrickGeo* __restrict__ geo,
+                             const int32_t* __restrict__ nbr, const uint32_t* __restrict__ mask,
+                             const uint16_t* __restrict__ pre, const int32_t* __restrict__ start,
+                             const uint2* __restrict__ tbl, int32_t nhalo, int32_t* __restrict__ count,
+                             const int32_t* __restrict__ hstart, uint16_t* __restrict__ hent,
+                             int32_t* __restrict__ hsrc) {
+    const int32_t b = blockIdx.x;
+    if (b >= nb) return;
+    const int4 in = info[b];
+    const BrickGeo g = geo[in.x];
+    const bool last[3] = {in.y == g.nbx - 1, in.z == g.nby - 1, in.w == g.nbz - 1};
+    __shared__ int32_t n_items;
+    if (threadIdx.x == 0) n_items = 0;
+    __syncthreads();
+    for (int h = threadIdx.x; h < nhalo; h += blockDim.x) {
+        const uint2 ee = tbl[h];
+        const int a = (ee.x >> 25) & 3;
+        const uint32_t e = (((ee.x >> 24) & 1u) && last[a]) ? ee.y : ee.x;
+        const int q = (e >> 27) & 15, slot = e & 0xFFF;
+        if (q == 0) continue;  // the brick's own plane part
+        const int32_t id = nbr[(int64_t)b * NNB + q];
+        if (id < 0) continue;
+        const uint32_t m = mask[(int64_t)id * MW + slot / 32];
+        if (!((m >> (slot & 31)) & 1u)) continue;
+        const int32_t src = start[id] + pre[(int64_t)id * MW + slot / 32] + __popc(m & ((1u << (slot & 31)) - 1u));
+        const int32_t k = atomicAdd(&n_items, 1);
+        if (PASS == 1) {
+            hent[hstart[b] + k] = (uint16_t)((ee.x >> 12) & 0xFFF);
+            hsrc[hstart[b] + k] = src;
+        }
+    }
+    __syncthreads();
+    if (PASS == 0 && threadIdx.x == 0) count[b] = n_items;
+}
+
+// per brick the k of the cells of its -x, -y and -z layers (the neighbours' boundary cells)
+__global__ void k_halo_k(int32_t nb, const int32_t* __restrict__ nbr, const float* __restrict__ kd,
+                         float* __restrict__ hk) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)nb * HK) return;
+    const int64_t b = i / HK;
+    const int t = (int)(i % HK);
+    int q, src;
+    if (t < HKX) {
+        q = 1;
+        src = ((BX - 1) * BY + t / BZ) * BZ + t % BZ;
+    } else if (t < HKX + HKY) {
+        q = 2;
+        src = ((t - HKX) / BZ * BY + BY - 1) * BZ + (t - HKX) % BZ;
+    } else {
+        q = 3;
+        src = ((t - HKX - HKY) / BY * BY + (t - HKX - HKY) % BY) * BZ + BZ - 1;
+    }
+    const int32_t id = nbr[b * NNB + q];
+    hk[i] = id >= 0 ? kd[(int64_t)id * BCELLS + src] : 0.0f;
+}
+
 BrickView view_of(const Bricks& K) {
-    return BrickView{K.start.get(),
-                     K.mask.get(),
-                     K.pre.get(),
-                     K.info.get(),
-                     K.nbr.get(),
-                     K.kd.get(),
-                     reinterpret_cast<const BrickGeo*>(K.geo.get()),
-                     reinterpret_cast<const uint4*>(K.box.get())};
+    BrickView v;
+    v.start = K.start.get();
+    v.mask = K.mask.get();
+    v.pre = K.pre.get();
+    v.info = K.info.get();
+    v.nbr = K.nbr.get();
+    v.kd = K.kd.get();
+    v.geo = reinterpret_cast<const BrickGeo*>(K.geo.get());
+    v.code = K.code.get();
+    v.hstart = K.hstart.get();
+    v.hent = K.hent.get();
+    v.hsrc = K.hsrc.get();
+    v.hk = K.hk.get();
+    return v;
+}
+
+// each brick-ordered part's part_code, from its sort key's slot
+__global__ void k_part_codes(int64_t n, const uint64_t* __restrict__ key, uint16_t* __restrict__ code) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int e = (int)(key[i] % NSLOT);
+    int a = 0;
+    if (e >= NS0 + NS1) {
+        a = 2;
+        e -= NS0 + NS1;
+    } else if (e >= NS0) {
+        a = 1;
+        e -= NS0;
+    }
+    const int e2 = slot_ext(a, 2), e1 = slot_ext(a, 1);
+    code[i] = (uint16_t)part_code(a, e / (e2 * e1), e / e2 % e1, e % e2);
 }
 
 }  // namespace
@@ -630,9 +724,10 @@ void bricks_build(Context& ctx, Batch& b) {
     }
     K.geo.alloc(np * sizeof(BrickGeo), st, ms);
     SC_CK(cudaMemcpyAsync(K.geo.get(), geo.data(), np * sizeof(BrickGeo), cudaMemcpyHostToDevice, st));
-    const std::vector<uint4> tbl = box_table();
-    K.box.alloc(tbl.size() * sizeof(uint4), st, ms);
-    SC_CK(cudaMemcpyAsync(K.box.get(), tbl.data(), tbl.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
+    const std::vector<uint2> tbl = halo_table();
+    K.nhalo = (int32_t)tbl.size();
+    K.halo.alloc(tbl.size() * sizeof(uint2), st, ms);
+    SC_CK(cudaMemcpyAsync(K.halo.get(), tbl.data(), tbl.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
     const BrickGeo* geo_d = reinterpret_cast<const BrickGeo*>(K.geo.get());
     DBuf<int32_t> flag, bid;
     flag.alloc(npos + 1, st, ms);
@@ -685,6 +780,34 @@ void bricks_build(Context& ctx, Batch& b) {
     if (nb > 0) {
         k_brick_k<<<grid_for((int64_t)nb * BCELLS, 256), 256, 0, st>>>(nb, K.info.get(), geo_d, g.gridmap.get(),
                                                                         g.cell.get(), K.kd.get());
+        SC_LAUNCH_CK();
+    }
+    K.code.alloc(n, st, ms);
+    k_part_codes<<<grid_for(n, 256), 256, 0, st>>>(n, key_s.get(), K.code.get());
+    SC_LAUNCH_CK();
+    // each brick's halo list and the k of its neighbours' boundary cells
+    K.hstart.alloc(nb1 + 1, st, ms);
+    K.hk.alloc(nb1 * HK, st, ms);
+    if (nb > 0) {
+        const uint2* tbl_d = reinterpret_cast<const uint2*>(K.halo.get());
+        DBuf<int32_t> hcount;
+        hcount.alloc(nb1 + 1, st, ms);
+        hcount.zero();
+        k_halo_lists<0><<<nb, 256, 0, st>>>(nb, K.info.get(), geo_d, K.nbr.get(), K.mask.get(), K.pre.get(),
+                                             K.start.get(), tbl_d, K.nhalo, hcount.get(), nullptr, nullptr, nullptr);
+        SC_LAUNCH_CK();
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, hcount.get(), K.hstart.get(), nb + 1, st);
+        cub::DeviceScan::ExclusiveSum(ctx.cub_scratch(tb), tb, hcount.get(), K.hstart.get(), nb + 1, st);
+        int32_t items = 0;
+        SC_CK(cudaMemcpyAsync(&items, K.hstart.get() + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SC_CK(cudaStreamSynchronize(st));
+        K.hent.alloc(std::max<int32_t>(items, 1), st, ms);
+        K.hsrc.alloc(std::max<int32_t>(items, 1), st, ms);
+        k_halo_lists<1><<<nb, 256, 0, st>>>(nb, K.info.get(), geo_d, K.nbr.get(), K.mask.get(), K.pre.get(),
+                                             K.start.get(), tbl_d, K.nhalo, nullptr, K.hstart.get(), K.hent.get(),
+                                             K.hsrc.get());
+        SC_LAUNCH_CK();
+        k_halo_k<<<grid_for((int64_t)nb * HK, 256), 256, 0, st>>>(nb, K.nbr.get(), K.kd.get(), K.hk.get());
         SC_LAUNCH_CK();
     }
     K.bo_of_ref.alloc(n, st, ms);

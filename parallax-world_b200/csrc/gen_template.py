@@ -159,6 +159,24 @@ def emit(K, fac):
                 for j, v in terms:
                     w(f"    acc[{i}] = fma(T({lit(v)}), x[{j}], acc[{i}]);\n")
             w("  }\n};\n")
+    # the same blocks at level 0's spacing s = UNIT = 1/8 (statics/src/lattice.rs:16): the
+    # cell matrix k s D T D with D = diag(1, 1, 1, s, s, s) per face, so a level-0 stencil
+    # that reads the motions as they are needs no scaling (every factor is a power of two,
+    # so each product, and each FMA's rounding, is the unscaled one's times that factor)
+    s0 = 0.125
+    d = [1.0, 1.0, 1.0, s0, s0, s0]
+    w("// The blocks of k s D T D at level 0's spacing s = 1/8, D = diag(1, 1, 1, s, s, s).\n")
+    w("template <int S, int F>\nstruct BlkS;\n")
+    for slot in range(6):
+        for f in range(6):
+            w(f"template <>\nstruct BlkS<{slot}, {f}> {{\n  template <class T>\n")
+            w("  __device__ __forceinline__ static void mac(const T (&x)[6], T (&acc)[6]) {\n")
+            for i in range(6):
+                terms = [(j, K[6 * slot + i, 6 * f + j]) for j in range(6) if K[6 * slot + i, 6 * f + j] != 0.0]
+                for j, v in terms:
+                    w(f"    acc[{i}] = fma(T({lit(v * s0 * d[i] * d[j])}), x[{j}], acc[{i}]);\n")
+            w("  }\n};\n")
+    w(f"constexpr double TPL_SPACING0 = {lit(s0)};\n")
     w("\n")
     nnz = int((K != 0).sum())
     w(f"constexpr int TPL_NNZ = {nnz};\n\n")

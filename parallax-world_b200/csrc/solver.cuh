@@ -31,7 +31,13 @@ struct Bricks {
     DBuf<int32_t> nbr;          // per brick: the 13 bricks its stencil reads from (-1 none)
     DBuf<float> kd;             // per brick: each cell's k (0 where not free)
     DBuf<uint8_t> geo;          // per piece: dimensions, brick grid, first cell and brick
-    DBuf<uint8_t> box;          // where each entry of a brick's shared-memory box comes from
+    DBuf<uint8_t> halo;         // the entries of a brick's shared-memory box its neighbours fill
+    int32_t nhalo = 0;
+    DBuf<uint16_t> code;        // per brick-ordered part: its axis and brick-local position
+    DBuf<int32_t> hstart;       // n_bricks + 1: each brick's halo list
+    DBuf<uint16_t> hent;        // per halo item: the box entry it fills
+    DBuf<int32_t> hsrc;         // per halo item: the brick-ordered part it comes from
+    DBuf<float> hk;             // per brick: the k of its -x, -y, -z neighbours' boundary cells
     DBuf<int32_t> ref_of_bo;    // brick-ordered part -> the reference's part index
     DBuf<int32_t> bo_of_ref;    // and back
     DBuf<float2> kk;            // per brick-ordered part: its cells' k, its axis in their signs
