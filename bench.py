@@ -674,7 +674,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--ref-budget", type=float, default=600.0,
+    ap.add_argument("--ref-budget", type=float, default=300.0,
                     help="--impl reference: seconds after which no further whole solve is started")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-pieces section")
     ap.add_argument("--no-large", action="store_true", help="skip the 256^3 forward + adjoint section")
