@@ -349,8 +349,8 @@ sc_status sc_compliance_noalloc(const double* loads, const double* motions, int6
  * The system: n unknowns with their octree site (3 int64), position `at` (3 doubles)
  * and 3x3 diagonal block (9 doubles, row-major); npairs pairs (pi, pj, 3x3 block pb:
  * pb in row pi, column pj, its transpose in row pj, column pi; a pair twice adds). All
- * host arrays. Makes the levels (Solver::new(system, size): rigid aggregates by octree
- * cell, their Galerkin blocks, Cholesky inverses with dropped pivots, a direct top) and
+ * host arrays. Makes the levels on the device (Solver::new(system, size): rigid aggregates
+ * by octree cell, their Galerkin blocks, Cholesky inverses with dropped pivots, a direct top) and
  * solves by PCG from x (3 n doubles, in/out) until r' P r <= tol^2 b' P b, P the V-cycle
  * preconditioner (Solver::solve). *rounds: the rounds taken (at most 300), or -1 where
  * the levels do not fit the system (not positive; the reference's None). *levels: the
@@ -372,6 +372,11 @@ sc_status sc_mech_voxel_system(const uint8_t* state, const float* e, int32_t nx,
 sc_status sc_mech_levels(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
                          const uint32_t* pi, const uint32_t* pj, const double* pb, double size, int32_t max_levels,
                          int64_t* sizes, double* steps, int32_t* nlevels);
+/* The same levels made on the context's device, as sc_mech_solve makes them (the same
+ * parts and steps, bit for bit, as sc_mech_levels): Solver::new (solve.rs:361-386). */
+sc_status sc_mech_levels_on(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
+                            int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, double size,
+                            int32_t max_levels, int64_t* sizes, double* steps, int32_t* nlevels);
 sc_status sc_mech_solve(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
                         int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b,
                         double* x, double tol, double size, int32_t* rounds, int32_t* levels);

@@ -595,6 +595,24 @@ sc_status sc_mech_levels(int64_t n, const int64_t* sites, const double* at, cons
     }
 }
 
+sc_status sc_mech_levels_on(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
+                            int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, double size,
+                            int32_t max_levels, int64_t* sizes, double* steps, int32_t* nlevels) {
+    if (n <= 0 || npairs < 0 || !sites || !at || !diag || !nlevels || !(size > 0.0) || max_levels < 0) return SC_BAD_INPUT;
+    if (!steps || (max_levels > 0 && !sizes)) return SC_BAD_INPUT;
+    if (npairs > 0 && (!pi || !pj || !pb)) return SC_BAD_INPUT;
+    for (int64_t p = 0; p < npairs; p++)
+        if ((int64_t)pi[p] >= n || (int64_t)pj[p] >= n || pi[p] == pj[p]) return SC_BAD_INPUT;
+    return guarded(ctx, [&] {
+        std::vector<int64_t> sz;
+        std::vector<double> st;
+        mech_levels_device(ctx->c, n, sites, at, diag, npairs, pi, pj, pb, size, sz, st);
+        *nlevels = (int32_t)sz.size();
+        for (size_t l = 0; l < sz.size() && (int32_t)l < max_levels; l++) sizes[l] = sz[l];
+        for (size_t l = 0; l < st.size() && (int32_t)l <= max_levels; l++) steps[l] = st[l];
+    });
+}
+
 sc_status sc_mech_solve(sc_context* ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
                         int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, const double* b,
                         double* x, double tol, double size, int32_t* rounds, int32_t* levels) {

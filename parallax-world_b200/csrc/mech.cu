@@ -1,14 +1,15 @@
 // The engine's solver, mechanics::solve::Solver (mechanics/src/solve.rs:356-538), on the
-// device. Its levels are made on the host, as Solver::new makes them (solve.rs:241-271,
-// 361-386: rigid aggregates of the parts joined within each octree cell a level up, their
-// Galerkin blocks T(r)' M T(s), block inverses by Cholesky with dropped pivots, the turn
-// regularisation, the smoother step by ten power steps, a direct top), and kept on the
-// device as block-sparse rows (3x3 at the cells' nodes, 6x6 above, both triangles). The
-// conjugate gradients and V-cycles (solve.rs:403-538) run there: block products,
-// block-Jacobi smoothing, the rigid restriction and prolongation, the top's dense
-// inverse, and deterministic dot products. Coarse pairs are kept in (a, c) order (the
-// reference collects them from a hash map, solve.rs:249-262): sums over pairs add in
-// another order, equal up to rounding.
+// device. Its levels (Solver::new, solve.rs:241-271, 361-386: rigid aggregates of the parts
+// joined within each octree cell a level up, their Galerkin blocks T(r)' M T(s), block
+// inverses by Cholesky with dropped pivots, the turn regularisation, the smoother step by
+// ten power steps, a direct top) are made on the device by mech_levels.cu and kept there
+// as block-sparse rows (3x3 at the cells' nodes, 6x6 above, both triangles). This file
+// keeps a host copy of that construction (sc_mech_levels, no device) and runs the
+// conjugate gradients and V-cycles (solve.rs:403-538): block products, block-Jacobi
+// smoothing, the rigid restriction and prolongation, the top's dense inverse, and
+// deterministic dot products. Coarse pairs are kept in (a, c) order (the reference
+// collects them from a hash map, solve.rs:249-262): sums over pairs add in another order,
+// equal up to rounding.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -18,6 +19,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "mech.cuh"
 
 namespace sc {
 
@@ -28,8 +30,7 @@ typedef std::array<H3, 3> HM3;
 typedef std::array<double, 6> H6;
 typedef std::array<H6, 6> HM6;
 
-constexpr int MECH_ROUNDS = 300;   // solve.rs:21
-constexpr size_t MECH_DIRECT = 24;  // solve.rs:23
+constexpr int MECH_ROUNDS = 300;  // solve.rs:21
 
 // ---- the levels, on the host ------------------------------------------------------
 struct HPair {
@@ -448,95 +449,6 @@ HLevel coarsen(const Fine& f, double size) {  // solve.rs:241-271
 }
 
 // ---- the device ---------------------------------------------------------------------
-struct DLevel {
-    int64_t n = 0;
-    DBuf<int32_t> of;  // finer part -> part here
-    DBuf<double> r;    // 3 per finer part
-    DBuf<int64_t> mptr;
-    DBuf<int32_t> mem;  // each part's finer parts, in order
-    DBuf<int64_t> rowptr;
-    DBuf<int32_t> col;
-    DBuf<double> val, inv, step;
-    int64_t nnzb = 0;
-    bool direct = false;
-    DBuf<double> top_inv;
-    DBuf<double> b, x, res, t;
-};
-
-// Full block rows (B x B blocks) of a symmetric system from its diagonal blocks and its
-// pairs (i, j, M: M in row i, column j, M' in row j, column i), columns in order: counted,
-// placed, then each row's few entries sorted by column.
-template <int B, class DiagAt, class PairAt>
-void block_rows(int64_t n, int64_t npairs, const uint32_t* pi, const uint32_t* pj, DiagAt diag_at, PairAt pair_at,
-                std::vector<int64_t>& rp, std::vector<int32_t>& col, std::vector<double>& val) {
-    rp.assign(n + 1, 0);
-    for (int64_t p = 0; p < n; p++) rp[p + 1] = 1;
-    for (int64_t e = 0; e < npairs; e++) {
-        rp[pi[e] + 1]++;
-        rp[pj[e] + 1]++;
-    }
-    for (int64_t p = 0; p < n; p++) rp[p + 1] += rp[p];
-    const int64_t nnz = rp[n];
-    // per entry: its column and its source (2 e + 1: pair e transposed; 2 e: pair e; -1 - p: diagonal p)
-    std::vector<int32_t> c(nnz);
-    std::vector<int64_t> src(nnz);
-    std::vector<int64_t> pos(rp.begin(), rp.end() - 1);
-    for (int64_t p = 0; p < n; p++) {
-        c[pos[p]] = (int32_t)p;
-        src[pos[p]++] = -1 - p;
-    }
-    for (int64_t e = 0; e < npairs; e++) {
-        c[pos[pi[e]]] = (int32_t)pj[e];
-        src[pos[pi[e]]++] = 2 * e;
-        c[pos[pj[e]]] = (int32_t)pi[e];
-        src[pos[pj[e]]++] = 2 * e + 1;
-    }
-    std::vector<int64_t> idx;
-    col.resize(nnz);
-    val.resize((size_t)nnz * B * B);
-    for (int64_t p = 0; p < n; p++) {
-        idx.resize(rp[p + 1] - rp[p]);
-        for (size_t t = 0; t < idx.size(); t++) idx[t] = rp[p] + (int64_t)t;
-        std::sort(idx.begin(), idx.end(), [&](int64_t u, int64_t v) { return c[u] < c[v]; });
-        for (size_t t = 0; t < idx.size(); t++) {
-            const int64_t k = rp[p] + (int64_t)t, from = src[idx[t]];
-            col[k] = c[idx[t]];
-            double* out = val.data() + (size_t)k * B * B;
-            if (from < 0) {
-                for (int r = 0; r < B; r++)
-                    for (int q = 0; q < B; q++) out[B * r + q] = diag_at(-1 - from, r, q);
-            } else {
-                const int64_t e = from >> 1;
-                const bool t2 = from & 1;
-                for (int r = 0; r < B; r++)
-                    for (int q = 0; q < B; q++) out[B * r + q] = t2 ? pair_at(e, q, r) : pair_at(e, r, q);
-            }
-        }
-    }
-}
-
-void upload_rows(Context& ctx, const HSys& s, DLevel& D) {
-    const int64_t n = (int64_t)s.diag.size(), m = (int64_t)s.pairs.size();
-    std::vector<uint32_t> pi(m), pj(m);
-    for (int64_t e = 0; e < m; e++) {
-        pi[e] = s.pairs[e].i;
-        pj[e] = s.pairs[e].j;
-    }
-    std::vector<int64_t> rp;
-    std::vector<int32_t> col;
-    std::vector<double> val;
-    block_rows<6>(
-        n, m, pi.data(), pj.data(), [&](int64_t p, int r, int q) { return s.diag[p][r][q]; },
-        [&](int64_t e, int r, int q) { return s.pairs[e].m[r][q]; }, rp, col, val);
-    D.nnzb = (int64_t)col.size();
-    D.rowptr.alloc(n + 1, ctx.stream, &ctx.mem);
-    D.rowptr.upload(rp.data(), n + 1);
-    D.col.alloc(std::max<int64_t>(D.nnzb, 1), ctx.stream, &ctx.mem);
-    D.col.upload(col.data(), col.size());
-    D.val.alloc(std::max<size_t>(val.size(), 1), ctx.stream, &ctx.mem);
-    D.val.upload(val.data(), val.size());
-}
-
 // y = S x (resid: y = b - S x) over the nodes' 3x3 block rows
 __global__ void k_bsr3(int64_t n, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                        const double* __restrict__ val, const double* __restrict__ x, const double* __restrict__ b,
@@ -665,16 +577,11 @@ __global__ void k_mupdate(int64_t n, int update, double s, double* __restrict__ 
 
 struct MechSolver {
     Context& ctx;
-    int64_t n0 = 0;
-    DBuf<int64_t> rowptr0;
-    DBuf<int32_t> col0;
-    DBuf<double> val0, inv0;
-    double step0 = 1.0;
-    std::vector<DLevel> lv;
+    MechLevels& M;
     DBuf<double> part;
     std::vector<double> hpart;
 
-    explicit MechSolver(Context& c) : ctx(c) {}
+    MechSolver(Context& c, MechLevels& m) : ctx(c), M(m) {}
 
     double dot(const double* a, const double* b, int64_t n) {
         k_mdot<<<MDOT_BLOCKS, 256, 0, ctx.stream>>>(n, a, b, part.get());
@@ -686,18 +593,19 @@ struct MechSolver {
         return s;
     }
     void times(const double* x, double* y, const double* b = nullptr) {
-        k_bsr3<<<grid_for(n0, 128), 128, 0, ctx.stream>>>(n0, rowptr0.get(), col0.get(), val0.get(), x, b, y);
+        k_bsr3<<<grid_for(M.n0, 128), 128, 0, ctx.stream>>>(M.n0, M.rowptr0.get(), M.col0.get(), M.val0.get(), x, b,
+                                                             y);
         SC_LAUNCH_CK();
     }
     // x = V-cycle of level l for its b (solve.rs:403-447)
     void cycle(size_t l) {
-        DLevel& L = lv[l];
+        MechLevel& L = M.lv[l];
         if (L.direct) {
             k_top<<<1, 256, 0, ctx.stream>>>(6 * L.n, L.top_inv.get(), L.b.get(), L.x.get());
             SC_LAUNCH_CK();
             return;
         }
-        DLevel& U = lv[l + 1];
+        MechLevel& U = M.lv[l + 1];
         jacobi<double>(ctx, L.n, L.inv.get(), L.b.get(), L.x.get(), L.step.get(), nullptr, nullptr, nullptr);
         spmv<double>(ctx, SPMV_RES, L.n, L.rowptr.get(), L.col.get(), L.val.get(), L.x.get(), L.b.get(), L.res.get(),
                      nullptr, nullptr, nullptr, nullptr, nullptr, L.nnzb);
@@ -715,19 +623,19 @@ struct MechSolver {
     }
     // out = the preconditioner of b (solve.rs:450-476); scratch: 3 n0
     void precondition(const double* b, double* out, double* scratch) {
-        const unsigned g = grid_for(n0, 256);
-        k_jacobi3<<<g, 256, 0, ctx.stream>>>(n0, inv0.get(), step0, b, nullptr, nullptr, out);
+        const unsigned g = grid_for(M.n0, 256);
+        k_jacobi3<<<g, 256, 0, ctx.stream>>>(M.n0, M.inv0.get(), M.step0, b, nullptr, nullptr, out);
         SC_LAUNCH_CK();
         times(out, scratch);
-        DLevel& U = lv[0];
+        MechLevel& U = M.lv[0];
         k_restrict<3><<<grid_for(U.n, 128), 128, 0, ctx.stream>>>(U.n, U.mptr.get(), U.mem.get(), U.r.get(), b,
                                                                    scratch, U.b.get());
         SC_LAUNCH_CK();
         cycle(0);
-        k_prolong<3><<<g, 256, 0, ctx.stream>>>(n0, U.of.get(), U.r.get(), U.x.get(), out);
+        k_prolong<3><<<g, 256, 0, ctx.stream>>>(M.n0, U.of.get(), U.r.get(), U.x.get(), out);
         SC_LAUNCH_CK();
         times(out, scratch);
-        k_jacobi3<<<g, 256, 0, ctx.stream>>>(n0, inv0.get(), step0, b, scratch, out, out);
+        k_jacobi3<<<g, 256, 0, ctx.stream>>>(M.n0, M.inv0.get(), M.step0, b, scratch, out, out);
         SC_LAUNCH_CK();
     }
 };
@@ -960,6 +868,40 @@ void mech_levels(int64_t n, const int64_t* sites, const double* at, const double
     }
 }
 
+// The same, made on the device as mech_solve makes them.
+void mech_levels_device(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
+                        int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, double size,
+                        std::vector<int64_t>& sizes, std::vector<double>& steps) {
+    MechLevels M;
+    mech_device_levels(ctx, n, sites, at, diag, npairs, pi, pj, pb, size, M);
+    sizes.clear();
+    steps.assign(1, M.step0);
+    for (const MechLevel& L : M.lv) {
+        sizes.push_back(L.n);
+        steps.push_back(L.direct ? 0.0 : L.step_h);
+    }
+}
+
+std::vector<double> mech_top_inverse(int64_t n, const double* diag36, int64_t npairs, const uint32_t* pi,
+                                     const uint32_t* pj, const double* pm36, double size) {
+    HLevel L;
+    L.size = size;
+    L.sys.diag.resize((size_t)n);
+    for (int64_t p = 0; p < n; p++)
+        for (int r = 0; r < 6; r++)
+            for (int c = 0; c < 6; c++) L.sys.diag[p][r][c] = diag36[36 * p + 6 * r + c];
+    L.sys.pairs.resize((size_t)npairs);
+    for (int64_t e = 0; e < npairs; e++) {
+        HPair& q = L.sys.pairs[e];
+        q.i = pi[e];
+        q.j = pj[e];
+        for (int r = 0; r < 6; r++)
+            for (int c = 0; c < 6; c++) q.m[r][c] = pm36[36 * e + 6 * r + c];
+    }
+    factor_top(L);
+    return std::move(L.top_inv);
+}
+
 // The levels of the system, then PCG from x (solve.rs:356-386, 485-538): the rounds taken,
 // -1 where the levels do not fit the system (not positive).
 int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
@@ -969,75 +911,13 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
     MemStats* ms = &ctx.mem;
     if (n == 0) return 0;
     PhaseTimer pt(ctx);  // SC_TIMING=1 prints the phases
-    HostLevels HL = make_levels(n, sites, at, diag, npairs, pi, pj, pb, size);
-    const std::vector<double>& inv0 = HL.inv0;
-    const double step0 = HL.step0;
-    std::vector<HLevel>& levels = HL.levels;
-    *nlevels = (int32_t)levels.size();
-    pt.mark("mech: levels (host)");
-    // to the device
-    MechSolver S(ctx);
-    S.n0 = n;
-    S.step0 = step0;
-    {
-        std::vector<int64_t> rp;
-        std::vector<int32_t> col;
-        std::vector<double> val;
-        block_rows<3>(
-            n, npairs, pi, pj, [&](int64_t p, int r, int q) { return diag[9 * p + 3 * r + q]; },
-            [&](int64_t e, int r, int q) { return pb[9 * e + 3 * r + q]; }, rp, col, val);
-        S.rowptr0.alloc(n + 1, st, ms);
-        S.rowptr0.upload(rp.data(), n + 1);
-        S.col0.alloc(col.size(), st, ms);
-        S.col0.upload(col.data(), col.size());
-        S.val0.alloc(val.size(), st, ms);
-        S.val0.upload(val.data(), val.size());
-        S.inv0.alloc(inv0.size(), st, ms);
-        S.inv0.upload(inv0.data(), inv0.size());
-    }
-    S.lv.resize(levels.size());
-    for (size_t l = 0; l < levels.size(); l++) {
-        const HLevel& H = levels[l];
-        DLevel& D = S.lv[l];
-        D.n = (int64_t)H.sys.diag.size();
-        const int64_t nf = (int64_t)H.of.size();
-        D.of.alloc(nf, st, ms);
-        D.of.upload(reinterpret_cast<const int32_t*>(H.of.data()), nf);
-        std::vector<double> rr(3 * (size_t)nf);
-        for (int64_t i = 0; i < nf; i++)
-            for (int k = 0; k < 3; k++) rr[3 * i + k] = H.r[i][k];
-        D.r.alloc(rr.size(), st, ms);
-        D.r.upload(rr.data(), rr.size());
-        std::vector<int64_t> mp(D.n + 1, 0);
-        for (int64_t i = 0; i < nf; i++) mp[H.of[i] + 1]++;
-        for (int64_t a = 0; a < D.n; a++) mp[a + 1] += mp[a];
-        std::vector<int32_t> mem(nf);
-        std::vector<int64_t> fill(mp.begin(), mp.end() - 1);
-        for (int64_t i = 0; i < nf; i++) mem[fill[H.of[i]]++] = (int32_t)i;
-        D.mptr.alloc(D.n + 1, st, ms);
-        D.mptr.upload(mp.data(), D.n + 1);
-        D.mem.alloc(nf, st, ms);
-        D.mem.upload(mem.data(), nf);
-        D.b.alloc(6 * D.n, st, ms);
-        D.x.alloc(6 * D.n, st, ms);
-        D.res.alloc(6 * D.n, st, ms);
-        D.t.alloc(6 * D.n, st, ms);
-        D.direct = H.direct;
-        if (H.direct) {
-            D.top_inv.alloc(H.top_inv.size(), st, ms);
-            D.top_inv.upload(H.top_inv.data(), H.top_inv.size());
-        } else {
-            upload_rows(ctx, H.sys, D);
-            D.inv.alloc(H.inv.size(), st, ms);
-            D.inv.upload(H.inv.data(), H.inv.size());
-            D.step.alloc(1, st, ms);
-            D.step.upload(&H.step, 1);
-        }
-    }
+    MechLevels levels;
+    mech_device_levels(ctx, n, sites, at, diag, npairs, pi, pj, pb, size, levels);
+    *nlevels = (int32_t)levels.lv.size();
+    pt.mark("mech: levels (device)");
+    MechSolver S(ctx, levels);
     S.part.alloc(MDOT_BLOCKS, st, ms);
     S.hpart.resize(MDOT_BLOCKS);
-    SC_CK(cudaStreamSynchronize(st));
-    pt.mark("mech: levels to the device");
     // PCG from x (solve.rs:485-538)
     const int64_t m = 3 * n;
     DBuf<double> db, dx, r, z, p, ap, scratch;

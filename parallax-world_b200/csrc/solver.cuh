@@ -189,6 +189,9 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
 void mech_levels(int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
                  const uint32_t* pi, const uint32_t* pj, const double* pb, double size, std::vector<int64_t>& sizes,
                  std::vector<double>& steps);
+void mech_levels_device(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag,
+                        int64_t npairs, const uint32_t* pi, const uint32_t* pj, const double* pb, double size,
+                        std::vector<int64_t>& sizes, std::vector<double>& steps);
 void mech_voxel_system(const uint8_t* state, const float* e, int nx, int ny, int nz, double h, double dt,
                        double mass, std::vector<int64_t>& sites, std::vector<double>& at, std::vector<double>& diag,
                        std::vector<uint32_t>& pi, std::vector<uint32_t>& pj, std::vector<double>& pb,

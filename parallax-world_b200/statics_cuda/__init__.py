@@ -137,6 +137,8 @@ def lib():
                                      C.POINTER(C.c_int32)]
         L.sc_mech_solve.argtypes = [P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, C.c_double, C.c_double,
                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.sc_mech_levels_on.argtypes = [P, C.c_int64, P, P, P, C.c_int64, P, P, P, C.c_double, C.c_int32, P, P,
+                                        C.POINTER(C.c_int32)]
         L.sc_used_standing.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
                                        C.POINTER(SolveInfo)]
         L.sc_settle.argtypes = [P, C.POINTER(LatticeC), C.POINTER(Strength), C.POINTER(Options), P,
@@ -417,6 +419,23 @@ class Solver:
         d = info.as_dict()
         d["status"] = s
         return out[:n_nodes], d
+
+    def mech_levels(self, system: dict, size: float | None = None):
+        """The levels the engine's solver makes on this context's device for `system`
+        (sc_mech_levels_on, as mech_solve makes them): (parts of each coarse level,
+        smoother steps: the nodes' then each level's, 0 at the direct top)."""
+        sites = np.ascontiguousarray(system["sites"], np.int64)
+        at = np.ascontiguousarray(system["at"], np.float64)
+        diag = np.ascontiguousarray(system["diag"], np.float64)
+        pi = np.ascontiguousarray(system["pi"], np.uint32)
+        pj = np.ascontiguousarray(system["pj"], np.uint32)
+        pb = np.ascontiguousarray(system["pb"], np.float64)
+        sizes, steps, nl = np.zeros(64, np.int64), np.zeros(65), C.c_int32()
+        s = lib().sc_mech_levels_on(self.h, len(sites), _ptr(sites), _ptr(at), _ptr(diag), len(pi), _ptr(pi),
+                                    _ptr(pj), _ptr(pb), size or system["h"], 64, _ptr(sizes), _ptr(steps),
+                                    C.byref(nl))
+        self._check(s, "sc_mech_levels_on")
+        return list(sizes[:nl.value]), list(steps[:nl.value + 1])
 
     def mech_solve(self, system: dict, b=None, x0=None, tol: float = 1e-3, size: float | None = None):
         """The engine's solver (mechanics::solve::Solver::new then solve, solve.rs:356-538)
