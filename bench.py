@@ -640,7 +640,8 @@ def batch_section(solver, sc, rank, world, args):
     setting = autotune.choose(solver, mine_p, sc.MIXED, TOL)
     tune_s = time.perf_counter() - t
     stream = torch.cuda.ExternalStream(solver.stream())
-    autotune.solve_batch(solver, mine_p[: min(8, len(mine_p))], sc.MIXED, TOL, setting=setting)  # warm-up
+    # warm-up: the same batch once, so the timed run finds the device pool grown to its peak
+    autotune.solve_batch(solver, mine_p, sc.MIXED, TOL, setting=setting)
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -137,9 +137,10 @@ sc_status sc_solve_grid(sc_context* ctx, const sc_grid* g, const sc_options* opt
                         int64_t capacity, int32_t motions_on_device, sc_solve_info* info);
 
 /* Many pieces at once: each its own hierarchy and its own CG, advanced together by
- * batched kernels in one CUDA graph per iteration. motions[i] receives piece i's
- * n_nodes x 6 values (host pointers); infos[i] its info. No counterpart in the
- * reference, which solves one structure per call. */
+ * batched kernels in one CUDA graph per iteration. The pieces are solved in groups of at
+ * most 5 M grid cells, taken largest first. motions[i] receives piece i's n_nodes x 6
+ * values (host pointers); infos[i] its info. No counterpart in the reference, which
+ * solves one structure per call. */
 sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, const sc_options* opt,
                               double* const* motions, sc_solve_info* infos);
 

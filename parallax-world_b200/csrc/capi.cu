@@ -684,18 +684,25 @@ sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, 
         c.last.reset();  // the previous solve's hierarchy is not kept through this one
         SC_CK(cudaStreamSynchronize(c.stream));
         c.mem.peak = c.mem.now;
+        // groups of pieces taken largest first (ties in the caller's order), so a group's
+        // pieces are of one size class and the groups' setups of similar size
+        std::vector<int> order(n);
+        for (int i = 0; i < n; i++) order[i] = i;
+        auto cells_of = [&](int i) { return (int64_t)all[i].nx * all[i].ny * all[i].nz; };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cells_of(a) > cells_of(b); });
         int first = 0;
         while (first < n) {
-            // the next group: consecutive pieces up to the cell budget (at least one)
+            // the next group: the next pieces in that order up to the cell budget (at least one)
             int last = first;
             int64_t cells = 0;
             while (last < n) {
-                int64_t gc = (int64_t)all[last].nx * all[last].ny * all[last].nz;
+                int64_t gc = cells_of(order[last]);
                 if (last > first && cells + gc > BATCH_CELLS) break;
                 cells += gc;
                 last++;
             }
-            std::vector<sc_grid> gs(all.begin() + first, all.begin() + last);
+            std::vector<sc_grid> gs;
+            for (int q = first; q < last; q++) gs.push_back(all[order[q]]);
             int m = last - first;
             c.last.reset();
             auto b = std::make_unique<Batch>();
@@ -716,16 +723,16 @@ sc_status sc_solve_grid_batch(sc_context* ctx, int32_t n, const sc_grid* grids, 
                                                                  b->part_node.get(), x.get(), out.get());
             SC_LAUNCH_CK();
             for (int p = 0; p < m; p++)
-                if (motions[first + p])
-                    SC_CK(cudaMemcpyAsync(motions[first + p], out.get() + 6 * start[p],
+                if (motions[order[first + p]])
+                    SC_CK(cudaMemcpyAsync(motions[order[first + p]], out.get() + 6 * start[p],
                                           6 * b->node_count[p] * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
             SC_CK(cudaStreamSynchronize(c.stream));
             if (infos) {
-                for (int p = 0; p < m; p++) fill_info(*b, p, st, infos + first + p, solve_ms, c.mem.peak);
+                for (int p = 0; p < m; p++) fill_info(*b, p, st, infos + order[first + p], solve_ms, c.mem.peak);
                 for (size_t l = 0; l < b->levels.size() && l < SC_MAX_LEVELS; l++) {
                     std::vector<double> steps = b->levels[l].step.to_host();
                     for (int p = 0; p < m; p++)
-                        if ((int)l < infos[first + p].levels) infos[first + p].steps[l] = steps[p];
+                        if ((int)l < infos[order[first + p]].levels) infos[order[first + p]].steps[l] = steps[p];
                 }
             }
             c.last = std::move(b);

@@ -47,7 +47,10 @@ inline void require(bool ok, sc_status s, const std::string& msg) {
 // as cudaFreeAsync / cudaMallocAsync would, but without calling the driver, whose
 // allocation calls were measured at milliseconds each: repeated solves of similar sizes
 // then allocate nothing. Requests are rounded up to size classes (1/8 steps of their
-// power of two, at least 512 bytes) so that similar sizes share blocks. Like a caching
+// power of two, at least 512 bytes) and served by the smallest cached block of at least
+// their class and at most twice it, so that similar sizes share blocks (a batch's groups
+// differ a little in size, and a miss grows the driver's pool by mapping new memory, at
+// tens of milliseconds a gigabyte). Like a caching
 // allocator, the cache keeps what it is given up to `cap` bytes (half the device's memory
 // by default); when the pool runs out, an allocation gives the cached blocks back and
 // tries again.
@@ -69,11 +72,13 @@ struct MemStats {
         size_t step = std::max<size_t>(p2 / 8, 512);
         return (bytes + step - 1) / step * step;
     }
-    // a cached block of exactly this size class, or null
-    void* take(size_t bytes) {
-        auto it = cache.find(bytes);
-        if (it == cache.end()) return nullptr;
+    // the smallest cached block of at least `bytes` (a size class) and at most twice it,
+    // or null; `bytes` becomes the block's size
+    void* take(size_t& bytes) {
+        auto it = cache.lower_bound(bytes);
+        if (it == cache.end() || it->first > 2 * bytes) return nullptr;
         void* p = it->second;
+        bytes = it->first;
         cached -= bytes;
         cache.erase(it);
         return p;
