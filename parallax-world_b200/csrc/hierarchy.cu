@@ -632,21 +632,23 @@ __global__ void k_dense_from_bsr_all(const int32_t* __restrict__ top, const int6
 // columns and Kinv = X' X written over A (A is not read once X is complete). One block.
 __device__ void cholesky_inverse_block(int n, double* A, double* __restrict__ X, int32_t* __restrict__ status,
                                        int piece) {
-    __shared__ double red[1024];
+    __shared__ double red[32];
     __shared__ double dsh;
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
+    const int nw = (int)(blockDim.x + 31) / 32;
     for (int j = 0; j < n; j++) {
+        // the diagonal's sum: within each warp by shuffles, then the warps' sums by thread
+        // 0 (two barriers a column)
         double s = 0.0;
         for (int k = threadIdx.x; k < j; k += blockDim.x) s = fma(A[(int64_t)j * n + k], A[(int64_t)j * n + k], s);
-        red[threadIdx.x] = s;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
         __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
-        }
         if (threadIdx.x == 0) {
-            double v = A[(int64_t)j * n + j] - red[0];
+            double sum = 0.0;
+            for (int w = 0; w < nw; w++) sum += red[w];
+            double v = A[(int64_t)j * n + j] - sum;
             if (!(v > 0.0)) bad = 1;
             dsh = sqrt(v);
             A[(int64_t)j * n + j] = dsh;
