@@ -540,14 +540,23 @@ def large_section(solver, sc, args):
                        f"as the gradient's reference",
            "grid": [n, n, n], "free_cells": int((st == sc.CELL_FREE).sum()), "dof": 6 * parts, "tol": TOL}
     res = {}
-    for name, prec, tol in (("mixed", sc.MIXED, TOL), ("fp64", sc.FP64, 1e-10)):
-        t = time.perf_counter()
-        try:
-            C, grad, u, info = solver.compliance_grad(st, k, sc.options(tol=tol, precision=prec, max_iter=20000))
-        except sc.StaticsError as e:  # e.g. the device's memory: report it, keep the bench line
-            out[name] = {"error": str(e)}
-            return out
-        wall = time.perf_counter() - t
+    # the mixed solve twice: the first call also grows the device's memory pool to this
+    # size's peak (the driver maps new memory at tens of ms a GB), the second is the
+    # steady state a caller that keeps its context sees
+    for name, prec, tol, calls in (("mixed", sc.MIXED, TOL, 2), ("fp64", sc.FP64, 1e-10, 1)):
+        first = None
+        for call in range(calls):
+            t = time.perf_counter()
+            try:
+                C, grad, u, info = solver.compliance_grad(st, k, sc.options(tol=tol, precision=prec,
+                                                                            max_iter=20000))
+            except sc.StaticsError as e:  # e.g. the device's memory: report it, keep the bench line
+                out[name] = {"error": str(e)}
+                return out
+            wall = time.perf_counter() - t
+            if call == 0 and calls > 1:
+                first = {"setup_ms": info["setup_ms"], "solve_ms": info["solve_ms"],
+                         "time_to_tol_ms": info["setup_ms"] + info["solve_ms"], "wall_s_with_copies": wall}
         res[name] = grad
         out[name] = {"tol": tol, "status": info["status"], "iterations": info["iterations"],
                      "refinements": info["refinements"], "residual": info["residual"],
@@ -555,6 +564,8 @@ def large_section(solver, sc, args):
                      "time_to_tol_ms": info["setup_ms"] + info["solve_ms"], "wall_s_with_copies": wall,
                      "peak_hbm_bytes": info["peak_bytes"], "levels": info["parts"][:info["levels"]],
                      "compliance": C}
+        if first:
+            out[name]["first_call"] = first
     g, g64 = res["mixed"].ravel(), res["fp64"].ravel()
     free = st.ravel() == sc.CELL_FREE
     err = np.abs(g[free] - g64[free])

@@ -49,8 +49,8 @@ inline void require(bool ok, sc_status s, const std::string& msg) {
 // then allocate nothing. Requests are rounded up to size classes (1/8 steps of their
 // power of two, at least 512 bytes) and served by the smallest cached block of at least
 // their class and at most twice it, so that similar sizes share blocks (a batch's groups
-// differ a little in size, and a miss grows the driver's pool by mapping new memory, at
-// tens of milliseconds a gigabyte). Like a caching
+// differ in size, and a miss grows the driver's pool by mapping new memory, at tens of
+// milliseconds a gigabyte; the slack counts as held). Like a caching
 // allocator, the cache keeps what it is given up to `cap` bytes (half the device's memory
 // by default); when the pool runs out, an allocation gives the cached blocks back and
 // tries again.
