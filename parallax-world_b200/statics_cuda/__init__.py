@@ -406,19 +406,20 @@ class Solver:
         if loads is not None:
             loads = np.ascontiguousarray(loads, np.float64)
         g = make_grid(state, k, rho=rho, gravity=gravity, loads=loads)
-        n_nodes, _ = grid_count(state)
         if out is None:
+            n_nodes, _ = grid_count(state)
             out = np.zeros((max(n_nodes, 1), 6))
-        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size < 6 * n_nodes:
-            raise ValueError("out must be a C-contiguous float64 array of at least n_nodes x 6 values")
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size % 6:
+            raise ValueError("out must be a C-contiguous float64 array of n x 6 values")
         out = out.reshape(-1, 6) if out.ndim != 2 else out
         info = SolveInfo()
+        # the call checks out's capacity against the piece's node count (SC_BAD_INPUT)
         s = lib().sc_solve_grid(self.h, C.byref(g), C.byref(opt or options()), _ptr(out), out.size, 0,
                                 C.byref(info))
         self._check(s, "sc_solve_grid")
         d = info.as_dict()
         d["status"] = s
-        return out[:n_nodes], d
+        return out[:d["n_nodes"]], d
 
     def mech_levels(self, system: dict, size: float | None = None):
         """The levels the engine's solver makes on this context's device for `system`

@@ -381,7 +381,8 @@ def test_unsupported_piece_is_not_ok(solver, precision):
 
 def test_solve_grid_into_caller_buffer(solver):
     """solve_grid(out=...) writes the motions into the caller's array (a larger one too)
-    and gives the same values as a new array."""
+    and gives the same values as a new array; the C ABI turns down one too small
+    (SC_BAD_INPUT)."""
     st, k = piece(16, 0)
     opt = sc.options(max_iter=5000, tol=1e-8)
     u, _ = solver.solve_grid(st, k, opt)
@@ -390,7 +391,7 @@ def test_solve_grid_into_caller_buffer(solver):
     assert info["status"] == sc.OK
     assert np.shares_memory(u2, buf)
     assert np.array_equal(u, u2)
-    with pytest.raises(ValueError):
+    with pytest.raises(sc.StaticsError):
         solver.solve_grid(st, k, opt, out=np.zeros((2, 6)))
 
 
