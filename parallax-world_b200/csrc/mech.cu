@@ -5,9 +5,9 @@
 // ten power steps, a direct top) are made on the device by mech_levels.cu and kept there
 // as block-sparse rows (3x3 at the cells' nodes, 6x6 above, both triangles). This file
 // keeps a host copy of that construction (sc_mech_levels, no device) and runs the
-// conjugate gradients and V-cycles (solve.rs:403-538): block products, block-Jacobi
-// smoothing, the rigid restriction and prolongation, the top's dense inverse, and
-// deterministic dot products. Coarse pairs are kept in (a, c) order (the reference
+// conjugate gradients and V-cycles (solve.rs:403-538) as a device-side loop: block
+// products, block-Jacobi smoothing, the rigid restriction and prolongation, the top's
+// dense inverse, and deterministic dot products. Coarse pairs are kept in (a, c) order (the reference
 // collects them from a hash map, solve.rs:249-262): sums over pairs add in another order,
 // equal up to rounding.
 #include <algorithm>
@@ -562,16 +562,71 @@ __global__ void __launch_bounds__(256) k_mdot(int64_t n, const double* __restric
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-// x += alpha p, r -= alpha ap; or (update = 1) p = z + beta p
-__global__ void k_mupdate(int64_t n, int update, double s, double* __restrict__ x, double* __restrict__ r,
-                          const double* __restrict__ p, const double* __restrict__ ap) {
+// The PCG's scalars (solve.rs:485-538) where the iterations run on the device: the loop
+// goes on until `stop`, with `rounds` the rounds the reference would report.
+struct MechCG {
+    double rz, target, pap, alpha, beta, nx;
+    int32_t stop, round, rounds;
+    uint32_t count;  // rounds since the graph's launch
+};
+
+// *out = the partial sums of k_mdot, added in order (as the host adds them)
+__global__ void k_mdot_sum(const double* __restrict__ part, double* __restrict__ out) {
+    double s = 0.0;
+    for (int i = 0; i < MDOT_BLOCKS; i++) s += part[i];
+    *out = s;
+}
+
+// after p'Ap: a round that meets p'Ap <= 0 stops (and counts), else alpha = rz / p'Ap
+__global__ void k_mcg_alpha(MechCG* c) {
+    if (c->stop) return;
+    if (c->pap <= 0.0) {
+        c->rounds = c->round;
+        c->stop = 1;
+    } else {
+        c->alpha = c->rz / c->pap;
+    }
+}
+
+// after r'z: beta = r'z / rz, rz = r'z, the round done, and the next round's tests
+// (solve.rs: the cap stops, rz < 0 gives None, rz <= target stops)
+__global__ void k_mcg_beta(MechCG* c) {
+    if (c->stop) return;
+    c->beta = c->nx / c->rz;
+    c->rz = c->nx;
+    c->round += 1;
+    if (c->round >= MECH_ROUNDS) {  // the cap ends the loop before its tests
+        c->rounds = MECH_ROUNDS;
+        c->stop = 1;
+    } else if (c->rz < 0.0) {
+        c->rounds = -1;
+        c->stop = 1;
+    } else if (c->rz <= c->target) {
+        c->rounds = c->round;
+        c->stop = 1;
+    }
+}
+
+// the loop's condition: on while not stopped and fewer than `chunk` rounds ran since the
+// launch (so the host looks in now and then)
+__global__ void k_mcg_more(cudaGraphConditionalHandle h, MechCG* c, uint32_t chunk) {
+    const uint32_t n = c->count + 1u;
+    c->count = n;
+    cudaGraphSetConditional(h, (!c->stop && n < chunk) ? 1u : 0u);
+}
+
+// k_mupdate with the step from the device's scalars; nothing once stopped
+__global__ void k_mupdate_d(int64_t n, int update, const MechCG* __restrict__ c, double* __restrict__ x,
+                            double* __restrict__ r, const double* __restrict__ p, const double* __restrict__ ap) {
+    if (c->stop) return;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (update == 0) {
+        const double s = c->alpha;
         x[i] = x[i] + p[i] * s;
         r[i] = r[i] - ap[i] * s;
     } else {
-        x[i] = r[i] + x[i] * s;  // x = p, r = z
+        x[i] = r[i] + x[i] * c->beta;  // x = p, r = z
     }
 }
 
@@ -591,6 +646,13 @@ struct MechSolver {
         double s = 0.0;
         for (int i = 0; i < MDOT_BLOCKS; i++) s += hpart[i];
         return s;
+    }
+    // *out = a . b on the device (the same partial sums, added in the same order, as dot)
+    void dot_d(const double* a, const double* b, int64_t n, double* out) {
+        k_mdot<<<MDOT_BLOCKS, 256, 0, ctx.stream>>>(n, a, b, part.get());
+        SC_LAUNCH_CK();
+        k_mdot_sum<<<1, 1, 0, ctx.stream>>>(part.get(), out);
+        SC_LAUNCH_CK();
     }
     void times(const double* x, double* y, const double* b = nullptr) {
         k_bsr3<<<grid_for(M.n0, 128), 128, 0, ctx.stream>>>(M.n0, M.rowptr0.get(), M.col0.get(), M.val0.get(), x, b,
@@ -902,6 +964,89 @@ std::vector<double> mech_top_inverse(int64_t n, const double* diag36, int64_t np
     return std::move(L.top_inv);
 }
 
+// The PCG's rounds from the first one on (solve.rs:495-536), all on the device: a round
+// is captured once into a graph whose conditional WHILE node replays it until the scalars
+// say stop (or `chunk` rounds ran, when the host looks in); without conditional nodes the
+// round is launched from the host, which looks in after each. The same kernels and the
+// same additions in the same order as rounds driven from the host.
+static int device_rounds(Context& ctx, MechSolver& S, int64_t m, double rz, double target, double* x, double* r,
+                         double* z, double* p, double* ap, double* scratch) {
+    cudaStream_t st = ctx.stream;
+    DBuf<MechCG> cg;
+    cg.alloc(1, st, &ctx.mem);
+    MechCG c0{};
+    c0.rz = rz;
+    c0.target = target;
+    c0.rounds = MECH_ROUNDS;
+    cg.upload(&c0, 1);
+    MechCG* c = cg.get();
+    const unsigned g = grid_for(m, 256);
+    auto round = [&] {
+        S.times(p, ap);
+        S.dot_d(p, ap, m, &c->pap);
+        k_mcg_alpha<<<1, 1, 0, st>>>(c);
+        SC_LAUNCH_CK();
+        k_mupdate_d<<<g, 256, 0, st>>>(m, 0, c, x, r, p, ap);
+        SC_LAUNCH_CK();
+        S.precondition(r, z, scratch);
+        S.dot_d(r, z, m, &c->nx);
+        k_mcg_beta<<<1, 1, 0, st>>>(c);
+        SC_LAUNCH_CK();
+        k_mupdate_d<<<g, 256, 0, st>>>(m, 1, c, p, z, nullptr, nullptr);
+        SC_LAUNCH_CK();
+    };
+    const uint32_t chunk = 64;
+    cudaGraphExec_t exec = nullptr;
+    {
+        cudaGraph_t graph = nullptr;
+        cudaGraphConditionalHandle h = 0;
+        cudaGraphNodeParams prm = {};
+        prm.type = cudaGraphNodeTypeConditional;
+        prm.conditional.type = cudaGraphCondTypeWhile;
+        prm.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphCreate(&graph, 0) == cudaSuccess &&
+            cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess &&
+            (prm.conditional.handle = h, cudaGraphAddNode(&node, graph, nullptr, 0, &prm) == cudaSuccess) &&
+            cudaStreamBeginCaptureToGraph(st, prm.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            cudaGraph_t body = nullptr;
+            try {
+                round();
+                k_mcg_more<<<1, 1, 0, st>>>(h, c, chunk);
+                SC_LAUNCH_CK();
+            } catch (...) {
+                cudaStreamEndCapture(st, &body);
+                cudaGraphDestroy(graph);
+                throw;
+            }
+            if (cudaStreamEndCapture(st, &body) == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+                exec = nullptr;
+        }
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+    }
+    MechCG now{};
+    try {
+        for (;;) {
+            if (exec) {
+                SC_CK(cudaMemsetAsync(&c->count, 0, sizeof(uint32_t), st));
+                SC_CK(cudaGraphLaunch(exec, st));
+            } else {
+                round();
+            }
+            cg.download(&now, 1);
+            SC_CK(cudaStreamSynchronize(st));
+            if (now.stop) break;
+        }
+    } catch (...) {
+        if (exec) cudaGraphExecDestroy(exec);
+        throw;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    return now.rounds;
+}
+
 // The levels of the system, then PCG from x (solve.rs:356-386, 485-538): the rounds taken,
 // -1 where the levels do not fit the system (not positive).
 int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, const double* diag, int64_t npairs,
@@ -931,34 +1076,10 @@ int mech_solve(Context& ctx, int64_t n, const int64_t* sites, const double* at, 
         S.times(dx.get(), r.get(), db.get());  // r = b - S x
         S.precondition(r.get(), z.get(), scratch.get());
         SC_CK(cudaMemcpyAsync(p.get(), z.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        double rz = S.dot(r.get(), z.get(), m);
-        const unsigned g = grid_for(m, 256);
-        rounds = MECH_ROUNDS;
-        for (int round = 0; round < MECH_ROUNDS; round++) {
-            if (rz < 0.0) {
-                rounds = -1;
-                break;
-            }
-            if (rz <= target) {
-                rounds = round;
-                break;
-            }
-            S.times(p.get(), ap.get());
-            const double pap = S.dot(p.get(), ap.get(), m);
-            if (pap <= 0.0) {
-                rounds = round;
-                break;
-            }
-            const double alpha = rz / pap;
-            k_mupdate<<<g, 256, 0, st>>>(m, 0, alpha, dx.get(), r.get(), p.get(), ap.get());
-            SC_LAUNCH_CK();
-            S.precondition(r.get(), z.get(), scratch.get());
-            const double nx = S.dot(r.get(), z.get(), m);
-            const double beta = nx / rz;
-            rz = nx;
-            k_mupdate<<<g, 256, 0, st>>>(m, 1, beta, p.get(), z.get(), nullptr, nullptr);
-            SC_LAUNCH_CK();
-        }
+        const double rz = S.dot(r.get(), z.get(), m);
+        rounds = rz < 0.0 ? -1 : rz <= target ? 0 : MECH_ROUNDS;
+        if (rounds == MECH_ROUNDS) rounds = device_rounds(ctx, S, m, rz, target, dx.get(), r.get(), z.get(), p.get(),
+                                                          ap.get(), scratch.get());
     }
     dx.download(x, m);
     SC_CK(cudaStreamSynchronize(st));
