@@ -432,11 +432,11 @@ constexpr int SUM_THREADS = 6 * SUM_GROUPS;
 // block (the same addresses across the six, one transaction) and its column of the
 // right one, so a contribution costs 42 loads a thread instead of 12 for each of 36
 // threads.
-template <bool TA>
+template <bool TA, class TB>
 __global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, const int64_t* __restrict__ seg,
                                                              const uint64_t* __restrict__ vals,
                                                              const double* __restrict__ A,
-                                                             const double* __restrict__ B, double* __restrict__ out) {
+                                                             const TB* __restrict__ B, double* __restrict__ out) {
     const int g = threadIdx.x / 6, c = threadIdx.x % 6;
     const int64_t q = (int64_t)blockIdx.x * SUM_GROUPS + g;
     if (q >= nout) return;
@@ -449,9 +449,9 @@ __global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, cons
         double av[36];
     };
     auto load = [&](uint64_t v, Ops& o) {
-        const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
+        const TB* bb = B + 36 * (int64_t)(v & 0xffffffffu);
 #pragma unroll
-        for (int j = 0; j < 6; j++) o.bc[j] = bb[j * 6 + c];
+        for (int j = 0; j < 6; j++) o.bc[j] = (double)bb[j * 6 + c];
         const double2* a2 = reinterpret_cast<const double2*>(A + 36 * (int64_t)(v >> 32));
 #pragma unroll
         for (int t = 0; t < 18; t++) {
@@ -496,10 +496,11 @@ __global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, cons
 // per block).
 constexpr int K0SUM_WARPS = 6;
 constexpr int K0SUM_GROUPS = 5 * K0SUM_WARPS;
+template <class TO>
 __global__ void __launch_bounds__(32 * K0SUM_WARPS) k_sum_products_k0(int64_t nout, const int64_t* __restrict__ seg,
                                                                      const uint64_t* __restrict__ vals,
                                                                      const double* __restrict__ B,
-                                                                     double* __restrict__ out, K0View k0,
+                                                                     TO* __restrict__ out, K0View k0,
                                                                      const int32_t* __restrict__ krow) {
     __shared__ double T[36 * 36];
     for (int t = threadIdx.x; t < 36 * 36; t += blockDim.x) T[t] = k0.tpl_s[t];
@@ -546,7 +547,7 @@ __global__ void __launch_bounds__(32 * K0SUM_WARPS) k_sum_products_k0(int64_t no
         }
         if (live)
 #pragma unroll
-            for (int r = 0; r < 6; r++) out[36 * q + 6 * r + c] = acc[r];
+            for (int r = 0; r < 6; r++) out[36 * q + 6 * r + c] = (TO)acc[r];
     }
 }
 
@@ -1132,6 +1133,11 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
     DBuf<int32_t> kpcol;
     int64_t kpnnz = 0, kp_cands = 0, c_cands = 0;
     DBuf<double> kpval;
+    // Under SC_MIXED the V-cycle reads the coarse operators in FP32 only, so a matrix-free
+    // level 0's K P blocks (the largest array of the setup: 27.5 M blocks at 128^3) are
+    // held in FP32 where both products go through sorted sums; P'(KP) still adds in FP64.
+    DBuf<float> kpval32;
+    bool kp32 = false;
     if (by_rows) {
         DBuf<int32_t> lo, hi;
         lo.alloc(n, st, ms);
@@ -1180,16 +1186,25 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         }
         koff.release();
         keys_to_csr_with(ctx, keys, vin, tot, n, nc, kprow, kpcol, kpnnz, seg, vals);
-        kpval.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
+        kp32 = virt && opt.precision == SC_MIXED && !(fits && (gal == "rows" || kpnnz >= 12 * n));
+        if (kp32)
+            kpval32.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
+        else
+            kpval.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
         if (kpnnz > 0) {
             unsigned nb = (unsigned)((kpnnz + SUM_GROUPS - 1) / SUM_GROUPS);
-            if (virt)
-                k_sum_products_k0<<<std::min((unsigned)((kpnnz + K0SUM_GROUPS - 1) / K0SUM_GROUPS), 148u * 8u),
-                                    32 * K0SUM_WARPS, 0, st>>>(kpnnz, seg.get(), vals.get(), F.pval.get(),
-                                                               kpval.get(), k0, krow.get());
+            const unsigned nb0 = std::min((unsigned)((kpnnz + K0SUM_GROUPS - 1) / K0SUM_GROUPS), 148u * 8u);
+            if (virt && kp32)
+                k_sum_products_k0<float><<<nb0, 32 * K0SUM_WARPS, 0, st>>>(kpnnz, seg.get(), vals.get(),
+                                                                          F.pval.get(), kpval32.get(), k0,
+                                                                          krow.get());
+            else if (virt)
+                k_sum_products_k0<double><<<nb0, 32 * K0SUM_WARPS, 0, st>>>(kpnnz, seg.get(), vals.get(),
+                                                                           F.pval.get(), kpval.get(), k0,
+                                                                           krow.get());
             else
-                k_sum_products<false><<<nb, SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(), F.val.get(),
-                                                                  F.pval.get(), kpval.get());
+                k_sum_products<false, double><<<nb, SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(),
+                                                                          F.val.get(), F.pval.get(), kpval.get());
             SC_LAUNCH_CK();
         }
     }
@@ -1243,12 +1258,18 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         keys_to_csr_with(ctx, keys, vin, tot, nc, nc, urow, ucol, unnz, seg, vals);
         uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
         if (unnz > 0) {
-            k_sum_products<true><<<(unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS), SUM_THREADS, 0, st>>>(
-                unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get());
+            const unsigned nbu = (unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS);
+            if (kp32)
+                k_sum_products<true, float><<<nbu, SUM_THREADS, 0, st>>>(unnz, seg.get(), vals.get(), F.pval.get(),
+                                                                        kpval32.get(), uval.get());
+            else
+                k_sum_products<true, double><<<nbu, SUM_THREADS, 0, st>>>(unnz, seg.get(), vals.get(),
+                                                                         F.pval.get(), kpval.get(), uval.get());
             SC_LAUNCH_CK();
         }
     }
     kpval.release();
+    kpval32.release();
     kprow.release();
     kpcol.release();
     prow_of.release();
