@@ -697,6 +697,13 @@ __global__ void __launch_bounds__(1024) k_cholesky_inverse_all(const int32_t* __
     cholesky_inverse_block(n, A_all + off[blockIdx.x], X_all + off[blockIdx.x], status, p);
 }
 
+// each piece's value of a per-part flag at its first part (0 where it has no part)
+__global__ void k_first_flags(int np, const int64_t* __restrict__ pstart, const int32_t* __restrict__ flag,
+                              int32_t* __restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np) out[p] = pstart[p] < pstart[p + 1] ? flag[pstart[p]] : 0;
+}
+
 __global__ void k_fill_i32(int64_t n, int32_t* __restrict__ a, int32_t v) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < n) a[i] = v;
@@ -1426,14 +1433,22 @@ void build_hierarchy(Context& ctx, Batch& b, const sc_options& opt) {
         bool more = l + 1 < SC_MAX_LEVELS && coarsen(ctx, b, l, octree, opt);
         pt.mark("coarsen");
         Level& F = b.levels[l];  // reference may have moved
-        // pieces whose top is this level
+        // pieces whose top is this level (each piece's flag read at its first part)
         std::vector<int32_t> tops;
         {
-            std::vector<int32_t> topp = F.top_of_part.size() ? F.top_of_part.to_host() : std::vector<int32_t>();
+            std::vector<int32_t> topp;
+            if (F.top_of_part.size() && np > 0) {
+                DBuf<int32_t> first;
+                first.alloc(np, ctx.stream, &ctx.mem);
+                k_first_flags<<<grid_for(np, 128), 128, 0, ctx.stream>>>(np, F.pstart_d.get(), F.top_of_part.get(),
+                                                                       first.get());
+                SC_LAUNCH_CK();
+                topp = first.to_host();
+            }
             for (int p = 0; p < np; p++) {
                 int64_t a = F.pstart[p], e = F.pstart[p + 1];
                 if (a == e) continue;  // not on this level
-                bool top = !more || topp.empty() || topp[a];
+                bool top = !more || topp.empty() || topp[p];
                 if (top) tops.push_back(p);
             }
         }
