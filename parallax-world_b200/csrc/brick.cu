@@ -903,11 +903,11 @@ void brick_stencil(Context& ctx, const Batch& b, const T* x, const T* r, T* y, T
     const Bricks& K = b.grid.bricks;
     if (K.n_bricks <= 0) return;
     constexpr size_t smem = brick_smem<T>();
-    static bool attr_set = false;
-    if (!attr_set) {
+    static const bool attr_set = [] {  // once per instantiation (thread-safe)
         SC_CK(cudaFuncSetAttribute(k_brick_stencil<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
+        return true;
+    }();
+    (void)attr_set;
     k_brick_stencil<T, MODE><<<(unsigned)K.n_bricks, BRICK_THREADS, smem, ctx.stream>>>(
         view_of(K), x, r, y, y2, (T)b.grid.s, step, skip_row, done);
     SC_LAUNCH_CK();

@@ -890,12 +890,12 @@ static void launch_stencil(Context& ctx, const Batch& b, const T* x, const T* r,
         // one piece per block: the step and done flag are the block's piece's
         size_t smem = sizeof(T) * ((size_t)2 * (PTY + 1) * (PTZ + 1) * 6 + (size_t)(PTY + 1) * (PTZ + 1) +
                                    (size_t)PTY * PTZ * 18);
-        static bool attr_set[2][8] = {};
-        if (!attr_set[sizeof(T) == 8][MODE]) {
+        static const bool attr_set = [smem] {  // once per instantiation (thread-safe)
             SC_CK(cudaFuncSetAttribute(k_stencil_pencil<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-            attr_set[sizeof(T) == 8][MODE] = true;
-        }
+            return true;
+        }();
+        (void)attr_set;
         k_stencil_pencil<T, MODE><<<(unsigned)g.ntiles, PENCIL_THREADS, smem, ctx.stream>>>(
             reinterpret_cast<const PencilTile*>(g.tiles.get()), reinterpret_cast<const PieceGeo*>(g.geo.get()),
             g.gridmap.get(), g.cell.get(), x, r, y, y2, (T)g.s, step, skip_row, done);

@@ -375,12 +375,12 @@ void launch_split(Context& ctx, int mode, int64_t nrows, const int64_t* rowptr, 
 // are too few to fill the device twice over and each warp would still stream 16 or more
 // blocks (doubling up to 32).
 static int warps_per_row(int64_t nrows, int64_t nnz) {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
+    static const int sms = [] {  // once (thread-safe)
+        int dev = 0, v = 0;
         SC_CK(cudaGetDevice(&dev));
-        SC_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    }
+        SC_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        return v;
+    }();
     const int64_t target = (int64_t)sms * 64;  // two waves of 32 warps an SM
     const int64_t avg = nnz / std::max<int64_t>(nrows, 1);
     if (avg < 12) return 0;
