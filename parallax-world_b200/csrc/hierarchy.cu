@@ -432,10 +432,10 @@ constexpr int SUM_THREADS = 6 * SUM_GROUPS;
 // block (the same addresses across the six, one transaction) and its column of the
 // right one, so a contribution costs 42 loads a thread instead of 12 for each of 36
 // threads.
-template <bool TA, class TB>
+template <bool TA, class TAV, class TB>
 __global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, const int64_t* __restrict__ seg,
                                                              const uint64_t* __restrict__ vals,
-                                                             const double* __restrict__ A,
+                                                             const TAV* __restrict__ A,
                                                              const TB* __restrict__ B, double* __restrict__ out) {
     const int g = threadIdx.x / 6, c = threadIdx.x % 6;
     const int64_t q = (int64_t)blockIdx.x * SUM_GROUPS + g;
@@ -452,12 +452,24 @@ __global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, cons
         const TB* bb = B + 36 * (int64_t)(v & 0xffffffffu);
 #pragma unroll
         for (int j = 0; j < 6; j++) o.bc[j] = (double)bb[j * 6 + c];
-        const double2* a2 = reinterpret_cast<const double2*>(A + 36 * (int64_t)(v >> 32));
+        if constexpr (sizeof(TAV) == 8) {
+            const double2* a2 = reinterpret_cast<const double2*>(A + 36 * (int64_t)(v >> 32));
 #pragma unroll
-        for (int t = 0; t < 18; t++) {
-            double2 w = a2[t];
-            o.av[2 * t] = w.x;
-            o.av[2 * t + 1] = w.y;
+            for (int t = 0; t < 18; t++) {
+                double2 w = a2[t];
+                o.av[2 * t] = w.x;
+                o.av[2 * t + 1] = w.y;
+            }
+        } else {
+            const float4* a4 = reinterpret_cast<const float4*>(A + 36 * (int64_t)(v >> 32));
+#pragma unroll
+            for (int t = 0; t < 9; t++) {
+                float4 w = a4[t];
+                o.av[4 * t] = (double)w.x;
+                o.av[4 * t + 1] = (double)w.y;
+                o.av[4 * t + 2] = (double)w.z;
+                o.av[4 * t + 3] = (double)w.w;
+            }
         }
     };
     // acc(r) += sum_j op(A)(r, j) B(j, c)
@@ -496,10 +508,10 @@ __global__ void __launch_bounds__(SUM_THREADS) k_sum_products(int64_t nout, cons
 // per block).
 constexpr int K0SUM_WARPS = 6;
 constexpr int K0SUM_GROUPS = 5 * K0SUM_WARPS;
-template <class TO>
+template <class TB, class TO>
 __global__ void __launch_bounds__(32 * K0SUM_WARPS) k_sum_products_k0(int64_t nout, const int64_t* __restrict__ seg,
                                                                      const uint64_t* __restrict__ vals,
-                                                                     const double* __restrict__ B,
+                                                                     const TB* __restrict__ B,
                                                                      TO* __restrict__ out, K0View k0,
                                                                      const int32_t* __restrict__ krow) {
     __shared__ double T[36 * 36];
@@ -529,9 +541,9 @@ __global__ void __launch_bounds__(32 * K0SUM_WARPS) k_sum_products_k0(int64_t no
             double bc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, ar[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             if (has) {
                 const uint64_t v = vals[i + t];
-                const double* bb = B + 36 * (int64_t)(v & 0xffffffffu);
+                const TB* bb = B + 36 * (int64_t)(v & 0xffffffffu);
 #pragma unroll
-                for (int j = 0; j < 6; j++) bc[j] = bb[j * 6 + c];
+                for (int j = 0; j < 6; j++) bc[j] = (double)bb[j * 6 + c];
                 const uint8_t d = k0.desc[v >> 32];
 #pragma unroll
                 for (int j = 0; j < 6; j++) ar[j] = k0_entry(T, row, d, c, j);  // row c of A
@@ -1194,24 +1206,27 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         koff.release();
         keys_to_csr_with(ctx, keys, vin, tot, n, nc, kprow, kpcol, kpnnz, seg, vals);
         kp32 = virt && opt.precision == SC_MIXED && !(fits && (gal == "rows" || kpnnz >= 12 * n));
-        if (kp32)
+        if (kp32) {
+            // P too: both products read it, nothing after them (a matrix-free level 0
+            // transfers through its rigid part and the stencil)
+            to_float(ctx, F.pval, F.pval32);
+            F.pval.release();
             kpval32.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
-        else
+        } else {
             kpval.alloc(36 * std::max<int64_t>(kpnnz, 1), st, ms);
+        }
         if (kpnnz > 0) {
             unsigned nb = (unsigned)((kpnnz + SUM_GROUPS - 1) / SUM_GROUPS);
             const unsigned nb0 = std::min((unsigned)((kpnnz + K0SUM_GROUPS - 1) / K0SUM_GROUPS), 148u * 8u);
             if (virt && kp32)
-                k_sum_products_k0<float><<<nb0, 32 * K0SUM_WARPS, 0, st>>>(kpnnz, seg.get(), vals.get(),
-                                                                          F.pval.get(), kpval32.get(), k0,
-                                                                          krow.get());
+                k_sum_products_k0<float, float><<<nb0, 32 * K0SUM_WARPS, 0, st>>>(
+                    kpnnz, seg.get(), vals.get(), F.pval32.get(), kpval32.get(), k0, krow.get());
             else if (virt)
-                k_sum_products_k0<double><<<nb0, 32 * K0SUM_WARPS, 0, st>>>(kpnnz, seg.get(), vals.get(),
-                                                                           F.pval.get(), kpval.get(), k0,
-                                                                           krow.get());
+                k_sum_products_k0<double, double><<<nb0, 32 * K0SUM_WARPS, 0, st>>>(
+                    kpnnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), k0, krow.get());
             else
-                k_sum_products<false, double><<<nb, SUM_THREADS, 0, st>>>(kpnnz, seg.get(), vals.get(),
-                                                                          F.val.get(), F.pval.get(), kpval.get());
+                k_sum_products<false, double, double><<<nb, SUM_THREADS, 0, st>>>(
+                    kpnnz, seg.get(), vals.get(), F.val.get(), F.pval.get(), kpval.get());
             SC_LAUNCH_CK();
         }
     }
@@ -1267,11 +1282,11 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         if (unnz > 0) {
             const unsigned nbu = (unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS);
             if (kp32)
-                k_sum_products<true, float><<<nbu, SUM_THREADS, 0, st>>>(unnz, seg.get(), vals.get(), F.pval.get(),
-                                                                        kpval32.get(), uval.get());
+                k_sum_products<true, float, float><<<nbu, SUM_THREADS, 0, st>>>(
+                    unnz, seg.get(), vals.get(), F.pval32.get(), kpval32.get(), uval.get());
             else
-                k_sum_products<true, double><<<nbu, SUM_THREADS, 0, st>>>(unnz, seg.get(), vals.get(),
-                                                                         F.pval.get(), kpval.get(), uval.get());
+                k_sum_products<true, double, double><<<nbu, SUM_THREADS, 0, st>>>(
+                    unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get());
             SC_LAUNCH_CK();
         }
     }
@@ -1404,6 +1419,7 @@ static void release_level0_setup(Batch& b) {
     L0.rowptr.release();
     L0.inv.release();
     L0.pval.release();
+    L0.pval32.release();
     L0.pcol.release();
     L0.prow.release();
     L0.tptr.release();
