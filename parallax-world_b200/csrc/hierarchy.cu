@@ -260,22 +260,40 @@ __global__ void k_count_C(int64_t pnnz, const int32_t* __restrict__ prow_of, con
     int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], pcol[e]);
     cnt[e] = kprow[k + 1] - lb;
 }
-// candidates of the upper P'KP: (c, d) for each entry (k, c) of P and each block
-// (k, d >= c) of K P, contribution (entry of P << 32 | entry of KP)
+// candidates of the upper P'KP: (c, d) for each entry (k, c) of P with c0 <= c < c1 and
+// each block (k, d >= c) of K P, contribution (entry of P << 32 | entry of KP)
 __global__ void k_fill_C(int64_t pnnz, const int32_t* __restrict__ prow_of, const int32_t* __restrict__ pcol,
                          const int64_t* __restrict__ kprow, const int32_t* __restrict__ kpcol,
                          const int64_t* __restrict__ off, uint64_t* __restrict__ keys, uint64_t* __restrict__ vals,
-                         int cb) {
+                         int cb, int32_t c0, int32_t c1) {
     int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= pnnz) return;
     int32_t k = prow_of[e];
     int32_t c = pcol[e];
+    if (c < c0 || c >= c1) return;
     int64_t lb = lower_bound_i32(kpcol, kprow[k], kprow[k + 1], c);
     int64_t o = off[e];
     for (int64_t f = lb; f < kprow[k + 1]; f++, o++) {
         keys[o] = ((uint64_t)(uint32_t)c << cb) | (uint32_t)kpcol[f];
         vals[o] = ((uint64_t)e << 32) | (uint64_t)f;
     }
+}
+// the upper P'KP's candidates per coarse row (cnt zeroed beforehand)
+__global__ void k_row_cands(int64_t pnnz, const int32_t* __restrict__ pcol, const int64_t* __restrict__ ecnt,
+                            int64_t* __restrict__ cnt) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < pnnz && ecnt[e]) atomicAdd(reinterpret_cast<unsigned long long*>(cnt + pcol[e]), (unsigned long long)ecnt[e]);
+}
+// the counts of the P entries whose coarse row is in [c0, c1), others 0
+__global__ void k_slice_counts(int64_t pnnz, const int32_t* __restrict__ pcol, const int64_t* __restrict__ ecnt,
+                               int32_t c0, int32_t c1, int64_t* __restrict__ out) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < pnnz) out[e] = (pcol[e] >= c0 && pcol[e] < c1) ? ecnt[e] : 0;
+}
+// a += b
+__global__ void k_add_i64(int64_t n, int64_t* __restrict__ a, const int64_t* __restrict__ b) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] += b[i];
 }
 // keys are (row << cb | col)
 __global__ void k_unpack_pattern(int64_t m, const uint64_t* __restrict__ keys, int32_t* __restrict__ col,
@@ -1267,27 +1285,110 @@ static bool coarsen(Context& ctx, Batch& b, int l, int octree_level, const sc_op
         exclusive_scan(ctx, ecnt.get(), eoff.get(), F.pnnz + 1);
         tot = d2h_i64(ctx, eoff.get() + F.pnnz);
         c_cands = tot;
-        DBuf<uint64_t> keys, vin, vals;
-        DBuf<int64_t> seg;
-        keys.alloc(std::max<int64_t>(tot, 1), st, ms);
-        vin.alloc(std::max<int64_t>(tot, 1), st, ms);
-        if (F.pnnz > 0) {
-            k_fill_C<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, prow_of.get(), F.pcol.get(), kprow.get(),
-                                                            kpcol.get(), eoff.get(), keys.get(), vin.get(),
-                                                            bits_for(nc));
-            SC_LAUNCH_CK();
-        }
-        keys_to_csr_with(ctx, keys, vin, tot, nc, nc, urow, ucol, unnz, seg, vals);
-        uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
-        if (unnz > 0) {
-            const unsigned nbu = (unsigned)((unnz + SUM_GROUPS - 1) / SUM_GROUPS);
-            if (kp32)
-                k_sum_products<true, float, float><<<nbu, SUM_THREADS, 0, st>>>(
-                    unnz, seg.get(), vals.get(), F.pval32.get(), kpval32.get(), uval.get());
-            else
-                k_sum_products<true, double, double><<<nbu, SUM_THREADS, 0, st>>>(
-                    unnz, seg.get(), vals.get(), F.pval.get(), kpval.get(), uval.get());
-            SC_LAUNCH_CK();
+        eoff.release();
+        const int cbc = bits_for(nc);
+        // One slice of coarse rows [c0, c1): its candidates made, sorted and summed into
+        // its own rows (rp: the slice's entries before each row), columns and blocks.
+        auto upper_slice = [&](int32_t c0, int32_t c1, DBuf<int64_t>& rp, DBuf<int32_t>& cl, int64_t& nn,
+                               DBuf<double>& vv) {
+            DBuf<int64_t> scnt, soff;
+            const int64_t* cnt = ecnt.get();
+            if (c0 > 0 || c1 < nc) {
+                scnt.alloc(F.pnnz + 1, st, ms);
+                SC_CK(cudaMemsetAsync(scnt.get() + F.pnnz, 0, sizeof(int64_t), st));
+                if (F.pnnz > 0) {
+                    k_slice_counts<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, F.pcol.get(), ecnt.get(), c0, c1,
+                                                                          scnt.get());
+                    SC_LAUNCH_CK();
+                }
+                cnt = scnt.get();
+            }
+            soff.alloc(F.pnnz + 1, st, ms);
+            exclusive_scan(ctx, cnt, soff.get(), F.pnnz + 1);
+            const int64_t ns = d2h_i64(ctx, soff.get() + F.pnnz);
+            DBuf<uint64_t> keys, vin, vals;
+            DBuf<int64_t> seg;
+            keys.alloc(std::max<int64_t>(ns, 1), st, ms);
+            vin.alloc(std::max<int64_t>(ns, 1), st, ms);
+            if (F.pnnz > 0) {
+                k_fill_C<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, prow_of.get(), F.pcol.get(), kprow.get(),
+                                                                kpcol.get(), soff.get(), keys.get(), vin.get(), cbc,
+                                                                c0, c1);
+                SC_LAUNCH_CK();
+            }
+            scnt.release();
+            soff.release();
+            keys_to_csr_with(ctx, keys, vin, ns, nc, nc, rp, cl, nn, seg, vals);
+            vv.alloc(36 * std::max<int64_t>(nn, 1), st, ms);
+            if (nn > 0) {
+                const unsigned nbu = (unsigned)((nn + SUM_GROUPS - 1) / SUM_GROUPS);
+                if (kp32)
+                    k_sum_products<true, float, float><<<nbu, SUM_THREADS, 0, st>>>(
+                        nn, seg.get(), vals.get(), F.pval32.get(), kpval32.get(), vv.get());
+                else
+                    k_sum_products<true, double, double><<<nbu, SUM_THREADS, 0, st>>>(
+                        nn, seg.get(), vals.get(), F.pval.get(), kpval.get(), vv.get());
+                SC_LAUNCH_CK();
+            }
+        };
+        // All at once, or, where the candidates are many, in slices of coarse rows of at
+        // most `slice` candidates each: every output block's candidates are the same and in
+        // the same order either way (the same bits), and a slice's lists are gone before
+        // the next one's are made. SC_UPPER_SLICE lowers the limit (to test the slices).
+        int64_t slice = 96LL << 20;
+        if (const char* v = std::getenv("SC_UPPER_SLICE")) slice = std::max<int64_t>(1, std::atoll(v));
+        if (tot <= slice) {
+            upper_slice(0, (int32_t)nc, urow, ucol, unnz, uval);
+        } else {
+            DBuf<int64_t> rc;
+            rc.alloc(nc + 1, st, ms);
+            rc.zero();
+            if (F.pnnz > 0) {
+                k_row_cands<<<grid_for(F.pnnz, 256), 256, 0, st>>>(F.pnnz, F.pcol.get(), ecnt.get(), rc.get());
+                SC_LAUNCH_CK();
+            }
+            const std::vector<int64_t> rch = rc.to_host();
+            std::vector<std::pair<int32_t, int32_t>> sl;
+            int32_t c0 = 0;
+            int64_t acc = 0;
+            for (int32_t c = 0; c < (int32_t)nc; c++) {
+                if (c > c0 && acc + rch[c] > slice) {
+                    sl.push_back({c0, c});
+                    c0 = c;
+                    acc = 0;
+                }
+                acc += rch[c];
+            }
+            sl.push_back({c0, (int32_t)nc});
+            urow.alloc(nc + 1, st, ms);
+            urow.zero();
+            std::vector<DBuf<int32_t>> cols(sl.size());
+            std::vector<DBuf<double>> vls(sl.size());
+            std::vector<int64_t> nns(sl.size(), 0);
+            for (size_t i = 0; i < sl.size(); i++) {
+                DBuf<int64_t> rp;
+                upper_slice(sl[i].first, sl[i].second, rp, cols[i], nns[i], vls[i]);
+                k_add_i64<<<grid_for(nc + 1, 256), 256, 0, st>>>(nc + 1, urow.get(), rp.get());
+                SC_LAUNCH_CK();
+            }
+            kpval.release();  // the products are done
+            kpval32.release();
+            unnz = 0;
+            for (int64_t v : nns) unnz += v;
+            ucol.alloc(std::max<int64_t>(unnz, 1), st, ms);
+            uval.alloc(36 * std::max<int64_t>(unnz, 1), st, ms);
+            int64_t o = 0;
+            for (size_t i = 0; i < sl.size(); i++) {
+                if (nns[i] > 0) {
+                    SC_CK(cudaMemcpyAsync(ucol.get() + o, cols[i].get(), nns[i] * sizeof(int32_t),
+                                          cudaMemcpyDeviceToDevice, st));
+                    SC_CK(cudaMemcpyAsync(uval.get() + 36 * o, vls[i].get(), 36 * nns[i] * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, st));
+                }
+                o += nns[i];
+                cols[i].release();
+                vls[i].release();
+            }
         }
     }
     kpval.release();

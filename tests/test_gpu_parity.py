@@ -203,14 +203,17 @@ def test_batch_mixed(solver):
                                  {"SC_GALERKIN": "rows", "SC_ROWS_VARIANT": "0"},
                                  {"SC_GALERKIN": "rows", "SC_ROWS_VARIANT": "1"},
                                  {"SC_GALERKIN": "rows", "SC_ROWS_VARIANT": "2"},
-                                 {"SC_GALERKIN": "rows", "SC_ROWS_SLOTS": "3", "SC_ROWS_META": "5"}],
-                         ids=["default", "rows", "rows-64", "rows-192", "rows-areg", "rows-tiled"])
+                                 {"SC_GALERKIN": "rows", "SC_ROWS_SLOTS": "3", "SC_ROWS_META": "5"},
+                                 {"SC_GALERKIN": "sort", "SC_UPPER_SLICE": "20000"}],
+                         ids=["default", "rows", "rows-64", "rows-192", "rows-areg", "rows-tiled", "sort-sliced"])
 def test_galerkin_rows_match_sorted(solver, monkeypatch, env):
     """The row-by-row Galerkin products (pieces with at most 65536 coarse parts a level)
     and the sorted-candidate ones add the same products in the same order: the same
     bits, for a single piece and a batch, with the default choice per product and with
     every product row by row (level 0's K P then reads the cell template). Tiles of 3
-    output blocks and 5 staged entries split a row over many blocks and walk it often."""
+    output blocks and 5 staged entries split a row over many blocks and walk it often.
+    The sorted upper products made in slices of coarse rows (at most 20000 candidates a
+    slice) give the same bits as made at once."""
     opts = sc.options(max_iter=5000, tol=1e-8)
     st, k = piece(0, 11, shape=(40, 28, 36))
     batch = [piece(0, 300 + i, shape=(16 + 8 * (i % 3), 24, 20)) for i in range(4)]
